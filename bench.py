@@ -1,0 +1,338 @@
+"""Benchmark of the symmetry-sector matvec and its Lanczos recurrence on B200.
+
+Workload: the periodic XXZ chain N = 32 (J = 1, Delta = 0.7) in the sector S^z = 0, k = 0, reflection-even,
+spin-flip-even (group D_32 x Z_2, 128 elements; 4,707,969 representatives found on the device). Synthetic
+input: a seeded complex Gaussian vector. One step = one H.v on device-resident vectors with FP32 storage
+(FP64 arithmetic); the FP64-storage matvec and time-to-E0 (FP64 plain vs FP32 storage + FP64 refinement)
+are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the path has no
+cross-GPU exchange, so the metric is the sum over replicas and the time the max over ranks.
+`--impl reference` times the reference engine's own CPU matvec (oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload():
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    N = 32
+    spec = lat.chain_a1_flip_sector(N)
+    prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.7)
+    prog = ops.row_program(ops.from_products(N, prods))
+    return spec, prog, prods
+
+
+CONFIG = {"workload": "XXZ chain N=32 J=1 Delta=0.7, Sz=0 k=0 reflection-even flip-even (D32 x Z2)",
+          "n_sites": 32, "group_size": 128}
+
+
+class Clocks:
+    """nvidia-smi clock / throttle samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/qb_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        except FileNotFoundError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    """The reference engine's own CPU matvec (oracle/_ref) on the host cores: H.v/s on the same workload."""
+    if rank != 0:
+        return None
+    from oracle import ref as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU engine was not built into oracle/_ref"}))
+        return None
+    spec, prog, prods = workload()
+    threads = os.cpu_count() or 1
+    R.set_threads(threads)
+    t0 = time.time()
+    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+    build_s = time.time() - t0
+    rp = R.Operator(spec.n_sites, prods).row_program()
+    x = R.staged_seed(1, rs.dim)
+    for _ in range(args.warmup):
+        rs.gather(rp, x)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        rs.gather(rp, x)
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    v = args.steps / tot
+    line = {"impl": "reference", "metric": "H.v/s", "value": v, "unit": "H.v/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG, dim=rs.dim, lane="sector_gather (host walk, OpenMP)"),
+            "cpu_baseline": {"value": v, "unit": "H.v/s", "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} full H.v on the {rs.dim}-state sector"},
+            "e2e": {"value": v, "unit": "H.v/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_sector_build_s": build_s}
+    print(json.dumps(line))
+    return line
+
+
+def cpu_baseline_sample(dim_gpu):
+    """The reference engine's CPU matvec on a bounded sample: a few full H.v on the host cores."""
+    from oracle import ref as R
+    if not R.available():
+        return None
+    spec, prog, prods = workload()
+    threads = os.cpu_count() or 1
+    R.set_threads(threads)
+    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+    assert rs.dim == dim_gpu
+    rp = R.Operator(spec.n_sites, prods).row_program()
+    x = R.staged_seed(1, rs.dim)
+    rs.gather(rp, x)
+    n, t0 = 0, time.perf_counter()
+    while n < 3 or (time.perf_counter() - t0 < 10.0 and n < 20):
+        rs.gather(rp, x)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "H.v/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} full H.v (sector_gather, the reference's host walk) on the {rs.dim}-state sector"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = dist_init() if args.impl == "b200" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                   int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+
+    from qed_spin_b200 import build
+    from qed_spin_b200 import device as D
+    build.build()
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+
+    spec, prog, prods = workload()
+    t0 = time.perf_counter()
+    S = D.Sector(spec)
+    torch.cuda.synchronize()
+    enum_s = time.perf_counter() - t0
+    P = D.Program(prog)
+    n = S.dim
+    info = S.info()
+
+    # algorithmic bytes per H.v (8 rep + 8 inv_norm + S_out per row, S_in per emitted entry)
+    rng = np.random.default_rng(1)
+    x64 = torch.from_numpy(rng.normal(size=n) + 1j * rng.normal(size=n)).to(dev)
+    x32 = x64.to(torch.complex64)
+    y32 = torch.empty_like(x32)
+    y64 = torch.empty_like(x64)
+    e_bar = emitted_per_row(S.reps()[0], prog)
+
+    def b_alg(S_bytes):
+        return n * (8 + 8 + S_bytes) + n * e_bar * S_bytes
+
+    def time_matvec(x, y, dt, steps, warm):
+        for _ in range(warm):
+            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        barrier(world)
+        return dist_max(ms, world)
+
+    with Clocks(dev) as clk:
+        ms32 = time_matvec(x32, y32, "c64", args.steps, args.warmup)
+    ms64 = time_matvec(x64, y64, "c128", max(10, args.steps // 2), 3)
+    per32 = ms32 / args.steps
+    per64 = ms64 / max(10, args.steps // 2)
+    hbm, peak_kind = peaks()
+    ach32 = b_alg(8) / (per32 * 1e-3) / 1e9
+    ach64 = b_alg(16) / (per64 * 1e-3) / 1e9
+
+    # end to end through the public C-ABI: host start vector in, alpha/beta out, K Lanczos steps
+    v0 = (rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex128)
+    D.lanczos(S, P, v0, 8, dtype="c64")
+    torch.cuda.synchronize()
+    barrier(world)
+    t = time.perf_counter()
+    a, b = D.lanczos(S, P, v0, args.steps, dtype="c64")
+    e2e_s = time.perf_counter() - t
+    e2e_s = dist_max(e2e_s, world)
+
+    # time to E0: FP64 plain lane vs FP32 storage + FP64 refinement
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r64 = D.eigs_lowest(S, P, dtype="c128")
+    t64 = time.perf_counter() - t
+    t = time.perf_counter()
+    r32 = D.eigs_lowest(S, P, dtype="c64", refine=True)
+    t32 = time.perf_counter() - t
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_sample(n)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"unavailable": str(e)}
+
+    if rank != 0:
+        return
+    value = world * args.steps / (ms32 * 1e-3)
+    line = {
+        "metric": "H.v/s", "value": value, "unit": "H.v/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per32, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(CONFIG, dim=n, emitted_per_row=e_bar, storage="complex64 vectors, FP64 arithmetic",
+                       lookup=info["lookup"], sublattice=[info["slc_L"], info["slc_m"]],
+                       l2="working set > 126 MB L2 (reps, inv_norms, x, y, lookup ~0.2 GB), no flush",
+                       parallelism=f"replicas x{world}"),
+        "roofline": {"bound": "hbm", "achieved": ach32, "peak": hbm, "unit": "GB/s", "frac": ach32 / hbm,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": b_alg(8)},
+        "fp64": {"ms_per_hv": per64, "hv_per_s": 1e3 / per64, "achieved_gbs": ach64, "frac": ach64 / hbm},
+        "e2e": {"value": world * args.steps / e2e_s, "unit": "H.v/s", "h2d_bytes_per_step": 16 * n / args.steps,
+                "d2h_bytes_per_step": 16, "path": "qb_lanczos (host v0 in, alpha/beta out, FP32 storage)"},
+        "time_to_e0": {"fp64_s": t64, "fp64_e0": r64["e0"], "fp64_iters": r64["iters"],
+                       "fp32_refined_s": t32, "fp32_refined_e0": r32["e0"], "fp32_matvecs": r32["matvecs"],
+                       "rel_err": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]), "speedup": t64 / t32},
+        "enumeration_s": enum_s,
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def emitted_per_row(reps: np.ndarray, prog) -> float:
+    """Mean number of program groups that act on a representative (each reads one x element): the
+    exact count over the sector's representatives."""
+    total = 0
+    for g in range(prog.n_groups):
+        F = np.uint64(prog.group_flip[g])
+        vals = prog.vsub_val[prog.group_vbegin[g]:prog.group_vbegin[g + 1]].astype(np.uint64)
+        total += int(np.count_nonzero(np.isin(reps & F, vals)))
+    return total / len(reps)
+
+
+if __name__ == "__main__":
+    main()

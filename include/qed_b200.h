@@ -1,0 +1,158 @@
+/* =============================================================================
+ * include/qed_b200.h -- the C-ABI of the B200 symmetry-sector matvec and its Krylov recurrences.
+ *
+ * The drop-in boundary for the reference engine's device lane: plain C types, opaque handles,
+ * integer status codes, an explicit CUDA stream (NULL: the legacy default stream, the one the
+ * reference's device lane orders its work on). Nothing here throws across the ABI.
+ *
+ * Conventions.
+ *   - A basis state is a uint64 bit string, a SET bit an UP spin (include/ed/ops/term.h:27-34 in the
+ *     reference). A group element maps s to permute_bits(s, perm) ^ flip, new bit i = old bit perm[i]
+ *     (include/ed/basis/compiled_group.h:8-14).
+ *   - Complex vectors are interleaved (re, im): double pairs (QB_C128, the reference's
+ *     std::complex<double>) or float pairs (QB_C64, the FP32-storage form).
+ *   - Multi-vector ("block") vectors are interleaved by row: element (row r, vector v) at r*k + v.
+ *
+ * Every function returns QB_OK or an error code; qb_last_error() describes the last failure of
+ * the calling thread.
+ * ============================================================================= */
+#ifndef QED_B200_H
+#define QED_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    QB_OK = 0,
+    QB_EINVAL = 1,       /* malformed arguments (maps onto std::invalid_argument) */
+    QB_ENOMEM = 2,       /* device allocation failed (maps onto ed::ResourceLimit) */
+    QB_ECUDA = 3,        /* a CUDA runtime error (maps onto std::runtime_error) */
+    QB_EUNSUPPORTED = 4, /* a form this build does not implement (maps onto ed::DeviceUnsupported) */
+    QB_ETIMEOUT = 5,     /* a bounded device wait ran out */
+    QB_ENODEV = 6        /* no CUDA device (maps onto ed::DeviceUnavailable) */
+};
+
+enum { QB_C128 = 0, QB_C64 = 1 };
+
+enum { QB_REORTH_NONE = 0, QB_REORTH_FULL = 1, QB_REORTH_LOCAL = 2 };
+
+enum { QB_LOOKUP_AUTO = 0, QB_LOOKUP_RANK = 1, QB_LOOKUP_BUCKETS = 2 };
+
+typedef struct qb_sector qb_sector;
+typedef struct qb_program qb_program;
+
+/* A sector: the fixed-S^z states of n_sites spins with n_up up spins, reduced by a group of
+ * group_size elements in the one-dimensional irrep with characters chars (interleaved complex).
+ * sublattice_mode picks the representative order (include/ed/basis/sublattice_code.h:23-34):
+ * 0 the plain order, 1 the sublattice key order whenever a block system exists, -1 the size rule
+ * of device verbs (N >= 24 and >= 16 distinct permutations), -2 the strict rule (>= 64).
+ * All pointers are host memory. */
+typedef struct {
+    int n_sites;
+    int n_up;
+    int group_size;
+    const int32_t* perms;  /* group_size x n_sites */
+    const uint64_t* flips; /* group_size XOR masks, or NULL */
+    const double* chars;   /* 2 x group_size */
+    int sublattice_mode;
+    int lookup;             /* QB_LOOKUP_* : state -> index structure */
+} qb_sector_desc;
+
+/* A row program in the reference's MaskedProgram layout (include/ed/ops/program.h:66-94):
+ * groups by ascending flip mask, value subgroups ascending, terms in key order. Host memory. */
+typedef struct {
+    uint32_t n_groups;
+    const uint64_t* group_flip;    /* n_groups */
+    const int32_t* group_setbits;  /* n_groups; -1: the subgroups differ in popcount */
+    const uint32_t* group_vbegin;  /* n_groups + 1 */
+    uint32_t n_vsub;
+    const uint64_t* vsub_val;      /* n_vsub */
+    const uint32_t* vsub_tbegin;   /* n_vsub + 1 */
+    uint32_t n_terms;
+    const uint64_t* term_sign;     /* n_terms */
+    const double* term_coeff;      /* 2 x n_terms */
+} qb_program_desc;
+
+const char* qb_last_error(void);
+int qb_device_count(int* count);
+
+/* ---- sectors -------------------------------------------------------------------------------
+ * qb_sector_create enumerates the sector on the device: the representatives ascending, their
+ * 1/norm, and the state -> index lookup. Replaces the reference's host orbit scan and sector
+ * filter (include/ed/basis/orbit_table.h:250-286 build_orbit_table_fixed_sz_streaming,
+ * src/engine/group_sector.cpp:159-205 filter_reps, src/engine/context.cpp:189-207 build_k_sector)
+ * and its device mirror upload (src/gpu/rep_matvec.cu:253-383 build_sector_mirror). */
+int qb_sector_create(const qb_sector_desc* desc, qb_sector** out);
+/* The same from host representatives computed elsewhere (reps ascending, inv_norms): the upload
+ * the reference's make_sector_matvec_gpu_rep performs from a RepSectorData
+ * (include/ed/gpu/rep_matvec.h:43-60). */
+int qb_sector_create_from_reps(const qb_sector_desc* desc, const uint64_t* reps, const double* inv_norms,
+                               uint64_t dim, qb_sector** out);
+int qb_sector_destroy(qb_sector* s);
+uint64_t qb_sector_dim(const qb_sector* s);
+/* Copies the representatives and 1/norms to host memory (either pointer may be NULL). */
+int qb_sector_download(const qb_sector* s, uint64_t* reps, double* inv_norms);
+/* Bytes of device memory the sector holds; sublattice block size L and block count m (0: none). */
+int qb_sector_info(const qb_sector* s, uint64_t* device_bytes, int* slc_L, int* slc_m, int* lookup_kind);
+/* The orbit index and projection phase of a state (index_and_projection,
+ * include/ed/matvec/rep_symmetry_basis_policy.h:221-241), for n states at once (host arrays). */
+int qb_index_and_projection(const qb_sector* s, const uint64_t* states, uint64_t n, int64_t* index, double* proj);
+
+/* ---- programs ------------------------------------------------------------------------------ */
+int qb_program_create(const qb_program_desc* desc, qb_program** out);
+int qb_program_destroy(qb_program* p);
+
+/* ---- the matvec ----------------------------------------------------------------------------
+ * outs[i] = O ins[i] for i < k: rows in sector `row`, columns in sector `col` (row == col: one
+ * sector, the diagonal without a lookup). Device pointers of the given dtype. Every output equals
+ * the single apply bit for bit. Replaces make_sector_matvec_gpu_rep / _multi and
+ * make_cross_matvec_gpu_rep (include/ed/gpu/rep_matvec.h:43-70, src/gpu/rep_matvec.cu:410-490) and
+ * serves LinearOperator::bind_cuda / bind_cuda_multi (include/ed/matvec/linear_operator.h:45-69). */
+int qb_matvec(const qb_sector* row, const qb_sector* col, const qb_program* prog, const void* const* ins,
+              void* const* outs, int k, int dtype, void* stream);
+/* out = O in on k vectors interleaved by row (element r*k + v): the block matvec of the sampled
+ * methods, one canonicalisation per emitted entry for all k vectors. */
+int qb_matvec_block(const qb_sector* row, const qb_sector* col, const qb_program* prog, const void* in, void* out,
+                    int k, int dtype, void* stream);
+/* The host-pointer twin (make_sector_matvec_gpu_rep_hostptr, include/ed/gpu/rep_matvec.h:61-66):
+ * host complex128 in / out, staged through the device. */
+int qb_matvec_host(const qb_sector* row, const qb_sector* col, const qb_program* prog, const double* in_host,
+                   double* out_host);
+
+/* ---- Krylov recurrences --------------------------------------------------------------------
+ * The Lanczos kernel (include/ed/krylov/lanczos.h:266-576) on one sector, device-resident: alpha,
+ * beta and every inner product in FP64, vectors stored as dtype. v0 is a host complex128 vector
+ * (it is normalised on the device). alpha has room for max_iter values, beta for max_iter + 1
+ * (beta[0] = 0). reorth: QB_REORTH_NONE or QB_REORTH_LOCAL (ring of 1, threshold sqrt(eps)). */
+int qb_lanczos(const qb_sector* sec, const qb_program* prog, const double* v0_host, int max_iter, int reorth,
+               double breakdown_tol, int dtype, double* alpha, double* beta, int* iters);
+
+/* The k = 1 block lane (lowest_scan_lane, src/engine/block_solve.cpp:528-598): a Lanczos scan from
+ * the staged Gaussian start of seed 0x51ED0B70 with the Paige-gated, ghost-aware lowest-level test
+ * after every step; budget max_iter (0: 400). dtype QB_C64 runs the recurrence on FP32-stored
+ * vectors; refine != 0 then polishes the level with FP64 restarted Lanczos from its Ritz vector to
+ * |dE|/|E| <= 1e-12. e0: the lowest level (NaN if none converged). */
+int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, int dtype, int refine, double* e0,
+                   int* iters, int* converged, int* matvecs);
+
+/* FTLM on one block (ftlm_kernel, include/ed/thermal/ftlm.h:277-480; sample vectors of
+ * include/ed/thermal/sample_seed.h:37-89): all samples advance together as one block matvec.
+ * Outputs per beta: lnZ, E, V; and the lowest weighted Ritz value. */
+int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth, uint64_t seed, const double* betas,
+            int n_beta, int dtype, double* lnZ, double* E, double* V, double* e_min);
+
+/* The T = 0 continued fraction from a host complex128 vector phi on one sector
+ * (cf_spectral_from_vector, include/ed/dynamics/cf.h:104-160): Lanczos without reorthogonalisation to
+ * `depth`, breakdown at `tolerance`, S(w) = -Im G(w + i eta)/pi with G weighted by ||phi||^2; shift: the
+ * energy w is measured from (NaN: the tridiagonal's lowest value). */
+int qb_cf(const qb_sector* sec, const qb_program* prog, const double* phi_host, int depth, const double* omega,
+          int n_omega, double eta, double shift, double tolerance, double* S, double* shift_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

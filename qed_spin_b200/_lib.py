@@ -1,0 +1,114 @@
+"""ctypes bindings of the C-ABI declared in include/qed_b200.h (libqed_b200.so, built in-tree).
+
+Loading fails loudly: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqed_b200.so")
+
+QB_OK, QB_EINVAL, QB_ENOMEM, QB_ECUDA, QB_EUNSUPPORTED, QB_ETIMEOUT, QB_ENODEV = range(7)
+QB_C128, QB_C64 = 0, 1
+QB_REORTH_NONE, QB_REORTH_FULL, QB_REORTH_LOCAL = 0, 1, 2
+QB_LOOKUP_AUTO, QB_LOOKUP_RANK, QB_LOOKUP_BUCKETS = 0, 1, 2
+
+#: every symbol include/qed_b200.h declares
+EXPORTS = [
+    "qb_last_error", "qb_device_count",
+    "qb_sector_create", "qb_sector_create_from_reps", "qb_sector_destroy", "qb_sector_dim", "qb_sector_download",
+    "qb_sector_info", "qb_index_and_projection",
+    "qb_program_create", "qb_program_destroy",
+    "qb_matvec", "qb_matvec_block", "qb_matvec_host",
+    "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_cf",
+]
+
+
+class SectorDesc(C.Structure):
+    _fields_ = [
+        ("n_sites", C.c_int), ("n_up", C.c_int), ("group_size", C.c_int),
+        ("perms", C.c_void_p), ("flips", C.c_void_p), ("chars", C.c_void_p),
+        ("sublattice_mode", C.c_int), ("lookup", C.c_int),
+    ]
+
+
+class ProgramDesc(C.Structure):
+    _fields_ = [
+        ("n_groups", C.c_uint32), ("group_flip", C.c_void_p), ("group_setbits", C.c_void_p),
+        ("group_vbegin", C.c_void_p), ("n_vsub", C.c_uint32), ("vsub_val", C.c_void_p),
+        ("vsub_tbegin", C.c_void_p), ("n_terms", C.c_uint32), ("term_sign", C.c_void_p),
+        ("term_coeff", C.c_void_p),
+    ]
+
+
+class QbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[qb error {code}] {msg}")
+        self.code = code
+
+
+class DeviceUnavailable(QbError):
+    pass
+
+
+class ResourceLimit(QbError):
+    pass
+
+
+class Unsupported(QbError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"the CUDA library is not built ({LIB_PATH}); run `python -m qed_spin_b200.build` "
+                           "-- there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    vp, i, u64, d = C.c_void_p, C.c_int, C.c_uint64, C.c_double
+    L.qb_last_error.restype = C.c_char_p
+    L.qb_device_count.argtypes = [C.POINTER(i)]
+    L.qb_sector_create.argtypes = [C.POINTER(SectorDesc), C.POINTER(vp)]
+    L.qb_sector_create_from_reps.argtypes = [C.POINTER(SectorDesc), vp, vp, u64, C.POINTER(vp)]
+    L.qb_sector_destroy.argtypes = [vp]
+    L.qb_sector_dim.argtypes = [vp]
+    L.qb_sector_dim.restype = u64
+    L.qb_sector_download.argtypes = [vp, vp, vp]
+    L.qb_sector_info.argtypes = [vp, C.POINTER(u64), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.qb_index_and_projection.argtypes = [vp, vp, u64, vp, vp]
+    L.qb_program_create.argtypes = [C.POINTER(ProgramDesc), C.POINTER(vp)]
+    L.qb_program_destroy.argtypes = [vp]
+    L.qb_matvec.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
+    L.qb_matvec_block.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
+    L.qb_matvec_host.argtypes = [vp, vp, vp, vp, vp]
+    L.qb_lanczos.argtypes = [vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i)]
+    L.qb_eigs_lowest.argtypes = [vp, vp, i, i, i, C.POINTER(d), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]
+    L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]
+    for name in EXPORTS:
+        if name not in ("qb_last_error", "qb_sector_dim"):
+            getattr(L, name).restype = i
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc == QB_OK:
+        return
+    msg = lib().qb_last_error().decode()
+    if rc == QB_ENODEV:
+        raise DeviceUnavailable(rc, msg)
+    if rc == QB_ENOMEM:
+        raise ResourceLimit(rc, msg)
+    if rc == QB_EUNSUPPORTED:
+        raise Unsupported(rc, msg)
+    if rc == QB_EINVAL:
+        raise ValueError(f"[qb error {rc}] {msg}")
+    raise QbError(rc, msg)

@@ -1,0 +1,191 @@
+// =============================================================================
+// qb_internal.cuh -- device-side types shared by the sector, matvec and Krylov translation units.
+//
+// Layout in HBM of one sector (qb_sector):
+//   reps       u64[dim]    the representatives, ascending (the basis index IS the array index)
+//   inv_norms  f64[dim]    1/norm per representative
+//   lut        u64[G][bpw][256]   the byte-decomposition image table of every group element
+//   flips      u64[G], chars f64x2[G]
+//   to_key     u64[bpw][256]      sublattice key order (when engaged)
+//   lead       u16[m][2^L], cand_off u32[m 2^L + 1], cand u16[...]  leading-block table / candidates
+//   lookup     either rank_table i32[C(N, n_up)] indexed by the combinadic rank (computed from
+//              rank_lut u64[bpw][N+1][256]), or bucket_off u32[n_buckets + 1] over the states.
+// The small tables (program, to_key) are staged in shared memory by each kernel.
+// =============================================================================
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qed_b200.h"
+
+namespace qb {
+
+using u64 = unsigned long long;
+using u32 = std::uint32_t;
+using u16 = std::uint16_t;
+
+// ---------------------------------------------------------------------------------------------
+// Errors: every C entry point catches qb::Error and returns its code.
+// ---------------------------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& m);
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const int code = (e == cudaErrorMemoryAllocation) ? QB_ENOMEM : (e == cudaErrorNoDevice ? QB_ENODEV : QB_ECUDA);
+    (void)cudaGetLastError();
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return QB_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return QB_ENOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return QB_EINVAL;
+    }
+}
+
+// A device allocation owned by a host object.
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    std::size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(std::size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p, n = o.n;
+            o.p = nullptr, o.n = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(std::size_t count) {
+        release();
+        if (count == 0) return;
+        cuda_check(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void upload(const T* h, std::size_t count) {
+        alloc(count);
+        if (count) cuda_check(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    }
+    void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
+    std::size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Device views (trivially copyable; passed by value to kernels).
+// ---------------------------------------------------------------------------------------------
+struct DSlc {
+    int on = 0, L = 0, m = 0;
+    const u64* to_key = nullptr;    // bpw x 256
+    const u16* lead = nullptr;      // m << L
+    const u32* cand_off = nullptr;  // (m << L) + 1
+    const u16* cand = nullptr;
+};
+
+struct DSector {
+    int N = 0, n_up = 0, G = 0, bpw = 0;
+    std::uint64_t dim = 0;
+    const u64* reps = nullptr;
+    const double* inv_norms = nullptr;
+    const u64* lut = nullptr;       // G x bpw x 256
+    const u64* flips = nullptr;     // G
+    const double2* chars = nullptr; // G
+    DSlc slc;
+    // lookup: kind 1 rank table, 2 state buckets
+    int lookup = 0;
+    const std::int32_t* rank_table = nullptr;
+    const u64* rank_lut = nullptr;  // bpw x (N + 1) x 256: byte b's share of the combinadic rank
+    const u32* bucket_off = nullptr;
+    u64 bucket_base = 0, bucket_count = 0;
+    int bucket_shift = 0;
+};
+
+struct DProgram {
+    u32 n_groups = 0, n_vsub = 0, n_terms = 0;
+    const u64* group_flip = nullptr;
+    const int* group_setbits = nullptr;
+    const u32* group_vbegin = nullptr;
+    const u64* vsub_val = nullptr;
+    const u32* vsub_tbegin = nullptr;
+    const u64* term_sign = nullptr;
+    const double2* term_coeff = nullptr;
+    std::size_t smem_bytes = 0;   // bytes to stage the whole program in shared memory
+};
+
+}  // namespace qb
+
+// The host objects behind the opaque handles.
+struct qb_sector {
+    int N = 0, n_up = 0, G = 0, bpw = 0;
+    std::uint64_t dim = 0;
+    qb::DevBuf<qb::u64> reps;
+    qb::DevBuf<double> inv_norms;
+    qb::DevBuf<qb::u64> lut, flips;
+    qb::DevBuf<double2> chars;
+    qb::DevBuf<qb::u64> to_key;
+    qb::DevBuf<qb::u16> lead, cand;
+    qb::DevBuf<qb::u32> cand_off;
+    qb::DevBuf<std::int32_t> rank_table;
+    qb::DevBuf<qb::u64> rank_lut;
+    qb::DevBuf<qb::u32> bucket_off;
+    int slc_on = 0, slc_L = 0, slc_m = 0;
+    int lookup = 0;
+    qb::u64 bucket_base = 0, bucket_count = 0;
+    int bucket_shift = 0;
+    std::vector<double> chars_host;   // 2G
+    qb::DSector view() const;
+    std::uint64_t device_bytes() const;
+};
+
+struct qb_program {
+    qb::DevBuf<unsigned char> blob;   // every array back to back (8-byte aligned), staged as one copy
+    qb::DProgram view;
+    double norm_bound = 0.0;          // sum of |coeff|
+};
+
+namespace qb {
+
+// ---------------------------------------------------------------------------------------------
+// Exact complex arithmetic: the operations std::complex<double> performs on the host, without
+// fused multiply-adds, so device results equal the reference's host arithmetic bit for bit.
+// ---------------------------------------------------------------------------------------------
+struct cplx {
+    double re, im;
+};
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+    return {__dsub_rn(__dmul_rn(a.re, b.re), __dmul_rn(a.im, b.im)),
+            __dadd_rn(__dmul_rn(a.re, b.im), __dmul_rn(a.im, b.re))};
+}
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {__dadd_rn(a.re, b.re), __dadd_rn(a.im, b.im)}; }
+__device__ __forceinline__ cplx cconj(cplx a) { return {a.re, -a.im}; }
+__device__ __forceinline__ cplx rscale(double w, cplx a) { return {__dmul_rn(w, a.re), __dmul_rn(w, a.im)}; }
+
+}  // namespace qb

@@ -1,0 +1,620 @@
+// =============================================================================
+// sector.cu -- a symmetry sector on the device: the group tables, the sublattice key order, the
+// device enumeration of the representatives, and the state -> index lookup.
+//
+// The enumeration replaces the reference's host orbit scan + filter
+// (include/ed/basis/orbit_table.h:147-286, src/engine/group_sector.cpp:159-205): the C(N, n_up)
+// states are cut into chunks of consecutive combinadic ranks; each thread unranks its chunk's
+// first state and walks the rest in Gosper order (include/ed/basis/gosper.h:24), keeping a state
+// when no element maps it below itself (in the key order with a sublattice code) and its projected
+// norm |sum_{h in Stab} chi(h)|^2 / |Stab| exceeds 1e-12. A count pass, an exclusive scan and a
+// write pass place the representatives in ascending order, bit-identical to the reference's table.
+// =============================================================================
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+
+#include "qb_canon.cuh"
+
+namespace qb {
+
+thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
+
+namespace {
+
+// -------------------------------------------------------------------------------------------
+// Host builders of the small tables.
+// -------------------------------------------------------------------------------------------
+
+// Byte-decomposition image table (compiled_group.h:108-140): lut[(g bpw + b) 256 + v].
+std::vector<u64> build_lut(const int32_t* perms, int G, int N) {
+    const int bpw = (N + 7) / 8;
+    std::vector<u64> lut(static_cast<std::size_t>(G) * bpw * 256, 0ULL);
+    for (int g = 0; g < G; ++g) {
+        int inv[64];
+        for (int i = 0; i < N; ++i) inv[perms[g * N + i]] = i;
+        for (int b = 0; b < bpw; ++b)
+            for (int v = 0; v < 256; ++v) {
+                u64 out = 0;
+                for (int t = 0; t < 8 && 8 * b + t < N; ++t)
+                    if ((v >> t) & 1) out |= 1ULL << inv[8 * b + t];
+                lut[(static_cast<std::size_t>(g) * bpw + b) * 256 + v] = out;
+            }
+    }
+    return lut;
+}
+
+struct SlcHost {
+    bool on = false;
+    int L = 0, m = 0;
+    std::vector<u64> to_key;
+    std::vector<u16> lead;
+    std::vector<u32> cand_off;
+    std::vector<u16> cand;
+};
+
+// The block system with the largest blocks (<= 16 sites, 2..8 equal blocks), first found on ties:
+// the finest group-invariant partition joining sites 0 and b, for every b (sublattice_code.h:232-270).
+std::vector<int> block_system(const std::vector<std::vector<int>>& sp, int N, int& L) {
+    L = 0;
+    std::vector<int> best, parent(N);
+    auto find = [&](int x) {
+        while (parent[x] != x) {
+            parent[x] = parent[parent[x]];
+            x = parent[x];
+        }
+        return x;
+    };
+    for (int b = 1; b < N; ++b) {
+        std::iota(parent.begin(), parent.end(), 0);
+        parent[b] = 0;
+        std::vector<std::pair<int, int>> todo{{0, b}};
+        while (!todo.empty()) {
+            const auto [x, y] = todo.back();
+            todo.pop_back();
+            for (const auto& p : sp) {
+                const int px = p[x], py = p[y];
+                const int u = find(px), v = find(py);
+                if (u == v) continue;
+                parent[std::max(u, v)] = std::min(u, v);
+                todo.emplace_back(px, py);
+            }
+        }
+        std::vector<int> size(N, 0);
+        for (int s = 0; s < N; ++s) ++size[find(s)];
+        const int l = size[0];
+        if (l > 16 || l <= L || N % l != 0 || N / l < 2 || N / l > 8) continue;
+        bool equal = true;
+        for (int s = 0; s < N && equal; ++s) equal = size[find(s)] == l;
+        if (!equal) continue;
+        std::vector<int> root_block(N, -1), block(N);
+        int nb = 0;
+        for (int s = 0; s < N; ++s) {
+            int& rb = root_block[find(s)];
+            if (rb < 0) rb = nb++;
+            block[s] = rb;
+        }
+        L = l;
+        best = std::move(block);
+    }
+    return best;
+}
+
+// The sublattice code of the group (sublattice_code.h:164-191 rule, 300-399 tables).
+SlcHost build_slc(const int32_t* perms, const u64* flips, int G, int N, int mode) {
+    SlcHost c;
+    if (mode == 0 || G <= 1 || N < 4 || N > 64 || G > 65535) return c;
+    const std::size_t min_perms = mode == 1 ? 0 : (mode == -1 ? 16 : 64);
+    std::vector<std::vector<int>> sp;
+    for (int g = 0; g < G; ++g) {
+        std::vector<int> p(perms + g * N, perms + (g + 1) * N);
+        if (std::find(sp.begin(), sp.end(), p) == sp.end()) sp.push_back(std::move(p));
+    }
+    if (min_perms > 0 && (N < 24 || sp.size() < min_perms)) return c;
+    int L = 0;
+    const std::vector<int> block = block_system(sp, N, L);
+    if (block.empty()) return c;
+    c.on = true;
+    c.L = L;
+    c.m = N / L;
+    const int bpw = (N + 7) / 8;
+    std::vector<int> key_bit(N, 0);
+    std::vector<std::vector<int>> sites(c.m);
+    for (int s = 0; s < N; ++s) sites[block[s]].push_back(s);
+    for (int j = 0; j < c.m; ++j)
+        for (int t = 0; t < L; ++t) key_bit[sites[j][t]] = N - (j + 1) * L + t;
+    c.to_key.assign(static_cast<std::size_t>(bpw) * 256, 0ULL);
+    for (int b = 0; b < bpw; ++b)
+        for (int v = 0; v < 256; ++v) {
+            u64 out = 0;
+            for (int t = 0; t < 8 && 8 * b + t < N; ++t)
+                if ((v >> t) & 1) out |= 1ULL << key_bit[8 * b + t];
+            c.to_key[b * 256 + v] = out;
+        }
+    const std::size_t P = std::size_t{1} << L;
+    const u32 lmask = (1u << L) - 1u;
+    std::vector<int> src_block(G), pos_in_block(N, -1);
+    std::vector<std::vector<u32>> e(G, std::vector<u32>(L, 0u));
+    std::vector<u32> fl(G, 0u);
+    for (int j = 0; j < c.m; ++j)
+        for (int t = 0; t < L; ++t) pos_in_block[sites[j][t]] = t;
+    for (int g = 0; g < G; ++g) {
+        const int32_t* p = perms + g * N;
+        src_block[g] = block[p[sites[0][0]]];
+        for (int t = 0; t < L; ++t) {
+            const int i = sites[0][t];
+            e[g][pos_in_block[p[i]]] = 1u << t;
+            if (flips && ((flips[g] >> i) & 1ULL)) fl[g] |= 1u << t;
+        }
+    }
+    const std::size_t M = static_cast<std::size_t>(c.m) * P;
+    c.lead.assign(M, 0xFFFFu);
+    std::vector<u32> img(P), count(M, 0);
+    auto images = [&](int g) {
+        img[0] = 0;
+        for (std::size_t x = 1; x < P; ++x) img[x] = img[x & (x - 1)] | e[g][__builtin_ctzll(x)];
+        for (std::size_t x = 0; x < P; ++x) img[x] = (img[x] ^ fl[g]) & lmask;
+    };
+    for (int g = 0; g < G; ++g) {
+        images(g);
+        u16* row = c.lead.data() + static_cast<std::size_t>(src_block[g]) * P;
+        for (std::size_t x = 0; x < P; ++x)
+            if (img[x] < row[x]) row[x] = static_cast<u16>(img[x]);
+    }
+    for (int g = 0; g < G; ++g) {
+        images(g);
+        const std::size_t base = static_cast<std::size_t>(src_block[g]) * P;
+        for (std::size_t x = 0; x < P; ++x) count[base + x] += c.lead[base + x] == img[x] ? 1u : 0u;
+    }
+    c.cand_off.assign(M + 1, 0);
+    for (std::size_t i = 0; i < M; ++i) c.cand_off[i + 1] = c.cand_off[i] + count[i];
+    c.cand.assign(c.cand_off[M], 0);
+    std::vector<u32> fill(c.cand_off.begin(), c.cand_off.end() - 1);
+    for (int g = 0; g < G; ++g) {
+        images(g);
+        const std::size_t base = static_cast<std::size_t>(src_block[g]) * P;
+        for (std::size_t x = 0; x < P; ++x)
+            if (c.lead[base + x] == img[x]) c.cand[fill[base + x]++] = static_cast<u16>(g);
+    }
+    return c;
+}
+
+// Pascal triangle C(n, k), n, k <= 64, row-major 65 x 65.
+std::vector<u64> pascal() {
+    std::vector<u64> c(65 * 65, 0ULL);
+    for (int n = 0; n <= 64; ++n) {
+        c[n * 65] = 1;
+        for (int k = 1; k <= n; ++k) c[n * 65 + k] = c[(n - 1) * 65 + k - 1] + (k <= n - 1 ? c[(n - 1) * 65 + k] : 0);
+    }
+    return c;
+}
+
+// rank_lut[(b (N+1) + below) 256 + v]: the share of byte b (value v, `below` set bits under it) of
+// the colex rank, sum over its set bits q (the i-th, 1-based) of C(8b + q, below + i).
+std::vector<u64> build_rank_lut(int N) {
+    const auto C = pascal();
+    const int bpw = (N + 7) / 8;
+    std::vector<u64> lut(static_cast<std::size_t>(bpw) * (N + 1) * 256, 0ULL);
+    for (int b = 0; b < bpw; ++b)
+        for (int below = 0; below <= N; ++below)
+            for (int v = 0; v < 256; ++v) {
+                u64 r = 0;
+                int i = 0;
+                for (int q = 0; q < 8 && 8 * b + q < N; ++q)
+                    if ((v >> q) & 1) {
+                        ++i;
+                        const int n = 8 * b + q, k = below + i;
+                        if (k <= 64 && n <= 64) r += C[n * 65 + k];
+                    }
+                lut[(static_cast<std::size_t>(b) * (N + 1) + below) * 256 + v] = r;
+            }
+    return lut;
+}
+
+// -------------------------------------------------------------------------------------------
+// Device enumeration.
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ u64 unrank_dev(u64 rank, int n, int k, const u64* C) {
+    u64 s = 0;
+    for (int i = k - 1; i >= 0; --i) {
+        int p = i;
+        while (p + 1 < n && __ldg(C + (p + 1) * 65 + (i + 1)) <= rank) ++p;
+        s |= 1ULL << p;
+        rank -= __ldg(C + p * 65 + (i + 1));
+    }
+    return s;
+}
+
+__device__ __forceinline__ u64 gosper_next(u64 v) {
+    const u64 c = v & (~v + 1ULL);
+    const u64 r = v + c;
+    return (((r ^ v) >> 2) >> (__ffsll(static_cast<long long>(c)) - 1)) | r;
+}
+
+// visit_state + projected norm (orbit_table.h:93-99, 147-171; group_sector.cpp:183-186): 0 when s is
+// not a kept representative, else 1/norm.
+__device__ __forceinline__ double visit_inv_norm(const DSector& S, const u64* to_key, u64 s) {
+    double sre = 0.0, sim = 0.0;
+    int cnt = 0;
+    if (S.slc.on) {
+        const u64 k = key_of(to_key, S.bpw, s);
+        // least leading block over the blocks vs the state's own (visit_state's early exit)
+        u32 least = 0xFFFFFFFFu;
+        for (int j = 0; j < S.slc.m; ++j) {
+            const u32 v = __ldg(S.slc.lead + ((static_cast<u32>(j) << S.slc.L) + pattern_of(k, j, S.N, S.slc.L)));
+            least = v < least ? v : least;
+        }
+        if (least < pattern_of(k, 0, S.N, S.slc.L)) return 0.0;
+        bool rep = true;
+        for_each_candidate(S, k, [&](int g) {
+            if (!rep) return;
+            const u64 ik = key_of(to_key, S.bpw, apply_elem(S, s, g));
+            if (ik < k) {
+                rep = false;
+            } else if (ik == k) {
+                const double2 c = __ldg(S.chars + g);
+                sre = __dadd_rn(sre, c.x);
+                sim = __dadd_rn(sim, c.y);
+                ++cnt;
+            }
+        });
+        if (!rep) return 0.0;
+    } else {
+        for (int g = 0; g < S.G; ++g) {
+            const u64 img = apply_elem(S, s, g);
+            if (img < s) return 0.0;
+            if (img == s) {
+                const double2 c = __ldg(S.chars + g);
+                sre = __dadd_rn(sre, c.x);
+                sim = __dadd_rn(sim, c.y);
+                ++cnt;
+            }
+        }
+    }
+    double nsq = 1.0;
+    if (cnt != 1) {
+        // |sum|^2 as std::norm takes it (|z| squared); exact for a real sum
+        const double a = (sim == 0.0) ? fabs(sre) : hypot(sre, sim);
+        nsq = __ddiv_rn(__dmul_rn(a, a), static_cast<double>(cnt));
+    }
+    return nsq <= 1e-12 ? 0.0 : __ddiv_rn(1.0, __dsqrt_rn(nsq));
+}
+
+__global__ void enum_kernel(DSector S, u64 total, u64 chunk, u64 n_chunks, const u64* C, u64* counts,
+                            const u64* offsets, u64* out_reps, double* out_inv) {
+    extern __shared__ u64 s_key[];
+    if (S.slc.on)
+        for (int i = threadIdx.x; i < S.bpw * 256; i += blockDim.x) s_key[i] = S.slc.to_key[i];
+    __syncthreads();
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 c = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; c < n_chunks; c += stride) {
+        const u64 begin = c * chunk;
+        const u64 end = begin + chunk < total ? begin + chunk : total;
+        u64 s = unrank_dev(begin, S.N, S.n_up, C);
+        u64 cnt = 0;
+        const u64 off = offsets ? offsets[c] : 0;
+        for (u64 i = begin; i < end; ++i) {
+            const double inv = visit_inv_norm(S, s_key, s);
+            if (inv != 0.0) {
+                if (offsets) {
+                    out_reps[off + cnt] = s;
+                    out_inv[off + cnt] = inv;
+                }
+                ++cnt;
+            }
+            if (i + 1 < end) s = gosper_next(s);
+        }
+        if (!offsets) counts[c] = cnt;
+    }
+}
+
+__global__ void rank_table_kernel(DSector S, std::int32_t* table) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= S.dim) return;
+    table[rank_of(S, S.reps[i])] = static_cast<std::int32_t>(i);
+}
+
+__global__ void bucket_kernel(const u64* reps, u64 dim, u64 base, int shift, u64 nb, u32* off) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= dim) return;
+    const u64 b = (reps[i] - base) >> shift;
+    const u64 from = i == 0 ? 0 : ((reps[i - 1] - base) >> shift) + 1;
+    for (u64 c = from; c <= b; ++c) off[c] = static_cast<u32>(i);
+    if (i == dim - 1)
+        for (u64 c = b + 1; c <= nb; ++c) off[c] = static_cast<u32>(dim);
+}
+
+__global__ void index_proj_kernel(DSector S, const u64* states, u64 n, long long* idx, double2* proj) {
+    extern __shared__ u64 s_key[];
+    if (S.slc.on)
+        for (int i = threadIdx.x; i < S.bpw * 256; i += blockDim.x) s_key[i] = S.slc.to_key[i];
+    __syncthreads();
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double pr = 0.0, pi = 0.0;
+    idx[i] = index_and_projection(S, s_key, states[i], pr, pi);
+    proj[i] = make_double2(pr, pi);
+}
+
+int sm_count() {
+    static int n = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    });
+    return n;
+}
+
+void upload_group(qb_sector& s, const qb_sector_desc& d) {
+    const int G = d.group_size, N = d.n_sites;
+    s.lut.upload(build_lut(d.perms, G, N));
+    std::vector<u64> fl(G, 0ULL);
+    if (d.flips) std::copy(d.flips, d.flips + G, fl.begin());
+    s.flips.upload(fl);
+    std::vector<double2> ch(G);
+    for (int g = 0; g < G; ++g) ch[g] = make_double2(d.chars[2 * g], d.chars[2 * g + 1]);
+    s.chars.upload(ch);
+    s.chars_host.assign(d.chars, d.chars + 2 * G);
+    const SlcHost slc = build_slc(d.perms, reinterpret_cast<const u64*>(d.flips), G, N, d.sublattice_mode);
+    s.slc_on = slc.on ? 1 : 0;
+    if (slc.on) {
+        s.slc_L = slc.L;
+        s.slc_m = slc.m;
+        s.to_key.upload(slc.to_key);
+        s.lead.upload(slc.lead);
+        s.cand_off.upload(slc.cand_off);
+        s.cand.upload(slc.cand);
+    }
+    s.rank_lut.upload(build_rank_lut(N));
+}
+
+void validate(const qb_sector_desc* d) {
+    if (!d) throw Error(QB_EINVAL, "null sector description");
+    if (d->n_sites < 1 || d->n_sites > 64) throw Error(QB_EINVAL, "n_sites must be in [1, 64]");
+    if (d->n_up < 0 || d->n_up > d->n_sites) throw Error(QB_EINVAL, "n_up must be in [0, n_sites]");
+    if (d->group_size < 1 || d->group_size > 65535) throw Error(QB_EINVAL, "group_size must be in [1, 65535]");
+    if (!d->perms || !d->chars) throw Error(QB_EINVAL, "perms and chars are required");
+    for (int g = 0; g < d->group_size; ++g) {
+        std::vector<int> seen(d->n_sites, 0);
+        for (int i = 0; i < d->n_sites; ++i) {
+            const int p = d->perms[g * d->n_sites + i];
+            if (p < 0 || p >= d->n_sites || seen[p]++) throw Error(QB_EINVAL, "element is not a permutation");
+        }
+        if (d->flips) {
+            const u64 allm = d->n_sites == 64 ? ~0ULL : ((1ULL << d->n_sites) - 1ULL);
+            const u64 f = d->flips[g];
+            if (f & ~allm) throw Error(QB_EINVAL, "flip mask beyond n_sites");
+            // an element must keep the popcount of every state of the sector
+            if (f != 0 && !(f == allm && 2 * d->n_up == d->n_sites))
+                throw Error(QB_EINVAL, "a flip element must be the global spin flip at half filling");
+        }
+    }
+}
+
+// The lookup structure: a rank table indexed by the combinadic rank, or state buckets over the
+// ascending representatives (include/ed/basis/rep_sector.h:85-117, 275-307).
+void build_lookup(qb_sector& s, int want) {
+    if (s.dim == 0) {
+        s.lookup = 0;
+        return;
+    }
+    const auto C = pascal();
+    const u64 ranks = C[s.N * 65 + s.n_up];
+    std::size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const double table_bytes = 4.0 * static_cast<double>(ranks);
+    // buckets: ~one per representative, at most 2^24
+    std::vector<u64> ends(2);
+    cuda_check(cudaMemcpy(&ends[0], s.reps.p, 8, cudaMemcpyDeviceToHost), "read reps");
+    cuda_check(cudaMemcpy(&ends[1], s.reps.p + (s.dim - 1), 8, cudaMemcpyDeviceToHost), "read reps");
+    int mode = want;
+    if (mode == QB_LOOKUP_AUTO) {
+        // the buckets while the representatives and their offsets stay cache-sized, else a rank table
+        // when it fits well inside free memory
+        const double bucket_bytes = 8.0 * static_cast<double>(s.dim) * 2.0;
+        if (bucket_bytes <= 96.0 * (1 << 20))
+            mode = QB_LOOKUP_BUCKETS;
+        else
+            mode = (table_bytes < 0.4 * static_cast<double>(free_b) && s.dim < (1ULL << 31)) ? QB_LOOKUP_RANK
+                                                                                            : QB_LOOKUP_BUCKETS;
+    }
+    if (mode == QB_LOOKUP_RANK) {
+        if (s.dim >= (1ULL << 31)) throw Error(QB_EUNSUPPORTED, "rank table: more than 2^31 representatives");
+        s.rank_table.alloc(static_cast<std::size_t>(ranks));
+        cuda_check(cudaMemset(s.rank_table.p, 0xFF, ranks * 4), "rank table clear");
+        s.lookup = 1;
+        const DSector v = s.view();
+        rank_table_kernel<<<static_cast<unsigned>((s.dim + 255) / 256), 256>>>(v, s.rank_table.p);
+        cuda_check(cudaGetLastError(), "rank table");
+    } else {
+        const u64 base = ends[0], span = ends[1] - ends[0] + 1;
+        int bits = 0;
+        while ((1ULL << bits) < s.dim && bits < 24) ++bits;
+        int key_bits = 0;
+        while (key_bits < 63 && (1ULL << key_bits) < span) ++key_bits;
+        const int shift = std::max(0, key_bits - bits);
+        const u64 nb = ((span - 1) >> shift) + 1;
+        s.bucket_off.alloc(static_cast<std::size_t>(nb + 1));
+        s.bucket_base = base;
+        s.bucket_shift = shift;
+        s.bucket_count = nb;
+        s.lookup = 2;
+        bucket_kernel<<<static_cast<unsigned>((s.dim + 255) / 256), 256>>>(s.reps.p, s.dim, base, shift, nb,
+                                                                              s.bucket_off.p);
+        cuda_check(cudaGetLastError(), "buckets");
+    }
+    cuda_check(cudaDeviceSynchronize(), "lookup build");
+}
+
+}  // namespace
+}  // namespace qb
+
+qb::DSector qb_sector::view() const {
+    qb::DSector v;
+    v.N = N;
+    v.n_up = n_up;
+    v.G = G;
+    v.bpw = bpw;
+    v.dim = dim;
+    v.reps = reps.p;
+    v.inv_norms = inv_norms.p;
+    v.lut = lut.p;
+    v.flips = flips.p;
+    v.chars = chars.p;
+    v.slc.on = slc_on;
+    v.slc.L = slc_L;
+    v.slc.m = slc_m;
+    v.slc.to_key = to_key.p;
+    v.slc.lead = lead.p;
+    v.slc.cand_off = cand_off.p;
+    v.slc.cand = cand.p;
+    v.lookup = lookup;
+    v.rank_table = rank_table.p;
+    v.rank_lut = rank_lut.p;
+    v.bucket_off = bucket_off.p;
+    v.bucket_base = bucket_base;
+    v.bucket_count = bucket_count;
+    v.bucket_shift = bucket_shift;
+    return v;
+}
+
+std::uint64_t qb_sector::device_bytes() const {
+    return reps.bytes() + inv_norms.bytes() + lut.bytes() + flips.bytes() + chars.bytes() + to_key.bytes() +
+           lead.bytes() + cand.bytes() + cand_off.bytes() + rank_table.bytes() + rank_lut.bytes() + bucket_off.bytes();
+}
+
+extern "C" {
+
+const char* qb_last_error(void) { return qb::g_last_error.c_str(); }
+
+int qb_device_count(int* count) {
+    return qb::guarded([&] {
+        int n = 0;
+        const cudaError_t e = cudaGetDeviceCount(&n);
+        *count = e == cudaSuccess ? n : 0;
+        if (e != cudaSuccess) (void)cudaGetLastError();
+    });
+}
+
+int qb_sector_create(const qb_sector_desc* d, qb_sector** out) {
+    return qb::guarded([&] {
+        using namespace qb;
+        validate(d);
+        auto s = std::make_unique<qb_sector>();
+        s->N = d->n_sites;
+        s->n_up = d->n_up;
+        s->G = d->group_size;
+        s->bpw = (d->n_sites + 7) / 8;
+        upload_group(*s, *d);
+        const auto Ch = pascal();
+        const u64 total = Ch[s->N * 65 + s->n_up];
+        DevBuf<u64> C;
+        C.upload(Ch);
+        // chunks of consecutive ranks: enough for every SM to stay busy, at least 64 states each
+        const u64 want_chunks = static_cast<u64>(sm_count()) * 2048 * 8;
+        u64 chunk = std::max<u64>(64, (total + want_chunks - 1) / want_chunks);
+        const u64 n_chunks = (total + chunk - 1) / chunk;
+        DevBuf<u64> counts(n_chunks), offsets(n_chunks + 1);
+        DSector v = s->view();
+        const std::size_t smem = s->slc_on ? static_cast<std::size_t>(s->bpw) * 256 * 8 : 0;
+        const unsigned threads = 256;
+        const unsigned blocks =
+            static_cast<unsigned>(std::min<u64>((n_chunks + threads - 1) / threads, static_cast<u64>(sm_count()) * 16));
+        enum_kernel<<<blocks, threads, smem>>>(v, total, chunk, n_chunks, C.p, counts.p, nullptr, nullptr, nullptr);
+        cuda_check(cudaGetLastError(), "enumeration (count)");
+        std::size_t tmp_bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, counts.p, offsets.p, static_cast<int>(n_chunks) + 0);
+        DevBuf<unsigned char> tmp(std::max<std::size_t>(tmp_bytes, 1));
+        cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, counts.p, offsets.p, static_cast<int>(n_chunks));
+        cuda_check(cudaGetLastError(), "enumeration (scan)");
+        u64 last_off = 0, last_cnt = 0;
+        cuda_check(cudaMemcpy(&last_off, offsets.p + (n_chunks - 1), 8, cudaMemcpyDeviceToHost), "scan read");
+        cuda_check(cudaMemcpy(&last_cnt, counts.p + (n_chunks - 1), 8, cudaMemcpyDeviceToHost), "scan read");
+        s->dim = last_off + last_cnt;
+        s->reps.alloc(s->dim);
+        s->inv_norms.alloc(s->dim);
+        if (s->dim > 0) {
+            enum_kernel<<<blocks, threads, smem>>>(v, total, chunk, n_chunks, C.p, counts.p, offsets.p, s->reps.p,
+                                                   s->inv_norms.p);
+            cuda_check(cudaGetLastError(), "enumeration (write)");
+        }
+        cuda_check(cudaDeviceSynchronize(), "enumeration");
+        build_lookup(*s, d->lookup);
+        *out = s.release();
+    });
+}
+
+int qb_sector_create_from_reps(const qb_sector_desc* d, const uint64_t* reps, const double* inv_norms, uint64_t dim,
+                               qb_sector** out) {
+    return qb::guarded([&] {
+        using namespace qb;
+        validate(d);
+        for (uint64_t i = 1; i < dim; ++i)
+            if (reps[i] <= reps[i - 1]) throw Error(QB_EINVAL, "representatives must ascend");
+        auto s = std::make_unique<qb_sector>();
+        s->N = d->n_sites;
+        s->n_up = d->n_up;
+        s->G = d->group_size;
+        s->bpw = (d->n_sites + 7) / 8;
+        upload_group(*s, *d);
+        s->dim = dim;
+        s->reps.upload(reinterpret_cast<const u64*>(reps), dim);
+        s->inv_norms.upload(inv_norms, dim);
+        build_lookup(*s, d->lookup);
+        *out = s.release();
+    });
+}
+
+int qb_sector_destroy(qb_sector* s) {
+    return qb::guarded([&] { delete s; });
+}
+
+uint64_t qb_sector_dim(const qb_sector* s) { return s ? s->dim : 0; }
+
+int qb_sector_download(const qb_sector* s, uint64_t* reps, double* inv_norms) {
+    return qb::guarded([&] {
+        if (!s) throw qb::Error(QB_EINVAL, "null sector");
+        if (reps && s->dim)
+            qb::cuda_check(cudaMemcpy(reps, s->reps.p, s->dim * 8, cudaMemcpyDeviceToHost), "download reps");
+        if (inv_norms && s->dim)
+            qb::cuda_check(cudaMemcpy(inv_norms, s->inv_norms.p, s->dim * 8, cudaMemcpyDeviceToHost), "download");
+    });
+}
+
+int qb_sector_info(const qb_sector* s, uint64_t* device_bytes, int* slc_L, int* slc_m, int* lookup_kind) {
+    return qb::guarded([&] {
+        if (!s) throw qb::Error(QB_EINVAL, "null sector");
+        if (device_bytes) *device_bytes = s->device_bytes();
+        if (slc_L) *slc_L = s->slc_on ? s->slc_L : 0;
+        if (slc_m) *slc_m = s->slc_on ? s->slc_m : 0;
+        if (lookup_kind) *lookup_kind = s->lookup;
+    });
+}
+
+int qb_index_and_projection(const qb_sector* s, const uint64_t* states, uint64_t n, int64_t* index, double* proj) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!s) throw Error(QB_EINVAL, "null sector");
+        if (n == 0) return;
+        DevBuf<u64> d_states;
+        d_states.upload(reinterpret_cast<const u64*>(states), n);
+        DevBuf<long long> d_idx(n);
+        DevBuf<double2> d_proj(n);
+        const std::size_t smem = s->slc_on ? static_cast<std::size_t>(s->bpw) * 256 * 8 : 0;
+        index_proj_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, smem>>>(s->view(), d_states.p, n, d_idx.p,
+                                                                                    d_proj.p);
+        cuda_check(cudaGetLastError(), "index_and_projection");
+        cuda_check(cudaMemcpy(index, d_idx.p, n * 8, cudaMemcpyDeviceToHost), "download");
+        cuda_check(cudaMemcpy(proj, d_proj.p, n * 16, cudaMemcpyDeviceToHost), "download");
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+"""Host handles over the C-ABI: device sectors and programs, the matvec, and the Krylov drivers.
+
+Every call goes to libqed_b200.so (CUDA, sm_100a). Device vectors are torch tensors (complex128 for
+QB_C128, complex64 for QB_C64) on the current CUDA device; host vectors are numpy complex128 arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .lattice import SectorSpec
+from .operators import Program as HostProgram
+
+DTYPES = {"c128": _lib.QB_C128, "c64": _lib.QB_C64, "fp64": _lib.QB_C128, "fp32": _lib.QB_C64}
+
+
+def _dt(dtype) -> int:
+    if isinstance(dtype, int):
+        return dtype
+    return DTYPES[dtype]
+
+
+def device_count() -> int:
+    n = C.c_int()
+    check(lib().qb_device_count(C.byref(n)))
+    return n.value
+
+
+class Sector:
+    """A symmetry sector resident on the device (its representatives enumerated there)."""
+
+    def __init__(self, spec: SectorSpec, sublattice_mode: int = -1, lookup: int = _lib.QB_LOOKUP_AUTO,
+                 reps=None, inv_norms=None):
+        self.spec = spec
+        self._perms = np.ascontiguousarray(spec.perms, np.int32)
+        chars = np.asarray(spec.chars, np.complex128)
+        self._chars = np.ascontiguousarray(np.stack([chars.real, chars.imag], 1).reshape(-1))
+        self._flips = None if spec.flips is None else np.ascontiguousarray(spec.flips, np.uint64)
+        d = _lib.SectorDesc(spec.n_sites, spec.n_up, self._perms.shape[0], self._perms.ctypes.data,
+                            None if self._flips is None else self._flips.ctypes.data, self._chars.ctypes.data,
+                            sublattice_mode, lookup)
+        h = C.c_void_p()
+        if reps is None:
+            check(lib().qb_sector_create(C.byref(d), C.byref(h)))
+        else:
+            r = np.ascontiguousarray(reps, np.uint64)
+            w = np.ascontiguousarray(inv_norms, np.float64)
+            check(lib().qb_sector_create_from_reps(C.byref(d), r.ctypes.data, w.ctypes.data, len(r), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().qb_sector_destroy(self.h)
+            self.h = C.c_void_p()
+
+    __del__ = close
+
+    @property
+    def dim(self) -> int:
+        return int(lib().qb_sector_dim(self.h))
+
+    def reps(self):
+        n = self.dim
+        reps = np.zeros(n, np.uint64)
+        inv = np.zeros(n, np.float64)
+        if n:
+            check(lib().qb_sector_download(self.h, reps.ctypes.data, inv.ctypes.data))
+        return reps, inv
+
+    def info(self) -> dict:
+        b, L, m, k = C.c_uint64(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().qb_sector_info(self.h, C.byref(b), C.byref(L), C.byref(m), C.byref(k)))
+        return dict(device_bytes=b.value, slc_L=L.value, slc_m=m.value,
+                    lookup={0: "none", 1: "rank", 2: "buckets"}[k.value])
+
+    def index_and_projection(self, states):
+        st = np.ascontiguousarray(states, np.uint64)
+        idx = np.zeros(len(st), np.int64)
+        proj = np.zeros(2 * len(st), np.float64)
+        check(lib().qb_index_and_projection(self.h, st.ctypes.data, len(st), idx.ctypes.data, proj.ctypes.data))
+        return idx, proj.view(np.complex128)
+
+
+class Program:
+    """A row program resident on the device."""
+
+    def __init__(self, prog: HostProgram):
+        self.host = prog
+        self._a = [
+            np.ascontiguousarray(prog.group_flip, np.uint64),
+            np.ascontiguousarray(prog.group_setbits, np.int32),
+            np.ascontiguousarray(prog.group_vbegin, np.uint32),
+            np.ascontiguousarray(prog.vsub_val, np.uint64),
+            np.ascontiguousarray(prog.vsub_tbegin, np.uint32),
+            np.ascontiguousarray(prog.term_sign, np.uint64),
+            np.ascontiguousarray(np.asarray(prog.term_coeff, np.complex128)).view(np.float64),
+        ]
+        a = self._a
+        d = _lib.ProgramDesc(len(a[0]), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, len(a[3]),
+                             a[3].ctypes.data, a[4].ctypes.data, len(a[5]), a[5].ctypes.data, a[6].ctypes.data)
+        h = C.c_void_p()
+        check(lib().qb_program_create(C.byref(d), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().qb_program_destroy(self.h)
+            self.h = C.c_void_p()
+
+    __del__ = close
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return getattr(stream, "cuda_stream", stream)
+
+
+def matvec(row: Sector, col: Sector, prog: Program, xs, outs, dtype="c128", stream=None):
+    """outs[i] = O xs[i] for device tensors (lists of equal length)."""
+    k = len(xs)
+    ins = (C.c_void_p * k)(*[x.data_ptr() for x in xs])
+    ous = (C.c_void_p * k)(*[y.data_ptr() for y in outs])
+    check(lib().qb_matvec(row.h, col.h, prog.h, ins, ous, k, _dt(dtype), _stream_ptr(stream)))
+
+
+def matvec_block(row: Sector, col: Sector, prog: Program, x, out, k: int, dtype="c128", stream=None):
+    """out = O x on k vectors interleaved by row (device tensors of row.dim * k elements)."""
+    check(lib().qb_matvec_block(row.h, col.h, prog.h, x.data_ptr(), out.data_ptr(), k, _dt(dtype),
+                                _stream_ptr(stream)))
+
+
+def matvec_host(row: Sector, col: Sector, prog: Program, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.complex128)
+    y = np.zeros(row.dim, np.complex128)
+    check(lib().qb_matvec_host(row.h, col.h, prog.h, x.ctypes.data, y.ctypes.data))
+    return y
+
+
+def lanczos(sec: Sector, prog: Program, v0: np.ndarray, max_iter: int, reorth: int = _lib.QB_REORTH_NONE,
+            breakdown_tol: float = 1e-300, dtype="c128"):
+    v0 = np.ascontiguousarray(v0, np.complex128)
+    a = np.zeros(max_iter)
+    b = np.zeros(max_iter + 1)
+    it = C.c_int()
+    check(lib().qb_lanczos(sec.h, prog.h, v0.ctypes.data, max_iter, reorth, breakdown_tol, _dt(dtype),
+                           a.ctypes.data, b.ctypes.data, C.byref(it)))
+    m = it.value
+    return a[:m].copy(), b[: m + 1].copy()
+
+
+def eigs_lowest(sec: Sector, prog: Program, max_iter: int = 0, dtype="c128", refine: bool = True) -> dict:
+    e, it, cv, mv = C.c_double(), C.c_int(), C.c_int(), C.c_int()
+    check(lib().qb_eigs_lowest(sec.h, prog.h, max_iter, _dt(dtype), 1 if refine else 0, C.byref(e), C.byref(it),
+                               C.byref(cv), C.byref(mv)))
+    return dict(e0=e.value, iters=it.value, converged=bool(cv.value), matvecs=mv.value)
+
+
+def ftlm(sec: Sector, prog: Program, samples: int, depth: int, seed: int, betas, dtype="c128") -> dict:
+    betas = np.ascontiguousarray(betas, np.float64)
+    nb = len(betas)
+    lnZ, E, V = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+    em = C.c_double()
+    check(lib().qb_ftlm(sec.h, prog.h, samples, depth, seed, betas.ctypes.data, nb, _dt(dtype), lnZ.ctypes.data,
+                        E.ctypes.data, V.ctypes.data, C.byref(em)))
+    return dict(lnZ=lnZ, E=E, V=V, e_min=em.value)
+
+
+def cf(sec: Sector, prog: Program, phi: np.ndarray, depth: int, omega, eta: float, shift: float = float("nan"),
+       tolerance: float = 1e-12):
+    phi = np.ascontiguousarray(phi, np.complex128)
+    omega = np.ascontiguousarray(omega, np.float64)
+    S = np.zeros(len(omega))
+    sh = C.c_double()
+    check(lib().qb_cf(sec.h, prog.h, phi.ctypes.data, depth, omega.ctypes.data, len(omega), eta, shift, tolerance,
+                      S.ctypes.data, C.byref(sh)))
+    return S, sh.value

@@ -1,0 +1,43 @@
+"""The C-ABI library loads without a GPU and exports every entry point include/qed_b200.h declares."""
+import ctypes
+import os
+import re
+import subprocess
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "qed_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(qb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    from qed_spin_b200 import build, _lib
+    path = build.build()
+    lib = ctypes.CDLL(path)
+    names = declared()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(_lib.EXPORTS) == names
+    nm = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(rf"\bT {n}$", nm, flags=re.M), n
+
+
+def test_kernels_are_sm100a():
+    from qed_spin_b200 import build
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    """Without a CUDA device the library reports no devices; every compute entry point then fails."""
+    from qed_spin_b200 import device
+    import torch
+    if torch.cuda.is_available():
+        return
+    assert device.device_count() == 0

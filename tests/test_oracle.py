@@ -1,0 +1,146 @@
+"""The restated oracle pinned against the reference: its golden suite's recorded energies, a textbook
+ground-state energy, and outputs of the reference engine itself (tests/golden/fixtures.npz)."""
+import numpy as np
+import pytest
+
+from cases import CASES, NAMES
+from conftest import host_program
+from oracle import oracle as O
+from qed_spin_b200 import lattice as lat
+from qed_spin_b200 import operators as ops
+
+
+def _spec(name):
+    return dict((c[0], c[1]) for c in CASES)[name]
+
+
+def _prods(name):
+    return dict((c[0], c[2]) for c in CASES)[name]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_program_compile_matches_reference(fixtures, name):
+    """The host operator algebra compiles the reference's row program bit for bit."""
+    spec = _spec(name)
+    p = ops.row_program(ops.from_products(spec.n_sites, _prods(name)))
+    for k in ("group_flip", "group_setbits", "group_vbegin", "vsub_val", "vsub_tbegin", "term_sign"):
+        ref = fixtures[f"{name}/prog/{k}"]
+        assert np.array_equal(np.asarray(getattr(p, k)).astype(ref.dtype), ref), k
+    assert np.array_equal(p.term_coeff.view(np.uint64), fixtures[f"{name}/prog/term_coeff"].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_sector_bit_exact(fixtures, name):
+    S = O.Sector(_spec(name))
+    reps, inv = S.reps()
+    assert np.array_equal(reps, fixtures[f"{name}/reps"])
+    assert np.array_equal(inv.view(np.uint64), fixtures[f"{name}/inv_norms"].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_gather_and_sparsity_bit_exact(fixtures, name):
+    S = O.Sector(_spec(name))
+    P = O.Program(host_program(fixtures, name))
+    y = S.gather(P, fixtures[f"{name}/x"])
+    assert np.array_equal(y.view(np.uint64), fixtures[f"{name}/y"].view(np.uint64))
+    rp, col, val = S.csr(P)
+    assert np.array_equal(rp, fixtures[f"{name}/csr_row_ptr"])
+    assert np.array_equal(col, fixtures[f"{name}/csr_col"])
+    np.testing.assert_allclose(val, fixtures[f"{name}/csr_val"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_lanczos_and_lowest(fixtures, name):
+    S = O.Sector(_spec(name))
+    P = O.Program(host_program(fixtures, name))
+    a, b = S.lanczos(P, fixtures[f"{name}/x"], 40)
+    ra, rb = fixtures[f"{name}/lz_alpha"], fixtures[f"{name}/lz_beta"]
+    assert len(a) == len(ra)
+    # the recurrence amplifies roundoff along the run: early steps agree to 1e-13, the tail to 1e-6
+    np.testing.assert_allclose(a[:10], ra[:10], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(b[:11], rb[:11], rtol=0, atol=1e-12)
+    e0, it, cv = S.scan_lowest(P)
+    re0, rit, rcv = fixtures[f"{name}/e0"]
+    assert cv and rcv
+    assert abs(e0 - re0) <= 1e-12 * abs(re0)
+    assert abs(it - rit) <= 1
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_ftlm_and_cf(fixtures, name):
+    S = O.Sector(_spec(name))
+    P = O.Program(host_program(fixtures, name))
+    betas = 1.0 / np.linspace(0.1, 4.0, 40)
+    f = S.ftlm(P, 8, 60, 20240601, betas)
+    for k in ("lnZ", "E", "V"):
+        ref = fixtures[f"{name}/ftlm_{k}"]
+        np.testing.assert_allclose(f[k], ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+    omega = np.linspace(-1.0, 6.0, 64)
+    Sw, sh = S.cf(P, fixtures[f"{name}/x"], 80, omega, 0.05)
+    ref = fixtures[f"{name}/cf_S"]
+    assert abs(sh - fixtures[f"{name}/cf_shift"][0]) <= 1e-9
+    np.testing.assert_allclose(Sw, ref, rtol=0, atol=1e-8 * np.abs(ref).max())
+
+
+def test_seed_streams(fixtures):
+    np.testing.assert_allclose(O.sample_vector(42, 3, 64), fixtures["sample_vector/42/3"], rtol=0, atol=1e-15)
+    assert np.array_equal(O.staged_seed(0x51ED0B70, 64), fixtures["staged_seed/0x51ED0B70"])
+
+
+def test_known_heisenberg_ring(golden):
+    spec = lat.chain_sector(12, 6, 0)
+    P = O.Program(ops.row_program(ops.from_products(12, ops.heisenberg_products(lat.chain_bonds(12)))))
+    e0, _, cv = O.Sector(spec).scan_lowest(P)
+    assert cv and abs(e0 - golden["known"]["heis12_k0_e0"]) < 1e-11
+
+
+def _sector_spectrum(spec, prog):
+    S = O.Sector(spec)
+    d = S.dim
+    if d == 0:
+        return np.zeros(0)
+    P = O.Program(prog)
+    H = np.zeros((d, d), complex)
+    for j in range(d):
+        e = np.zeros(d, complex)
+        e[j] = 1.0
+        H[:, j] = S.gather(P, e)
+    assert np.allclose(H, H.conj().T, atol=1e-12)
+    return np.linalg.eigvalsh(H)
+
+
+@pytest.mark.parametrize("model", ["chain4", "chain5_odd", "j1j2_chain12", "xy_chain10"])
+def test_golden_fixed_sz_spectra(golden, model):
+    """The lowest levels of a fixed-S^z space, reassembled from its momentum sectors, equal the energies the
+    reference recorded in its golden suite (tier exact, 1e-10)."""
+    g = golden["models"][model]
+    N = g["n_sites"]
+    prods = [(o, tuple(s), complex(c[0], c[1])) for o, s, c in g["products"]]
+    prog = ops.row_program(ops.from_products(N, prods))
+    for key, ref in g["records"].items():
+        n_up = int(key.split("sz=")[1].split("/")[0])
+        levels = np.sort(np.concatenate([_sector_spectrum(lat.chain_sector(N, n_up, k), prog) for k in range(N)]))
+        np.testing.assert_allclose(levels[: len(ref)], ref, rtol=0, atol=1e-10)
+
+
+def test_sublattice_engagement():
+    """The key order engages exactly where the reference's relaxed rule does (sublattice_code.h:23-34)."""
+    assert O.Sector(lat.chain_sector(20, 1, 0)).sublattice() is None
+    s24 = O.Sector(lat.chain_sector(24, 1, 0)).sublattice()
+    assert s24 is not None and (s24["L"], s24["m"]) == (12, 2)
+    spec = lat.chain_a1_flip_sector(32).with_n_up(1)
+    s32 = O.Sector(spec).sublattice()
+    assert s32 is not None and (s32["L"], s32["m"]) == (16, 2)
+    sq = O.Sector(lat.square_k0_sector(6, 6, 1)).sublattice()
+    assert sq is not None and (sq["L"], sq["m"]) == (6, 6)
+
+
+def test_tridiagonal_solver():
+    rng = np.random.default_rng(3)
+    for m in (1, 2, 5, 40, 120):
+        a = rng.normal(size=m)
+        b = np.concatenate([[0.0], np.abs(rng.normal(size=m))])
+        T = np.diag(a) + np.diag(b[1:m], 1) + np.diag(b[1:m], -1)
+        vals, vecs = O.tridiag_eig(a, b)
+        np.testing.assert_allclose(vals, np.linalg.eigvalsh(T), atol=1e-12 * max(1, np.abs(vals).max()))
+        np.testing.assert_allclose(T @ vecs, vecs * vals, atol=1e-10)
