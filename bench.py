@@ -205,8 +205,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36"], default=None,
+                    help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        profile_case(args)
+        return
 
     world, rank, local = dist_init() if args.impl == "b200" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                    int(os.environ.get("RANK", "0")), 0)
@@ -321,6 +326,39 @@ def main():
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
+
+
+def profile_case(args):
+    """The small profiling workloads of the ncu summaries under profiles/: the sector is built on the device,
+    then H is applied to one complex64 vector `warmup + steps` times."""
+    import torch
+
+    from qed_spin_b200 import build
+    from qed_spin_b200 import device as D
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    build.build()
+    if args.profile_case == "chain32":
+        spec, prog, _ = workload()
+    else:
+        Ly = 5 if args.profile_case == "sq30" else 6
+        nn, nnn = lat.square_j1j2_bonds(6, Ly)
+        spec = lat.square_k0_sector(6, Ly, 3 * Ly)
+        prog = ops.row_program(ops.from_products(6 * Ly, ops.heisenberg_products(nn, 1.0)
+                                                 + ops.heisenberg_products(nnn, 0.5)))
+    S = D.Sector(spec)
+    P = D.Program(prog)
+    x = torch.randn(S.dim, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(args.warmup):
+        D.matvec(S, S, P, [x], [y], dtype="c64")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        D.matvec(S, S, P, [x], [y], dtype="c64")
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": args.profile_case, "dim": S.dim, "ms_per_matvec": (time.perf_counter() - t)
+                      / args.steps * 1e3, "sector": S.info()}))
 
 
 def emitted_per_row(reps: np.ndarray, prog) -> float:

@@ -758,8 +758,7 @@ bool lowest_level(const std::vector<double>& alpha, const std::vector<double>& b
 }
 
 // ---------------------------------------------------------------------------------------------
-// Seeds (sample_seed.h:37-89; block_solve.cpp:268-277). The (re, im) draw order is the one
-// `Complex(nd(gen), nd(gen))` takes with this compiler, pinned against the reference by the tests.
+// Seeds (sample_seed.h:37-89; block_solve.cpp:268-277).
 // ---------------------------------------------------------------------------------------------
 std::mt19937 sample_engine(std::uint64_t base_seed, std::uint64_t sample) {
     std::uint64_t z = base_seed + 0x9E3779B97F4A7C15ULL * (sample + 1);
@@ -769,10 +768,16 @@ std::mt19937 sample_engine(std::uint64_t base_seed, std::uint64_t sample) {
     return std::mt19937(static_cast<std::mt19937::result_type>(z));
 }
 
+// The reference draws Complex(nd(gen), nd(gen)) (sample_seed.h:84-85, lanczos.h:70-77); GCC evaluates
+// those arguments right to left, so the imaginary part is the first draw (pinned by the seed tests).
 template <class Gen> Vec gaussian_draw(std::size_t n, Gen& gen) {
     std::normal_distribution<double> nd(0.0, 1.0);
     Vec v(n);
-    for (std::size_t i = 0; i < n; ++i) v[i] = Complex(nd(gen), nd(gen));
+    for (std::size_t i = 0; i < n; ++i) {
+        const double im = nd(gen);
+        const double re = nd(gen);
+        v[i] = Complex(re, im);
+    }
     return v;
 }
 

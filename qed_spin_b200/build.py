@@ -47,21 +47,26 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
         return OUT
     nvcc = _nvcc()
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    for src in sources():
+    from concurrent.futures import ThreadPoolExecutor
+
+    def compile_one(src):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         cmd = [nvcc, *ARCH, *FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
-        if ptxas_v or verbose:
-            sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    objs = []
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        for src, obj, r in ex.map(compile_one, sources()):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
+            if ptxas_v or verbose:
+                sys.stderr.write(r.stderr)
+            objs.append(obj)
     tmp = OUT + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

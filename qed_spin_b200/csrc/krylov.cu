@@ -222,6 +222,64 @@ template <class T> __global__ void rec_next(std::uint64_t n, int j, const double
     }
 }
 
+// ---- full reorthogonalisation (CGS2 with the DGKS gate, lanczos.h:428-451) against the kept basis ----
+constexpr double kDgksKappa = 0.7071067811865476;
+
+// slot[0] = ||w|| (deterministic grid reduction).
+__global__ void k_norm_to(std::uint64_t n, const double2* w, Scal S, double* slot, const int* flag) {
+    if (flag && *flag == 0) return;
+    __shared__ double sm[4 * 32];
+    double v[1] = {0.0};
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const double2 a = w[i];
+        v[0] += a.x * a.x + a.y * a.y;
+    }
+    block_reduce<1>(v, sm);
+    double tot[1];
+    if (last_block_total<1>(v, S.partials, S.counter, sm, tot)) *slot = sqrt(tot[0]);
+}
+
+// coeff[k] = -<V_k, w>, one block per basis vector.
+template <class T>
+__global__ void k_dot_many(std::uint64_t n, const T* const* basis, const double2* w, double2* coeff, const int* flag) {
+    if (flag && *flag == 0) return;
+    __shared__ double sm[4 * 32];
+    const T* v = basis[blockIdx.x];
+    double acc[2] = {0.0, 0.0};
+    for (std::uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double2 b = V<T>::ld(v, i);
+        const double2 y = w[i];
+        acc[0] += b.x * y.x + b.y * y.y;
+        acc[1] += b.x * y.y - b.y * y.x;
+    }
+    block_reduce<2>(acc, sm);
+    if (threadIdx.x == 0) coeff[blockIdx.x] = make_double2(-acc[0], -acc[1]);
+}
+
+// w += sum_k coeff[k] V_k, each element accumulated in k order.
+template <class T>
+__global__ void k_axpy_many(std::uint64_t n, int m, const T* const* basis, const double2* coeff, double2* w,
+                            const int* flag) {
+    if (flag && *flag == 0) return;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        double2 y = w[i];
+        for (int k = 0; k < m; ++k) {
+            const double2 c = coeff[k];
+            const double2 b = V<T>::ld(basis[k], i);
+            y.x += c.x * b.x - c.y * b.y;
+            y.y += c.x * b.y + c.y * b.x;
+        }
+        w[i] = y;
+    }
+}
+
+// The DGKS gate: a second pass only when the first removed more than 1 - kappa of the norm.
+__global__ void k_dgks_gate(const double* before, const double* after, int* flag) {
+    *flag = (*after < kDgksKappa * *before) ? 1 : 0;
+}
+
 // x += c v (a Ritz-vector accumulation, FP64 destination).
 template <class T> __global__ void k_axpy_into(std::uint64_t n, double c, const T* v, double2* x) {
     for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -626,9 +684,15 @@ bool lowest_level(const std::vector<double>& alpha, const std::vector<double>& b
 // Seeds: the block lanes' staged Gaussian start (block_solve.cpp:268-277) and the FTLM sample
 // vectors (sample_seed.h:37-89), drawn on the host exactly as the reference draws them.
 // -------------------------------------------------------------------------------------------
+// The reference draws each entry as Complex(nd(gen), nd(gen)); GCC evaluates those arguments right to
+// left, so the imaginary part is the first draw. Written out here so no compiler reorders it.
 template <class Gen> void gaussian_fill(std::vector<std::complex<double>>& v, Gen& gen) {
     std::normal_distribution<double> nd(0.0, 1.0);
-    for (auto& c : v) c = std::complex<double>(nd(gen), nd(gen));
+    for (auto& c : v) {
+        const double im = nd(gen);
+        const double re = nd(gen);
+        c = std::complex<double>(re, im);
+    }
 }
 
 std::vector<std::complex<double>> staged_seed(std::size_t n, std::uint64_t seed) {
@@ -660,7 +724,12 @@ struct Recurrence {
     DevBuf<unsigned char> vbuf[2];        // v_prev, v_curr (dtype)
     DevBuf<double> d_alpha, d_beta, d_ovl, d_partials;
     DevBuf<unsigned> d_counter;
-    std::vector<DevBuf<unsigned char>> basis;   // kept Lanczos vectors (optional)
+    DevBuf<unsigned char> basis_block;          // kept Lanczos vectors, back to back (optional)
+    std::vector<unsigned char*> basis;
+    DevBuf<void*> d_basis;                      // their device pointers (full reorthogonalisation)
+    DevBuf<double2> d_coeff;
+    DevBuf<double> d_norms;                     // [0] before, [1] after
+    DevBuf<int> d_flag;
     cudaEvent_t ev = nullptr;
     int cur = 1;   // vbuf[cur] = v_j, vbuf[cur ^ 1] = v_{j-1}
 
@@ -706,24 +775,66 @@ struct Recurrence {
     }
 
     void keep_current() {
-        DevBuf<unsigned char> b(n * esize());
-        cuda_check(cudaMemcpyAsync(b.p, vbuf[cur].p, n * esize(), cudaMemcpyDeviceToDevice, st), "basis copy");
-        basis.push_back(std::move(b));
+        if (basis_block.n == 0) basis_block.alloc(static_cast<std::size_t>(max_iter + 1) * n * esize());
+        if (basis.size() >= static_cast<std::size_t>(max_iter + 1)) throw Error(QB_EINVAL, "basis capacity exceeded");
+        unsigned char* b = basis_block.p + basis.size() * n * esize();
+        cuda_check(cudaMemcpyAsync(b, vbuf[cur].p, n * esize(), cudaMemcpyDeviceToDevice, st), "basis copy");
+        basis.push_back(b);
+    }
+
+    // CGS2 of w against the kept basis V_0..V_j, then beta_{j+1} = ||w|| (lanczos.h:428-451, 481-484).
+    void full_reorth(int j) {
+        const int m = static_cast<int>(basis.size());
+        if (m == 0) return;
+        if (d_basis.n < static_cast<std::size_t>(max_iter + 1)) {
+            d_basis.alloc(max_iter + 1);
+            d_coeff.alloc(max_iter + 1);
+            d_norms.alloc(2);
+            d_flag.alloc(1);
+        }
+        std::vector<void*> ptrs(m);
+        for (int k = 0; k < m; ++k) ptrs[k] = basis[k];
+        cuda_check(cudaMemcpyAsync(d_basis.p, ptrs.data(), m * sizeof(void*), cudaMemcpyHostToDevice, st), "basis ptrs");
+        cuda_check(cudaStreamSynchronize(st), "basis ptrs");
+        const int nb = red_blocks(n);
+        const int one = 1;
+        cuda_check(cudaMemcpyAsync(d_flag.p, &one, 4, cudaMemcpyHostToDevice, st), "flag");
+        for (int pass = 0; pass < 2; ++pass) {
+            const int* flag = pass == 0 ? nullptr : d_flag.p;
+            double* before = d_norms.p;
+            k_norm_to<<<nb, kThreads, 0, st>>>(n, w.p, scal(), before, flag);
+            if (dtype == QB_C64) {
+                k_dot_many<float2><<<m, kThreads, 0, st>>>(n, reinterpret_cast<const float2* const*>(d_basis.p), w.p, d_coeff.p, flag);
+                k_axpy_many<float2><<<nb, kThreads, 0, st>>>(n, m, reinterpret_cast<const float2* const*>(d_basis.p), d_coeff.p, w.p, flag);
+            } else {
+                k_dot_many<double2><<<m, kThreads, 0, st>>>(n, reinterpret_cast<const double2* const*>(d_basis.p), w.p, d_coeff.p, flag);
+                k_axpy_many<double2><<<nb, kThreads, 0, st>>>(n, m, reinterpret_cast<const double2* const*>(d_basis.p), d_coeff.p, w.p, flag);
+            }
+            k_norm_to<<<nb, kThreads, 0, st>>>(n, w.p, scal(), d_norms.p + 1, flag);
+            if (pass == 0) k_dgks_gate<<<1, 1, 0, st>>>(d_norms.p, d_norms.p + 1, d_flag.p);
+        }
+        k_norm_to<<<nb, kThreads, 0, st>>>(n, w.p, scal(), d_beta.p + j + 1, nullptr);
+        cuda_check(cudaGetLastError(), "full reorthogonalisation");
+        cuda_check(cudaStreamSynchronize(st), "full reorthogonalisation");
     }
 
     // Step j: w = H v_j, alpha_j, beta_{j+1}, v_{j+1}. Records the event after the scalars.
-    void step(int j, int local) {
+    // reorth: QB_REORTH_NONE, QB_REORTH_LOCAL, or QB_REORTH_FULL (against the kept basis)
+    void step(int j, int reorth) {
         const int nb = red_blocks(n);
         void* vc = vbuf[cur].p;
         void* vp = vbuf[cur ^ 1].p;
+        const int local = reorth == QB_REORTH_LOCAL;
         launch_walk_mixed(sec, sec, prog, vc, w.p, dtype, QB_C128, st);
         if (dtype == QB_C64) {
             rec_alpha<float2><<<nb, kThreads, 0, st>>>(n, j, w.p, static_cast<float2*>(vp), static_cast<float2*>(vc), scal());
             rec_beta<float2><<<nb, kThreads, 0, st>>>(n, j, local, w.p, static_cast<float2*>(vc), scal());
+            if (reorth == QB_REORTH_FULL) full_reorth(j);
             rec_next<float2><<<nb, kThreads, 0, st>>>(n, j, w.p, static_cast<float2*>(vc), static_cast<float2*>(vp), scal());
         } else {
             rec_alpha<double2><<<nb, kThreads, 0, st>>>(n, j, w.p, static_cast<double2*>(vp), static_cast<double2*>(vc), scal());
             rec_beta<double2><<<nb, kThreads, 0, st>>>(n, j, local, w.p, static_cast<double2*>(vc), scal());
+            if (reorth == QB_REORTH_FULL) full_reorth(j);
             rec_next<double2><<<nb, kThreads, 0, st>>>(n, j, w.p, static_cast<double2*>(vc), static_cast<double2*>(vp), scal());
         }
         cuda_check(cudaGetLastError(), "recurrence");
@@ -760,10 +871,11 @@ struct ScanOut {
     int matvecs = 0;
 };
 
-ScanOut run_scan(Recurrence& R, int max_iter, int local, bool gate, double breakdown_tol, bool keep) {
+ScanOut run_scan(Recurrence& R, int max_iter, int reorth, bool gate, double breakdown_tol, bool keep) {
     ScanOut o;
     o.beta.push_back(0.0);
     const int cap = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(max_iter), R.n));
+    if (reorth == QB_REORTH_FULL) keep = true;
     if (keep) R.keep_current();
     // pipelined: step j runs while the host tests step j - 1's prefix
     int launched = 0;
@@ -778,7 +890,7 @@ ScanOut run_scan(Recurrence& R, int max_iter, int local, bool gate, double break
         // no test between steps: launch every step, read the scalars once, cut at the first breakdown
         for (int j = 0; j < cap; ++j) {
             if (keep && j > 0) R.keep_current();
-            R.step(j, local);
+            R.step(j, reorth);
             ++o.matvecs;
         }
         std::vector<double> a(cap), b(cap + 1);
@@ -796,7 +908,7 @@ ScanOut run_scan(Recurrence& R, int max_iter, int local, bool gate, double break
     bool stop = false;
     for (int j = 0; j < cap && !stop; ++j) {
         if (launched == j) {
-            R.step(j, local);
+            R.step(j, reorth);
             ++launched;
             ++o.matvecs;
         }
@@ -808,7 +920,7 @@ ScanOut run_scan(Recurrence& R, int max_iter, int local, bool gate, double break
         // launch step j + 1 before testing step j (the device stays busy while the host tests)
         if (j + 1 < cap) {
             if (keep) R.keep_current();
-            R.step(j + 1, local);
+            R.step(j + 1, reorth);
             ++launched;
             ++o.matvecs;
         }
@@ -837,14 +949,14 @@ int qb_lanczos(const qb_sector* sec, const qb_program* prog, const double* v0_ho
     return qb::guarded([&] {
         using namespace qb;
         if (!sec || !prog || !v0_host || !alpha || !beta || !iters) throw Error(QB_EINVAL, "null argument");
-        if (reorth != QB_REORTH_NONE && reorth != QB_REORTH_LOCAL)
-            throw Error(QB_EUNSUPPORTED, "qb_lanczos: reorth must be QB_REORTH_NONE or QB_REORTH_LOCAL");
+        if (reorth != QB_REORTH_NONE && reorth != QB_REORTH_LOCAL && reorth != QB_REORTH_FULL)
+            throw Error(QB_EINVAL, "qb_lanczos: unknown reorthogonalisation policy");
         if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "bad dtype");
         *iters = 0;
         if (max_iter <= 0 || sec->dim == 0) return;
         Recurrence R(sec, prog, dtype, max_iter);
         R.start_from_host(reinterpret_cast<const std::complex<double>*>(v0_host));
-        const ScanOut o = run_scan(R, max_iter, reorth == QB_REORTH_LOCAL, false, breakdown_tol, false);
+        const ScanOut o = run_scan(R, max_iter, reorth, false, breakdown_tol, false);
         std::copy(o.alpha.begin(), o.alpha.end(), alpha);
         std::copy(o.beta.begin(), o.beta.end(), beta);
         *iters = static_cast<int>(o.alpha.size());
@@ -865,8 +977,8 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         if (nb == 0) return;
         const int budget = max_iter > 0 ? max_iter : 400;
         const int mi = static_cast<int>(std::min<std::uint64_t>(nb, static_cast<std::uint64_t>(budget)));
-        if (static_cast<std::uint64_t>(mi) >= nb)
-            throw Error(QB_EUNSUPPORTED, "qb_eigs_lowest: a block within the iteration budget takes the dense lane");
+        // a run that may span the whole block reorthogonalises fully (block_solve.cpp:544-548)
+        const int reorth = static_cast<std::uint64_t>(mi) >= nb ? QB_REORTH_FULL : QB_REORTH_NONE;
         const auto v0 = staged_seed(nb, 0x51ED0B70ULL);
         const bool mixed = dtype == QB_C64 && refine;
         // FP32 storage keeps its Krylov basis when it fits comfortably (the Ritz vector for the
@@ -877,7 +989,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         auto Rp = std::make_unique<Recurrence>(sec, prog, dtype, mi);
         Recurrence& R = *Rp;
         R.start_from_host(v0.data());
-        ScanOut o = run_scan(R, mi, 0, true, 1e-300, keep);
+        ScanOut o = run_scan(R, mi, reorth, true, 1e-300, keep);
         int total_mv = o.matvecs;
         if (iters) *iters = static_cast<int>(o.alpha.size());
         if (!mixed || !o.converged) {
@@ -897,7 +1009,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         DevBuf<double2> x(nb);
         cuda_check(cudaMemsetAsync(x.p, 0, nb * 16, R.st), "zero");
         if (keep) {
-            for (int j = 0; j < m; ++j) R.accumulate(x.p, z[j], R.basis[j].p);
+            for (int j = 0; j < m; ++j) R.accumulate(x.p, z[j], R.basis[j]);
             R.basis.clear();
         } else {
             // second pass from the same start: the same vectors, bit for bit
@@ -906,7 +1018,8 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
             for (int j = 0; j < m; ++j) {
                 R2.accumulate(x.p, z[j], R2.vbuf[R2.cur].p);
                 if (j + 1 < m) {
-                    R2.step(j, 0);
+                    if (reorth == QB_REORTH_FULL) R2.keep_current();
+                    R2.step(j, reorth);
                     ++total_mv;
                 }
             }
@@ -923,7 +1036,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
             Recurrence F(sec, prog, QB_C128, cyc);
             F.start_from_device(x.p);
             // the short FP64 cycle keeps its basis (the restart vector is built from it)
-            ScanOut f = run_scan(F, cyc, 0, false, 1e-300, true);
+            ScanOut f = run_scan(F, cyc, QB_REORTH_NONE, false, 1e-300, true);
             total_mv += f.matvecs;
             const int mm = static_cast<int>(f.alpha.size());
             std::vector<double> ee(std::max(1, mm - 1));
@@ -939,7 +1052,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
                 break;
             }
             cuda_check(cudaMemsetAsync(x.p, 0, nb * 16, F.st), "zero");
-            for (int j = 0; j < mm; ++j) F.accumulate(x.p, zz[j], F.basis[j].p);
+            for (int j = 0; j < mm; ++j) F.accumulate(x.p, zz[j], F.basis[j]);
             cuda_check(cudaStreamSynchronize(F.st), "refine");
         }
         *e0 = best;
@@ -969,11 +1082,10 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
             std::normal_distribution<double> nd(0.0, 1.0);
             double n2 = 0.0;
             for (std::uint64_t i = 0; i < n; ++i) {
+                const double im = nd(gen);   // the imaginary part is drawn first (see gaussian_fill)
                 const double re = nd(gen);
-                const double im = nd(gen);
                 host[i * k + s] = std::complex<double>(re, im);
             }
-            // the draw order (re, im) of Complex(nd(gen), nd(gen)) with this compiler
             for (std::uint64_t i = 0; i < n; ++i) n2 += std::norm(host[i * k + s]);
             const double inv = 1.0 / std::sqrt(n2);
             for (std::uint64_t i = 0; i < n; ++i) host[i * k + s] *= inv;
@@ -1119,7 +1231,7 @@ int qb_cf(const qb_sector* sec, const qb_program* prog, const double* phi_host, 
             throw;
         }
         if (nrm < 1e-14) return;
-        ScanOut o = run_scan(R, depth, 0, false, tolerance, false);
+        ScanOut o = run_scan(R, depth, QB_REORTH_NONE, false, tolerance, false);
         if (o.alpha.empty()) return;
         std::vector<double> a = o.alpha;
         const int m = static_cast<int>(a.size());

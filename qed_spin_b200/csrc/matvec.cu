@@ -21,6 +21,7 @@
 // =============================================================================
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -31,24 +32,21 @@ namespace qb {
 
 namespace {
 
-// The row program and key table staged in shared memory (or left in global memory when too large).
+// The column sector's tables and the row program staged in shared memory (the program stays in global
+// memory when too large).
 struct SmemProgram {
     DProgram P;
-    const u64* to_key;
+    Tables T;
 };
 
 __device__ __forceinline__ SmemProgram stage(const DProgram& P, const DSector& col, unsigned char* smem, bool in_smem) {
-    SmemProgram out{P, col.slc.to_key};
-    unsigned char* p = smem;
+    SmemProgram out{P, stage_tables(col, smem)};
+    unsigned char* p = smem + ((tables_smem_bytes(col) + 15) & ~std::size_t(15));
     auto take = [&](std::size_t bytes) {
         unsigned char* r = p;
         p += (bytes + 15) & ~std::size_t(15);
         return r;
     };
-    const int nk = col.slc.on ? col.bpw * 256 : 0;
-    u64* key = reinterpret_cast<u64*>(take(static_cast<std::size_t>(nk) * 8));
-    for (int i = threadIdx.x; i < nk; i += blockDim.x) key[i] = col.slc.to_key[i];
-    if (nk) out.to_key = key;
     if (in_smem) {
         u64* gf = reinterpret_cast<u64*>(take(P.n_groups * 8ull));
         int* gs = reinterpret_cast<int*>(take(P.n_groups * 4ull));
@@ -110,7 +108,7 @@ __device__ __forceinline__ bool connection(const DProgram& P, u64 s, u32 g, u64&
 
 // The entry of one connection: column j and value c, or false when the target's orbit cancels.
 template <bool kSame>
-__device__ __forceinline__ bool entry(const DSector& col, const u64* to_key, u64 s, long long r, double w, u64 t,
+__device__ __forceinline__ bool entry(const DSector& col, const Tables& T, u64 s, long long r, double w, u64 t,
                                       cplx h, long long& j, cplx& c) {
     if (kSame && t == s) {
         j = r;
@@ -118,7 +116,7 @@ __device__ __forceinline__ bool entry(const DSector& col, const u64* to_key, u64
         return true;
     }
     double pre, pim;
-    j = index_and_projection(col, to_key, t, pre, pim);
+    j = index_and_projection(col, T, t, pre, pim);
     if (j < 0) return false;
     c = rscale(w, cconj(cmul(h, {pre, pim})));
     return true;
@@ -147,9 +145,64 @@ template <int NV> struct VecPtrs {
     void* out[NV];
 };
 
-template <int NV, bool kInF32, bool kOutF32, bool kSame>
-__global__ void __launch_bounds__(256) walk_rows(DSector row, DSector col, DProgram P, bool prog_in_smem,
-                                                 VecPtrs<NV> io) {
+// Resolve up to B connections of one row at once: every target's canonicalisation first, then all the
+// hash probes, so a thread keeps B independent loads in flight where the single-target walk kept one.
+// j[b] = -1 when connection b is absent or its orbit cancels in the column sector.
+template <int B, bool kSame>
+__device__ __forceinline__ void resolve_batch(const DSector& col, const Tables& T, u64 s, long long r, double w,
+                                              const u64 (&t)[B], const cplx (&h)[B], int nb, long long (&j)[B],
+                                              cplx (&c)[B]) {
+    if (col.lookup != 3) {
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            j[b] = -1;
+            if (b < nb && !entry<kSame>(col, T, s, r, w, t[b], h[b], j[b], c[b])) j[b] = -1;
+        }
+        return;
+    }
+    u64 rb[B];
+    double are[B], aim[B];
+    bool need[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        j[b] = -1;
+        need[b] = false;
+        if (b >= nb) continue;
+        if (kSame && t[b] == s) {
+            j[b] = r;
+            c[b] = cconj(h[b]);
+        } else if (__popcll(t[b]) == col.n_up) {
+            need[b] = true;
+            rb[b] = canonicalize(col, T, t[b], are[b], aim[b]);
+        }
+    }
+    const u64 mask = (1ULL << col.hash_bits) - 1ULL;
+    u64 slot[B];
+    ulonglong2 e[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+        if (need[b]) {
+            slot[b] = hash_slot(rb[b], col.hash_bits);
+            e[b] = __ldg(col.slots + slot[b]);
+        }
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        if (!need[b]) continue;
+        while (e[b].x != rb[b] && e[b].x != ~0ULL) {
+            slot[b] = (slot[b] + 1) & mask;
+            e[b] = __ldg(col.slots + slot[b]);
+        }
+        if (e[b].x != rb[b]) continue;   // the target's orbit cancels in this sector
+        const long long jj = static_cast<long long>(e[b].y & 0xFFFFFFFFULL);
+        const double sc = col.n_class ? T.inv_class[static_cast<int>(e[b].y >> 32)] : __ldg(col.inv_norms + jj);
+        j[b] = jj;
+        c[b] = rscale(w, cconj(cmul(h[b], {__dmul_rn(are[b], sc), __dmul_rn(aim[b], sc)})));
+    }
+}
+
+template <int NV, int B, bool kInF32, bool kOutF32, bool kSame>
+__global__ void __launch_bounds__(256, (B >= 4 ? 2 : (B == 2 ? 3 : 4))) walk_rows(DSector row, DSector col, DProgram P,
+                                                                                 bool prog_in_smem, VecPtrs<NV> io) {
     extern __shared__ __align__(16) unsigned char smem[];
     using St = Store<kInF32>;
     using So = Store<kOutF32>;
@@ -163,18 +216,33 @@ __global__ void __launch_bounds__(256) walk_rows(DSector row, DSector col, DProg
     for (int v = 0; v < NV; ++v) acc[v] = {0.0, 0.0};
     u32 g = live ? 0u : sp.P.n_groups;
     for (;;) {
-        u64 t = 0;
-        cplx h{0.0, 0.0};
-        bool have = false;
-        while (!have && g < sp.P.n_groups) have = connection(sp.P, s, g++, t, h);
-        if (!__any_sync(0xffffffffu, have)) break;
-        if (!have) continue;
-        long long j;
-        cplx c;
-        if (!entry<kSame>(col, sp.to_key, s, static_cast<long long>(r), w, t, h, j, c)) continue;
+        u64 t[B];
+        cplx h[B];
+        int nb = 0;
 #pragma unroll
-        for (int v = 0; v < NV; ++v)
-            acc[v] = cadd(acc[v], cmul(c, St::load(static_cast<const typename St::T*>(io.in[v]), static_cast<std::size_t>(j))));
+        for (int b = 0; b < B; ++b) {
+            bool have = false;
+            t[b] = 0;
+            h[b] = {0.0, 0.0};
+            while (!have && g < sp.P.n_groups) have = connection(sp.P, s, g++, t[b], h[b]);
+            if (have) nb = b + 1;
+        }
+        if (!__any_sync(0xffffffffu, nb > 0)) break;
+        long long j[B];
+        cplx c[B];
+        resolve_batch<B, kSame>(col, sp.T, s, static_cast<long long>(r), w, t, h, nb, j, c);
+        cplx xv[B][NV];
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+            if (j[b] >= 0)
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+                    xv[b][v] = St::load(static_cast<const typename St::T*>(io.in[v]), static_cast<std::size_t>(j[b]));
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+            if (j[b] >= 0)
+#pragma unroll
+                for (int v = 0; v < NV; ++v) acc[v] = cadd(acc[v], cmul(c[b], xv[b][v]));
     }
     if (!live) return;
 #pragma unroll
@@ -212,7 +280,7 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
         long long j = -1;
         cplx cv{0.0, 0.0};
         bool act = live && g < sp.P.n_groups && connection(sp.P, s, g, t, h);
-        if (act) act = entry<kSame>(col, sp.to_key, s, static_cast<long long>(r), w, t, h, j, cv);
+        if (act) act = entry<kSame>(col, sp.T, s, static_cast<long long>(r), w, t, h, j, cv);
         unsigned acting = __ballot_sync(0xffffffffu, act) & team_mask;
         while (acting) {
             const int src = __ffs(acting) - 1;
@@ -233,15 +301,44 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
 }
 
 std::size_t smem_for(const qb_program* P, const qb_sector* col, bool& in_smem) {
-    const std::size_t key = col->slc_on ? static_cast<std::size_t>(col->bpw) * 256 * 8 + 16 : 0;
+    const std::size_t tables = (tables_smem_bytes(col->view()) + 15) & ~std::size_t(15);
     in_smem = P->view.smem_bytes <= 40 * 1024;
-    return key + (in_smem ? P->view.smem_bytes : 0);
+    return tables + (in_smem ? P->view.smem_bytes : 0);
 }
 
 template <class K> void set_smem(K kernel, std::size_t bytes) {
     if (bytes > 48 * 1024)
         cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
                    "smem attribute");
+}
+
+// Targets resolved together per thread in walk_rows (1, 2 or 4): QB_WALK_BATCH, default 1 (measured on
+// B200: batches of 2 and 4 ran 2x and 5x slower, their register pressure outweighing the extra loads in flight).
+int walk_batch() {
+    static int b = [] {
+        const char* e = std::getenv("QB_WALK_BATCH");
+        const int v = e ? std::atoi(e) : 1;
+        return v >= 4 ? 4 : (v >= 2 ? 2 : 1);
+    }();
+    return b;
+}
+
+template <int NV, int B, bool kF32, bool kOutF32>
+void launch_rows_b(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
+                   cudaStream_t st) {
+    bool in_smem = false;
+    const std::size_t smem = smem_for(P, col, in_smem);
+    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
+    if (row == col) {
+        auto k = walk_rows<NV, B, kF32, kOutF32, true>;
+        set_smem(k, smem);
+        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
+    } else {
+        auto k = walk_rows<NV, B, kF32, kOutF32, false>;
+        set_smem(k, smem);
+        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
+    }
+    cuda_check(cudaGetLastError(), "walk_rows launch");
 }
 
 template <int NV, bool kF32, bool kOutF32 = kF32>
@@ -252,19 +349,19 @@ void launch_rows_nv(const qb_sector* row, const qb_sector* col, const qb_program
         io.in[v] = ins[v];
         io.out[v] = outs[v];
     }
-    bool in_smem = false;
-    const std::size_t smem = smem_for(P, col, in_smem);
-    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
-    if (row == col) {
-        auto k = walk_rows<NV, kF32, kOutF32, true>;
-        set_smem(k, smem);
-        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
+    if constexpr (NV == 1) {
+        const int b = walk_batch();
+        if (b == 4)
+            launch_rows_b<1, 4, kF32, kOutF32>(row, col, P, io, st);
+        else if (b == 2)
+            launch_rows_b<1, 2, kF32, kOutF32>(row, col, P, io, st);
+        else
+            launch_rows_b<1, 1, kF32, kOutF32>(row, col, P, io, st);
+    } else if constexpr (NV == 2) {
+        launch_rows_b<2, 2, kF32, kOutF32>(row, col, P, io, st);
     } else {
-        auto k = walk_rows<NV, kF32, kOutF32, false>;
-        set_smem(k, smem);
-        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
+        launch_rows_b<NV, 1, kF32, kOutF32>(row, col, P, io, st);
     }
-    cuda_check(cudaGetLastError(), "walk_rows launch");
 }
 
 template <int kCpl, bool kF32, bool kOutF32>

@@ -14,17 +14,47 @@
 
 namespace qb {
 
-// Image of s under element g: OR of bpw byte-table words, XOR the element's flip mask
-// (include/ed/basis/compiled_group.h:73-78).
-__device__ __forceinline__ u64 apply_elem(const DSector& S, u64 s, int g) {
+// The small per-sector tables a kernel stages in shared memory (pointers into smem, or into global
+// memory when a table is too large to stage).
+struct Tables {
+    const u64* to_key;      // bpw x 256
+    const u64* flips;       // G
+    const double2* chars;   // G
+    const u64* edesc;       // G (arithmetic action)
+    const u64* emask;       // G (torus rows)
+    const double* inv_class;  // the distinct 1/norm values (hash lookup)
+    const u64* pack;          // the sublattice leading-block table when small enough to stage
+};
+
+// Image of s under element g (include/ed/basis/compiled_group.h:73-78): new bit i = old bit perm[i], then
+// XOR the flip mask. Chains and tori act by rotations, a reversal, and row rotations; any other group
+// through its byte tables.
+__device__ __forceinline__ u64 apply_elem(const DSector& S, const Tables& T, u64 s, int g) {
+    if (S.gkind != 0) {
+        const u64 d = T.edesc[g];
+        const int kind = static_cast<int>(d & 0xFF);
+        const int c = static_cast<int>((d >> 8) & 0xFF);
+        const int N = S.N;
+        const u64 full = N == 64 ? ~0ULL : ((1ULL << N) - 1ULL);
+        if (kind == kElemRefl) s = __brevll(s) >> (64 - N);
+        if (c) s = ((s >> c) | (s << (N - c))) & full;
+        if (kind == kElemTorus) {
+            const int a = static_cast<int>((d >> 16) & 0xFF);
+            if (a) {
+                const u64 lo = T.emask[g];
+                s = ((s >> a) & lo) | ((s << (S.Lx - a)) & ~lo & full);
+            }
+        }
+        return s ^ T.flips[g];
+    }
     const u64* l = S.lut + static_cast<std::size_t>(g) * S.bpw * 256;
     u64 r = 0;
 #pragma unroll 8
     for (int b = 0; b < S.bpw; ++b) r |= __ldg(l + b * 256 + static_cast<int>((s >> (8 * b)) & 0xFFu));
-    return r ^ __ldg(S.flips + g);
+    return r ^ T.flips[g];
 }
 
-// A state's bits moved to their key positions (to_key staged in shared memory).
+// A state's bits moved to their key positions.
 __device__ __forceinline__ u64 key_of(const u64* to_key, int bpw, u64 s) {
     u64 k = 0;
 #pragma unroll 8
@@ -36,71 +66,98 @@ __device__ __forceinline__ u32 pattern_of(u64 k, int j, int N, int L) {
     return static_cast<u32>(k >> (N - (j + 1) * L)) & ((1u << L) - 1u);
 }
 
-// fn(g) in ascending order for the elements whose image has the least leading block
-// (sublattice_code.h:102-131). `first_lead`: the state's own leading block vs the least one
-// (visit_state's early rejection) is reported through least / own.
+// The several-blocks case of for_each_candidate: merge the ascending candidate lists of every block that
+// reaches the least leading block (each element maps exactly one block to the lead). Rare; kept out of
+// line so the common path holds no local arrays.
 template <class Fn>
-__device__ __forceinline__ void for_each_candidate(const DSector& S, u64 k, Fn&& fn) {
+__device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pack, u64 k, u32 best, Fn& fn) {
     const int L = S.slc.L, m = S.slc.m, N = S.N;
-    u32 entry[8];
-    u32 best = 0xFFFFFFFFu;
-    for (int j = 0; j < m; ++j) {
-        entry[j] = (static_cast<u32>(j) << L) + pattern_of(k, j, N, L);
-        const u32 v = __ldg(S.slc.lead + entry[j]);
-        best = v < best ? v : best;
-    }
-    u32 pos[8], end[8];
+    u64 sel[8];
+    u32 pos[8];
     int n = 0;
-    for (int j = 0; j < m; ++j)
-        if (__ldg(S.slc.lead + entry[j]) == best) {
-            pos[n] = __ldg(S.slc.cand_off + entry[j]);
-            end[n] = __ldg(S.slc.cand_off + entry[j] + 1);
+    for (int j = 0; j < m; ++j) {
+        const u64 e = pack[(static_cast<u32>(j) << L) + pattern_of(k, j, N, L)];
+        if (static_cast<u32>(e & 0xFFFFu) == best) {
+            sel[n] = e;
+            pos[n] = 0;
             ++n;
         }
-    if (n == 1) {
-        for (u32 p = pos[0]; p < end[0]; ++p) fn(static_cast<int>(__ldg(S.slc.cand + p)));
-        return;
     }
     for (;;) {
         int pick = -1;
         u32 g = 0xFFFFFFFFu;
-        for (int i = 0; i < n; ++i)
-            if (pos[i] < end[i]) {
-                const u32 c = __ldg(S.slc.cand + pos[i]);
-                if (c < g) {
-                    g = c;
-                    pick = i;
-                }
+        for (int i = 0; i < n; ++i) {
+            const u32 cnt = static_cast<u32>((sel[i] >> 16) & 0xFFFFu);
+            if (pos[i] >= cnt) continue;
+            const u32 pay = static_cast<u32>(sel[i] >> 32);
+            const u32 c = cnt == 1 ? pay : static_cast<u32>(__ldg(S.slc.cand + pay + pos[i]));
+            if (c < g) {
+                g = c;
+                pick = i;
             }
+        }
         if (pick < 0) return;
         ++pos[pick];
         fn(static_cast<int>(g));
     }
 }
 
+// fn(g) in ascending order for the elements whose image has the least leading block
+// (sublattice_code.h:102-131); returns that least leading block. One packed load per block.
+template <class Fn>
+__device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* pack, u64 k, Fn&& fn) {
+    const int L = S.slc.L, m = S.slc.m, N = S.N;
+    u32 best = 0xFFFFFFFFu;
+    u64 first = 0;
+    int n = 0;
+    for (int j = 0; j < m; ++j) {
+        const u64 e = pack[(static_cast<u32>(j) << L) + pattern_of(k, j, N, L)];
+        const u32 v = static_cast<u32>(e & 0xFFFFu);
+        if (v < best) {
+            best = v;
+            first = e;
+            n = 1;
+        } else if (v == best) {
+            ++n;
+        }
+    }
+    if (n == 1) {
+        const u32 cnt = static_cast<u32>((first >> 16) & 0xFFFFu);
+        const u32 pay = static_cast<u32>(first >> 32);
+        if (cnt == 1) {
+            fn(static_cast<int>(pay));
+        } else {
+            for (u32 p = 0; p < cnt; ++p) fn(static_cast<int>(__ldg(S.slc.cand + pay + p)));
+        }
+        return best;
+    }
+    merge_candidates(S, pack, k, best, fn);
+    return best;
+}
+
 // Representative of t and the conjugated character sum over the elements that reach it.
-__device__ __forceinline__ u64 canonicalize(const DSector& S, const u64* to_key, u64 t, double& acc_re,
+__device__ __forceinline__ u64 canonicalize(const DSector& S, const Tables& T, u64 t, double& acc_re,
                                             double& acc_im) {
     u64 rb = ~0ULL, best = ~0ULL;
     acc_re = 0.0;
     acc_im = 0.0;
     auto visit = [&](int g) {
-        const u64 img = apply_elem(S, t, g);
-        const u64 k = S.slc.on ? key_of(to_key, S.bpw, img) : img;
+        const u64 img = apply_elem(S, T, t, g);
+        const u64 k = S.slc.on ? key_of(T.to_key, S.bpw, img) : img;
         if (k < best) {
             best = k;
             rb = img;
-            const double2 c = __ldg(S.chars + g);
+            const double2 c = T.chars[g];
             acc_re = __dadd_rn(0.0, c.x);
             acc_im = __dsub_rn(0.0, c.y);
         } else if (k == best) {
-            const double2 c = __ldg(S.chars + g);
+            const double2 c = T.chars[g];
             acc_re = __dadd_rn(acc_re, c.x);
             acc_im = __dsub_rn(acc_im, c.y);
         }
     };
     if (S.slc.on) {
-        for_each_candidate(S, key_of(to_key, S.bpw, t), visit);
+        for_each_candidate(S, T.pack, key_of(T.to_key, S.bpw, t), visit);
     } else {
         for (int g = 0; g < S.G; ++g) visit(g);
     }
@@ -121,8 +178,37 @@ __device__ __forceinline__ u64 rank_of(const DSector& S, u64 s) {
     return r;
 }
 
+// The slot a state hashes to (a 64-bit finaliser, then the top hash_bits bits).
+__device__ __forceinline__ u64 hash_slot(u64 s, int bits) {
+    s ^= s >> 31;
+    s *= 0x7fb5d329728ea185ULL;
+    s ^= s >> 27;
+    s *= 0x81dadef4bc2dd44dULL;
+    s ^= s >> 33;
+    return s >> (64 - bits);
+}
+
+// Hash lookup: index of rb (or -1) and its 1/norm class, by linear probing.
+__device__ __forceinline__ long long hash_find(const DSector& S, u64 rb, int& cls) {
+    const u64 mask = (1ULL << S.hash_bits) - 1ULL;
+    u64 h = hash_slot(rb, S.hash_bits);
+    for (;;) {
+        const ulonglong2 e = __ldg(S.slots + h);
+        if (e.x == rb) {
+            cls = static_cast<int>(e.y >> 32);
+            return static_cast<long long>(e.y & 0xFFFFFFFFULL);
+        }
+        if (e.x == ~0ULL) return -1;
+        h = (h + 1) & mask;
+    }
+}
+
 // Index of representative rb in the sector, or -1 (index_of_rep, rep_symmetry_basis_policy.h:169-202).
 __device__ __forceinline__ long long index_of_rep(const DSector& S, u64 rb) {
+    if (S.lookup == 3) {
+        int cls;
+        return hash_find(S, rb, cls);
+    }
     if (S.lookup == 1) return static_cast<long long>(__ldg(S.rank_table + rank_of(S, rb)));
     std::uint64_t lo = 0, hi = S.dim;
     if (S.lookup == 2) {
@@ -143,17 +229,114 @@ __device__ __forceinline__ long long index_of_rep(const DSector& S, u64 rb) {
 }
 
 // index_and_projection: index of t's orbit in S (or -1) and conj(beta_t) * inv_norm[index].
-__device__ __forceinline__ long long index_and_projection(const DSector& S, const u64* to_key, u64 t, double& pre,
+__device__ __forceinline__ long long index_and_projection(const DSector& S, const Tables& T, u64 t, double& pre,
                                                           double& pim) {
     if (__popcll(t) != S.n_up) return -1;
     double are, aim;
-    const u64 rb = canonicalize(S, to_key, t, are, aim);
-    const long long j = index_of_rep(S, rb);
-    if (j < 0) return -1;
-    const double s = __ldg(S.inv_norms + j);
+    const u64 rb = canonicalize(S, T, t, are, aim);
+    long long j;
+    double s;
+    if (S.lookup == 3) {
+        int cls = 0;
+        j = hash_find(S, rb, cls);
+        if (j < 0) return -1;
+        s = S.n_class ? T.inv_class[cls] : __ldg(S.inv_norms + j);
+    } else {
+        j = index_of_rep(S, rb);
+        if (j < 0) return -1;
+        s = __ldg(S.inv_norms + j);
+    }
     pre = __dmul_rn(are, s);
     pim = __dmul_rn(aim, s);
     return j;
+}
+
+// Bytes of shared memory stage_tables takes for a sector (0 for the parts left in global memory).
+constexpr std::size_t kPackSmemMax = 16 * 1024;
+
+// Byte offsets of the staged tables; every array starts on a 16-byte boundary. Host sizing and device
+// staging both read this one layout.
+struct TablesLayout {
+    std::size_t key = 0, pack = 0, chars = 0, flips = 0, desc = 0, mask = 0, cls = 0, total = 0;
+    bool stage_key = false, stage_pack = false, stage_elems = false, stage_cls = false;
+};
+
+__host__ __device__ inline std::size_t align16(std::size_t x) { return (x + 15) & ~std::size_t(15); }
+
+__host__ __device__ inline TablesLayout tables_layout(const DSector& S) {
+    TablesLayout l;
+    std::size_t p = 0;
+    if (S.slc.on) {
+        l.stage_key = true;
+        l.key = p;
+        p = align16(p + static_cast<std::size_t>(S.bpw) * 256 * 8);
+        const std::size_t np = (static_cast<std::size_t>(S.slc.m) << S.slc.L) * 8;
+        if (np <= kPackSmemMax) {
+            l.stage_pack = true;
+            l.pack = p;
+            p = align16(p + np);
+        }
+    }
+    if (S.G <= 1024) {
+        l.stage_elems = true;
+        l.chars = p;
+        p = align16(p + static_cast<std::size_t>(S.G) * 16);
+        l.flips = p;
+        p = align16(p + static_cast<std::size_t>(S.G) * 8);
+        l.desc = p;
+        p = align16(p + static_cast<std::size_t>(S.G) * 8);
+        l.mask = p;
+        p = align16(p + static_cast<std::size_t>(S.G) * 8);
+    }
+    if (S.n_class > 0) {
+        l.stage_cls = true;
+        l.cls = p;
+        p = align16(p + static_cast<std::size_t>(S.n_class) * 8);
+    }
+    l.total = p;
+    return l;
+}
+
+__host__ __device__ inline std::size_t tables_smem_bytes(const DSector& S) { return tables_layout(S).total; }
+
+// Stage a sector's small tables into shared memory at `smem` (16-byte aligned, tables_smem_bytes long).
+// Every thread of the block takes part; the caller synchronises afterwards.
+__device__ __forceinline__ Tables stage_tables(const DSector& S, unsigned char* smem) {
+    Tables T{S.slc.to_key, S.flips, S.chars, S.edesc, S.emask, S.inv_class, S.slc.pack};
+    const TablesLayout l = tables_layout(S);
+    if (l.stage_key) {
+        u64* key = reinterpret_cast<u64*>(smem + l.key);
+        for (int i = threadIdx.x; i < S.bpw * 256; i += blockDim.x) key[i] = S.slc.to_key[i];
+        T.to_key = key;
+    }
+    if (l.stage_pack) {
+        u64* pk = reinterpret_cast<u64*>(smem + l.pack);
+        const std::size_t np = static_cast<std::size_t>(S.slc.m) << S.slc.L;
+        for (std::size_t i = threadIdx.x; i < np; i += blockDim.x) pk[i] = S.slc.pack[i];
+        T.pack = pk;
+    }
+    if (l.stage_elems) {
+        double2* ch = reinterpret_cast<double2*>(smem + l.chars);
+        u64* fl = reinterpret_cast<u64*>(smem + l.flips);
+        u64* de = reinterpret_cast<u64*>(smem + l.desc);
+        u64* em = reinterpret_cast<u64*>(smem + l.mask);
+        for (int i = threadIdx.x; i < S.G; i += blockDim.x) {
+            ch[i] = S.chars[i];
+            fl[i] = S.flips[i];
+            de[i] = S.edesc ? S.edesc[i] : 0ULL;
+            em[i] = S.emask ? S.emask[i] : 0ULL;
+        }
+        T.chars = ch;
+        T.flips = fl;
+        T.edesc = de;
+        T.emask = em;
+    }
+    if (l.stage_cls) {
+        double* ic = reinterpret_cast<double*>(smem + l.cls);
+        for (int i = threadIdx.x; i < S.n_class; i += blockDim.x) ic[i] = S.inv_class[i];
+        T.inv_class = ic;
+    }
+    return T;
 }
 
 }  // namespace qb

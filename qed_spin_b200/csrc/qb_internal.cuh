@@ -4,12 +4,15 @@
 // Layout in HBM of one sector (qb_sector):
 //   reps       u64[dim]    the representatives, ascending (the basis index IS the array index)
 //   inv_norms  f64[dim]    1/norm per representative
-//   lut        u64[G][bpw][256]   the byte-decomposition image table of every group element
-//   flips      u64[G], chars f64x2[G]
+//   lut        u64[G][bpw][256]   the byte-decomposition image table of every group element (used when
+//                                 the group has no arithmetic action: chains and tori rotate bits instead)
+//   flips      u64[G], chars f64x2[G], edesc / emask u64[G]  per-element action parameters
 //   to_key     u64[bpw][256]      sublattice key order (when engaged)
-//   lead       u16[m][2^L], cand_off u32[m 2^L + 1], cand u16[...]  leading-block table / candidates
-//   lookup     either rank_table i32[C(N, n_up)] indexed by the combinadic rank (computed from
-//              rank_lut u64[bpw][N+1][256]), or bucket_off u32[n_buckets + 1] over the states.
+//   pack       u64[m][2^L]        least leading block | candidate count | candidate or list offset
+//   cand       u16[...]           the candidate lists of the entries with more than one
+//   lookup     hash slots u64x2[2^b]: (state, index | 1/norm class << 32), open addressing, load <= 1/2;
+//              or rank_table i32[C(N, n_up)] indexed by the combinadic rank (rank_lut
+//              u64[bpw][N+1][256]); or bucket_off u32[n_buckets + 1] over the ascending states.
 // The small tables (program, to_key) are staged in shared memory by each kernel.
 // =============================================================================
 #pragma once
@@ -105,10 +108,14 @@ template <class T> struct DevBuf {
 struct DSlc {
     int on = 0, L = 0, m = 0;
     const u64* to_key = nullptr;    // bpw x 256
-    const u16* lead = nullptr;      // m << L
-    const u32* cand_off = nullptr;  // (m << L) + 1
+    // per (block j, pattern): least leading block (bits 0-15) | candidate count (16-31) | payload (32-63):
+    // the candidate itself when there is one, else the offset of the block's list in `cand`
+    const u64* pack = nullptr;      // m << L
     const u16* cand = nullptr;
 };
+
+// Group element kinds with an arithmetic action (0: the byte-LUT action).
+enum : int { kElemLut = 0, kElemRot = 1, kElemRefl = 2, kElemTorus = 3 };
 
 struct DSector {
     int N = 0, n_up = 0, G = 0, bpw = 0;
@@ -118,9 +125,18 @@ struct DSector {
     const u64* lut = nullptr;       // G x bpw x 256
     const u64* flips = nullptr;     // G
     const double2* chars = nullptr; // G
+    // arithmetic group action (gkind != 0): per element kind | rotation << 8 | row shift << 16, and the
+    // torus row mask; gkind 1 chains (rotations, reflections), 2 torus translations with row length Lx
+    int gkind = 0, Lx = 0;
+    const u64* edesc = nullptr;     // G
+    const u64* emask = nullptr;     // G
     DSlc slc;
-    // lookup: kind 1 rank table, 2 state buckets
+    // lookup: kind 1 rank table, 2 state buckets, 3 hash slots
     int lookup = 0;
+    const ulonglong2* slots = nullptr;   // [state, index | class << 32], 2^hash_bits slots; empty: state ~0
+    int hash_bits = 0;
+    const double* inv_class = nullptr;   // the distinct 1/norm values, indexed by class (hash lookup)
+    int n_class = 0;
     const std::int32_t* rank_table = nullptr;
     const u64* rank_lut = nullptr;  // bpw x (N + 1) x 256: byte b's share of the combinadic rank
     const u32* bucket_off = nullptr;
@@ -150,12 +166,15 @@ struct qb_sector {
     qb::DevBuf<double> inv_norms;
     qb::DevBuf<qb::u64> lut, flips;
     qb::DevBuf<double2> chars;
-    qb::DevBuf<qb::u64> to_key;
-    qb::DevBuf<qb::u16> lead, cand;
-    qb::DevBuf<qb::u32> cand_off;
+    qb::DevBuf<qb::u64> to_key, lead_pack, edesc, emask;
+    qb::DevBuf<qb::u16> cand;
+    int gkind = 0, Lx = 0;
     qb::DevBuf<std::int32_t> rank_table;
     qb::DevBuf<qb::u64> rank_lut;
     qb::DevBuf<qb::u32> bucket_off;
+    qb::DevBuf<ulonglong2> slots;
+    qb::DevBuf<double> inv_class;
+    int hash_bits = 0, n_class = 0;
     int slc_on = 0, slc_L = 0, slc_m = 0;
     int lookup = 0;
     qb::u64 bucket_base = 0, bucket_count = 0;

@@ -238,26 +238,27 @@ __device__ __forceinline__ u64 gosper_next(u64 v) {
 
 // visit_state + projected norm (orbit_table.h:93-99, 147-171; group_sector.cpp:183-186): 0 when s is
 // not a kept representative, else 1/norm.
-__device__ __forceinline__ double visit_inv_norm(const DSector& S, const u64* to_key, u64 s) {
+__device__ __forceinline__ double visit_inv_norm(const DSector& S, const Tables& T, u64 s) {
     double sre = 0.0, sim = 0.0;
     int cnt = 0;
     if (S.slc.on) {
-        const u64 k = key_of(to_key, S.bpw, s);
-        // least leading block over the blocks vs the state's own (visit_state's early exit)
+        const u64 k = key_of(T.to_key, S.bpw, s);
+        // the least leading block over the blocks vs the state's own (visit_state's early exit)
         u32 least = 0xFFFFFFFFu;
         for (int j = 0; j < S.slc.m; ++j) {
-            const u32 v = __ldg(S.slc.lead + ((static_cast<u32>(j) << S.slc.L) + pattern_of(k, j, S.N, S.slc.L)));
+            const u32 v = static_cast<u32>(T.pack[(static_cast<u32>(j) << S.slc.L) + pattern_of(k, j, S.N, S.slc.L)] &
+                                           0xFFFFu);
             least = v < least ? v : least;
         }
         if (least < pattern_of(k, 0, S.N, S.slc.L)) return 0.0;
         bool rep = true;
-        for_each_candidate(S, k, [&](int g) {
+        for_each_candidate(S, T.pack, k, [&](int g) {
             if (!rep) return;
-            const u64 ik = key_of(to_key, S.bpw, apply_elem(S, s, g));
+            const u64 ik = key_of(T.to_key, S.bpw, apply_elem(S, T, s, g));
             if (ik < k) {
                 rep = false;
             } else if (ik == k) {
-                const double2 c = __ldg(S.chars + g);
+                const double2 c = T.chars[g];
                 sre = __dadd_rn(sre, c.x);
                 sim = __dadd_rn(sim, c.y);
                 ++cnt;
@@ -266,10 +267,10 @@ __device__ __forceinline__ double visit_inv_norm(const DSector& S, const u64* to
         if (!rep) return 0.0;
     } else {
         for (int g = 0; g < S.G; ++g) {
-            const u64 img = apply_elem(S, s, g);
+            const u64 img = apply_elem(S, T, s, g);
             if (img < s) return 0.0;
             if (img == s) {
-                const double2 c = __ldg(S.chars + g);
+                const double2 c = T.chars[g];
                 sre = __dadd_rn(sre, c.x);
                 sim = __dadd_rn(sim, c.y);
                 ++cnt;
@@ -287,9 +288,8 @@ __device__ __forceinline__ double visit_inv_norm(const DSector& S, const u64* to
 
 __global__ void enum_kernel(DSector S, u64 total, u64 chunk, u64 n_chunks, const u64* C, u64* counts,
                             const u64* offsets, u64* out_reps, double* out_inv) {
-    extern __shared__ u64 s_key[];
-    if (S.slc.on)
-        for (int i = threadIdx.x; i < S.bpw * 256; i += blockDim.x) s_key[i] = S.slc.to_key[i];
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Tables T = stage_tables(S, smem);
     __syncthreads();
     const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
     for (u64 c = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; c < n_chunks; c += stride) {
@@ -299,7 +299,7 @@ __global__ void enum_kernel(DSector S, u64 total, u64 chunk, u64 n_chunks, const
         u64 cnt = 0;
         const u64 off = offsets ? offsets[c] : 0;
         for (u64 i = begin; i < end; ++i) {
-            const double inv = visit_inv_norm(S, s_key, s);
+            const double inv = visit_inv_norm(S, T, s);
             if (inv != 0.0) {
                 if (offsets) {
                     out_reps[off + cnt] = s;
@@ -329,15 +329,61 @@ __global__ void bucket_kernel(const u64* reps, u64 dim, u64 base, int shift, u64
         for (u64 c = b + 1; c <= nb; ++c) off[c] = static_cast<u32>(dim);
 }
 
+// The distinct 1/norm values (bit patterns) into a small open-addressing set; overflow flags a set
+// too small (the lookup then reads inv_norms directly).
+constexpr int kClassSet = 4096;
+__global__ void class_set_kernel(const double* inv, u64 dim, u64* set, int* overflow) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= dim) return;
+    const u64 v = static_cast<u64>(__double_as_longlong(inv[i]));
+    u32 h = static_cast<u32>((v * 0x9E3779B97F4A7C15ULL) >> 52) & (kClassSet - 1);
+    for (int probe = 0; probe < kClassSet; ++probe) {
+        const u64 old = atomicCAS(reinterpret_cast<unsigned long long*>(set + h), ~0ULL, v);
+        if (old == ~0ULL || old == v) return;
+        h = (h + 1) & (kClassSet - 1);
+    }
+    *overflow = 1;
+}
+
+// Insert every representative: its state, index and 1/norm class (binary search in the sorted classes).
+__global__ void hash_insert_kernel(const u64* reps, const double* inv, u64 dim, ulonglong2* slots, int bits,
+                                   const u64* classes, int n_class) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= dim) return;
+    const u64 s = reps[i];
+    u64 cls = 0;
+    if (n_class > 0) {
+        const u64 v = static_cast<u64>(__double_as_longlong(inv[i]));
+        int lo = 0, hi = n_class;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (classes[mid] < v)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        cls = static_cast<u64>(lo);
+    }
+    const u64 mask = (1ULL << bits) - 1ULL;
+    u64 h = hash_slot(s, bits);
+    for (;;) {
+        const u64 old = atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].x), ~0ULL, s);
+        if (old == ~0ULL) {
+            slots[h].y = i | (cls << 32);
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+}
+
 __global__ void index_proj_kernel(DSector S, const u64* states, u64 n, long long* idx, double2* proj) {
-    extern __shared__ u64 s_key[];
-    if (S.slc.on)
-        for (int i = threadIdx.x; i < S.bpw * 256; i += blockDim.x) s_key[i] = S.slc.to_key[i];
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Tables T = stage_tables(S, smem);
     __syncthreads();
     const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double pr = 0.0, pi = 0.0;
-    idx[i] = index_and_projection(S, s_key, states[i], pr, pi);
+    idx[i] = index_and_projection(S, T, states[i], pr, pi);
     proj[i] = make_double2(pr, pi);
 }
 
@@ -351,6 +397,56 @@ int sm_count() {
         if (n <= 0) n = 148;
     });
     return n;
+}
+
+// Arithmetic actions: chain rotations p[i] = i + t and reflections p[i] = t - i (mod N), or torus
+// translations of rows of Lx sites, p[x + Lx y] = (x + a mod Lx) + Lx (y + b mod Ly). gkind 0 when some
+// element is neither (the byte tables then act).
+int classify_group(const int32_t* perms, int G, int N, int& Lx, std::vector<u64>& desc, std::vector<u64>& mask) {
+    desc.assign(G, 0ULL);
+    mask.assign(G, 0ULL);
+    Lx = 0;
+    bool chain = true;
+    for (int g = 0; g < G && chain; ++g) {
+        const int32_t* p = perms + g * N;
+        const int t = p[0];
+        bool rot = true, refl = true;
+        for (int i = 0; i < N; ++i) {
+            rot = rot && p[i] == (i + t) % N;
+            refl = refl && p[i] == ((t - i) % N + N) % N;
+        }
+        if (rot)
+            desc[g] = kElemRot | (static_cast<u64>(t) << 8);
+        else if (refl)
+            desc[g] = kElemRefl | (static_cast<u64>(((N - 1 - t) % N + N) % N) << 8);
+        else
+            chain = false;
+    }
+    if (chain) return 1;
+    for (int lx = 2; lx < N; ++lx) {
+        if (N % lx) continue;
+        const int ly = N / lx;
+        bool ok = true;
+        for (int g = 0; g < G && ok; ++g) {
+            const int32_t* p = perms + g * N;
+            const int a = p[0] % lx, b = p[0] / lx;
+            for (int y = 0; y < ly && ok; ++y)
+                for (int x = 0; x < lx && ok; ++x) ok = p[x + lx * y] == (x + a) % lx + lx * ((y + b) % ly);
+            if (!ok) break;
+            u64 lo = 0;
+            for (int y = 0; y < ly; ++y)
+                for (int x = 0; x < lx - a; ++x) lo |= 1ULL << (x + lx * y);
+            desc[g] = kElemTorus | (static_cast<u64>(lx * b) << 8) | (static_cast<u64>(a) << 16);
+            mask[g] = lo;
+        }
+        if (ok) {
+            Lx = lx;
+            return 2;
+        }
+    }
+    desc.assign(G, 0ULL);
+    mask.assign(G, 0ULL);
+    return 0;
 }
 
 void upload_group(qb_sector& s, const qb_sector_desc& d) {
@@ -369,9 +465,21 @@ void upload_group(qb_sector& s, const qb_sector_desc& d) {
         s.slc_L = slc.L;
         s.slc_m = slc.m;
         s.to_key.upload(slc.to_key);
-        s.lead.upload(slc.lead);
-        s.cand_off.upload(slc.cand_off);
+        std::vector<u64> pack(slc.lead.size());
+        for (std::size_t i = 0; i < pack.size(); ++i) {
+            const u64 cnt = slc.cand_off[i + 1] - slc.cand_off[i];
+            if (cnt > 0xFFFF) throw Error(QB_EUNSUPPORTED, "sublattice code: more than 65535 candidates");
+            const u64 pay = cnt == 1 ? slc.cand[slc.cand_off[i]] : slc.cand_off[i];
+            pack[i] = static_cast<u64>(slc.lead[i]) | (cnt << 16) | (pay << 32);
+        }
+        s.lead_pack.upload(pack);
         s.cand.upload(slc.cand);
+    }
+    std::vector<u64> desc, mask;
+    s.gkind = classify_group(d.perms, G, N, s.Lx, desc, mask);
+    if (s.gkind) {
+        s.edesc.upload(desc);
+        s.emask.upload(mask);
     }
     s.rank_lut.upload(build_rank_lut(N));
 }
@@ -416,17 +524,45 @@ void build_lookup(qb_sector& s, int want) {
     cuda_check(cudaMemcpy(&ends[0], s.reps.p, 8, cudaMemcpyDeviceToHost), "read reps");
     cuda_check(cudaMemcpy(&ends[1], s.reps.p + (s.dim - 1), 8, cudaMemcpyDeviceToHost), "read reps");
     int mode = want;
-    if (mode == QB_LOOKUP_AUTO) {
-        // the buckets while the representatives and their offsets stay cache-sized, else a rank table
-        // when it fits well inside free memory
-        const double bucket_bytes = 8.0 * static_cast<double>(s.dim) * 2.0;
-        if (bucket_bytes <= 96.0 * (1 << 20))
-            mode = QB_LOOKUP_BUCKETS;
-        else
-            mode = (table_bytes < 0.4 * static_cast<double>(free_b) && s.dim < (1ULL << 31)) ? QB_LOOKUP_RANK
-                                                                                            : QB_LOOKUP_BUCKETS;
-    }
-    if (mode == QB_LOOKUP_RANK) {
+    if (mode == QB_LOOKUP_AUTO) mode = QB_LOOKUP_HASH;
+    if (mode == QB_LOOKUP_HASH && (s.dim >= (1ULL << 32) || (s.N == 64 && s.n_up == 64))) mode = QB_LOOKUP_BUCKETS;
+    (void)table_bytes;
+    if (mode == QB_LOOKUP_HASH) {
+        // load factor <= 1/2
+        int bits = 4;
+        while ((1ULL << bits) < 2 * s.dim) ++bits;
+        s.hash_bits = bits;
+        s.slots.alloc(1ULL << bits);
+        cuda_check(cudaMemset(s.slots.p, 0xFF, (1ULL << bits) * sizeof(ulonglong2)), "hash clear");
+        // the 1/norm classes
+        DevBuf<u64> set(kClassSet);
+        DevBuf<int> ovf(1);
+        cuda_check(cudaMemset(set.p, 0xFF, kClassSet * 8), "class set clear");
+        cuda_check(cudaMemset(ovf.p, 0, 4), "class set clear");
+        const unsigned blocks = static_cast<unsigned>((s.dim + 255) / 256);
+        class_set_kernel<<<blocks, 256>>>(s.inv_norms.p, s.dim, set.p, ovf.p);
+        cuda_check(cudaGetLastError(), "class set");
+        std::vector<u64> hs(kClassSet);
+        int overflow = 0;
+        cuda_check(cudaMemcpy(hs.data(), set.p, kClassSet * 8, cudaMemcpyDeviceToHost), "class set read");
+        cuda_check(cudaMemcpy(&overflow, ovf.p, 4, cudaMemcpyDeviceToHost), "class set read");
+        std::vector<u64> cls;
+        for (u64 v : hs)
+            if (v != ~0ULL) cls.push_back(v);
+        std::sort(cls.begin(), cls.end());
+        if (overflow || cls.size() > 2048) cls.clear();
+        DevBuf<u64> dcls;
+        dcls.upload(cls);
+        if (!cls.empty()) {
+            std::vector<double> vals(cls.size());
+            std::memcpy(vals.data(), cls.data(), cls.size() * 8);
+            s.inv_class.upload(vals);
+        }
+        s.n_class = static_cast<int>(cls.size());
+        hash_insert_kernel<<<blocks, 256>>>(s.reps.p, s.inv_norms.p, s.dim, s.slots.p, bits, dcls.p, s.n_class);
+        cuda_check(cudaGetLastError(), "hash insert");
+        s.lookup = 3;
+    } else if (mode == QB_LOOKUP_RANK) {
         if (s.dim >= (1ULL << 31)) throw Error(QB_EUNSUPPORTED, "rank table: more than 2^31 representatives");
         s.rank_table.alloc(static_cast<std::size_t>(ranks));
         cuda_check(cudaMemset(s.rank_table.p, 0xFF, ranks * 4), "rank table clear");
@@ -473,9 +609,12 @@ qb::DSector qb_sector::view() const {
     v.slc.L = slc_L;
     v.slc.m = slc_m;
     v.slc.to_key = to_key.p;
-    v.slc.lead = lead.p;
-    v.slc.cand_off = cand_off.p;
+    v.slc.pack = lead_pack.p;
     v.slc.cand = cand.p;
+    v.gkind = gkind;
+    v.Lx = Lx;
+    v.edesc = edesc.p;
+    v.emask = emask.p;
     v.lookup = lookup;
     v.rank_table = rank_table.p;
     v.rank_lut = rank_lut.p;
@@ -483,12 +622,17 @@ qb::DSector qb_sector::view() const {
     v.bucket_base = bucket_base;
     v.bucket_count = bucket_count;
     v.bucket_shift = bucket_shift;
+    v.slots = slots.p;
+    v.hash_bits = hash_bits;
+    v.inv_class = inv_class.p;
+    v.n_class = n_class;
     return v;
 }
 
 std::uint64_t qb_sector::device_bytes() const {
     return reps.bytes() + inv_norms.bytes() + lut.bytes() + flips.bytes() + chars.bytes() + to_key.bytes() +
-           lead.bytes() + cand.bytes() + cand_off.bytes() + rank_table.bytes() + rank_lut.bytes() + bucket_off.bytes();
+           lead_pack.bytes() + cand.bytes() + edesc.bytes() + emask.bytes() + rank_table.bytes() + rank_lut.bytes() +
+           bucket_off.bytes() + slots.bytes() + inv_class.bytes();
 }
 
 extern "C" {
@@ -524,7 +668,10 @@ int qb_sector_create(const qb_sector_desc* d, qb_sector** out) {
         const u64 n_chunks = (total + chunk - 1) / chunk;
         DevBuf<u64> counts(n_chunks), offsets(n_chunks + 1);
         DSector v = s->view();
-        const std::size_t smem = s->slc_on ? static_cast<std::size_t>(s->bpw) * 256 * 8 : 0;
+        const std::size_t smem = tables_smem_bytes(v);
+        if (smem > 48 * 1024)
+            cuda_check(cudaFuncSetAttribute(enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                       "smem attribute");
         const unsigned threads = 256;
         const unsigned blocks =
             static_cast<unsigned>(std::min<u64>((n_chunks + threads - 1) / threads, static_cast<u64>(sm_count()) * 16));
@@ -608,7 +755,10 @@ int qb_index_and_projection(const qb_sector* s, const uint64_t* states, uint64_t
         d_states.upload(reinterpret_cast<const u64*>(states), n);
         DevBuf<long long> d_idx(n);
         DevBuf<double2> d_proj(n);
-        const std::size_t smem = s->slc_on ? static_cast<std::size_t>(s->bpw) * 256 * 8 : 0;
+        const std::size_t smem = tables_smem_bytes(s->view());
+        if (smem > 48 * 1024)
+            cuda_check(cudaFuncSetAttribute(index_proj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                       "smem attribute");
         index_proj_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, smem>>>(s->view(), d_states.p, n, d_idx.p,
                                                                                     d_proj.p);
         cuda_check(cudaGetLastError(), "index_and_projection");

@@ -53,7 +53,10 @@ class Sector:
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:
-            lib().qb_sector_destroy(self.h)
+            try:
+                lib().qb_sector_destroy(self.h)
+            except Exception:   # interpreter shutdown: the library is already gone
+                pass
             self.h = C.c_void_p()
 
     __del__ = close
@@ -74,7 +77,7 @@ class Sector:
         b, L, m, k = C.c_uint64(), C.c_int(), C.c_int(), C.c_int()
         check(lib().qb_sector_info(self.h, C.byref(b), C.byref(L), C.byref(m), C.byref(k)))
         return dict(device_bytes=b.value, slc_L=L.value, slc_m=m.value,
-                    lookup={0: "none", 1: "rank", 2: "buckets"}[k.value])
+                    lookup={0: "none", 1: "rank", 2: "buckets", 3: "hash"}[k.value])
 
     def index_and_projection(self, states):
         st = np.ascontiguousarray(states, np.uint64)
@@ -107,7 +110,10 @@ class Program:
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:
-            lib().qb_program_destroy(self.h)
+            try:
+                lib().qb_program_destroy(self.h)
+            except Exception:   # interpreter shutdown: the library is already gone
+                pass
             self.h = C.c_void_p()
 
     __del__ = close
