@@ -155,6 +155,25 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
 int qb_cf(const qb_sector* sec, const qb_program* prog, const double* phi_host, int depth, const double* omega,
           int n_omega, double eta, double shift, double tolerance, double* S, double* shift_out);
 
+/* ---- the Lanczos kernel without allocation ---------------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot let a library call cudaMalloc
+ * -- a framework whose caching allocator already holds the device, or a service that fixed its memory
+ * plan at start-up; there a mid-run cudaMalloc can fail on a full pool, and it synchronises the device.
+ * Same recurrence as qb_lanczos, on buffers the caller owns:
+ *   v0    device complex128, sector dim (the start, not necessarily normalised; left untouched)
+ *   work  device scratch the caller owns: dim x (2 x element size of dtype + 16) bytes
+ *   alpha / beta  host outputs as for qb_lanczos (max_iter and max_iter + 1 values)
+ * Its own scratch (the alpha / beta history, reduction partials, a counter) is a file-scope device array
+ * of about 54 KB that every GPU which loads the library holds until exit; max_iter above
+ * QB_NOALLOC_MAX_ITER is refused (QB_EINVAL). The first call on a device resolves that array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture. Calls share the array and clear
+ * what must start at zero; calls that overlap on the GPU (two streams, two threads) race on it.
+ * reorth: QB_REORTH_NONE or QB_REORTH_LOCAL. */
+#define QB_NOALLOC_MAX_ITER 1024
+int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void* v0, void* work, int max_iter,
+                       int reorth, double breakdown_tol, int dtype, double* alpha, double* beta, int* iters,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

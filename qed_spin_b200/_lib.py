@@ -14,6 +14,7 @@ QB_OK, QB_EINVAL, QB_ENOMEM, QB_ECUDA, QB_EUNSUPPORTED, QB_ETIMEOUT, QB_ENODEV =
 QB_C128, QB_C64 = 0, 1
 QB_REORTH_NONE, QB_REORTH_FULL, QB_REORTH_LOCAL = 0, 1, 2
 QB_LOOKUP_AUTO, QB_LOOKUP_RANK, QB_LOOKUP_BUCKETS, QB_LOOKUP_HASH = 0, 1, 2, 3
+QB_NOALLOC_MAX_ITER = 1024
 
 #: every symbol include/qed_b200.h declares
 EXPORTS = [
@@ -22,7 +23,7 @@ EXPORTS = [
     "qb_sector_info", "qb_index_and_projection",
     "qb_program_create", "qb_program_destroy",
     "qb_matvec", "qb_matvec_block", "qb_matvec_host",
-    "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_cf",
+    "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_cf", "qb_lanczos_noalloc",
 ]
 
 
@@ -92,6 +93,7 @@ def lib():
     L.qb_eigs_lowest.argtypes = [vp, vp, i, i, i, C.POINTER(d), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]
     L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]
+    L.qb_lanczos_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i), vp]
     for name in EXPORTS:
         if name not in ("qb_last_error", "qb_sector_dim"):
             getattr(L, name).restype = i

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <vector>
@@ -939,6 +940,33 @@ ScanOut run_scan(Recurrence& R, int max_iter, int reorth, bool gate, double brea
 
 double norm_bound(const qb_program* p) { return p->norm_bound > 0.0 ? p->norm_bound : 1.0; }
 
+// ---- the allocation-free Lanczos (qb_lanczos_noalloc) ----
+// Its scratch -- the alpha / beta history, the local-projection overlap, the block partials of the
+// deterministic reductions and the last-block counter -- lives in this file-scope device array, held by
+// every GPU that loads the library until the process exits. Calls share it: two calls that overlap on the
+// GPU race on it.
+constexpr int kNoAllocMaxIter = QB_NOALLOC_MAX_ITER;
+constexpr std::size_t kNoAllocDoubles =
+    static_cast<std::size_t>(kNoAllocMaxIter) + (kNoAllocMaxIter + 1) + 2 + 4 * kMaxRedBlocks + 2;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// The device address of g_noalloc_scratch on the current device, resolved once per device (host code
+// cannot use the symbol's name as an address).
+double* noalloc_scratch() {
+    static std::mutex mu;
+    static std::vector<double*> per_device;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    if (per_device.size() <= static_cast<std::size_t>(dev)) per_device.resize(dev + 1, nullptr);
+    if (!per_device[dev]) {
+        void* ptr = nullptr;
+        cuda_check(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
+        per_device[dev] = static_cast<double*>(ptr);
+    }
+    return per_device[dev];
+}
+
 }  // namespace
 }  // namespace qb
 
@@ -1259,6 +1287,80 @@ int qb_cf(const qb_sector* sec, const qb_program* prog, const double* phi_host, 
                 std::abs(d) > 1e-300 ? std::complex<double>(norm_sq, 0.0) / d : std::complex<double>(0.0, 0.0);
             S[iw] = -G0.imag() / 3.14159265358979323846;
         }
+    });
+}
+
+
+// The Lanczos kernel on caller-owned device buffers, allocating nothing (see include/qed_b200.h).
+int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void* v0, void* work, int max_iter,
+                       int reorth, double breakdown_tol, int dtype, double* alpha, double* beta, int* iters,
+                       void* stream) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!sec || !prog || !v0 || !work || !alpha || !beta || !iters) throw Error(QB_EINVAL, "null argument");
+        if (reorth != QB_REORTH_NONE && reorth != QB_REORTH_LOCAL)
+            throw Error(QB_EUNSUPPORTED, "qb_lanczos_noalloc: reorth must be QB_REORTH_NONE or QB_REORTH_LOCAL");
+        if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "bad dtype");
+        if (max_iter < 0 || max_iter > kNoAllocMaxIter)
+            throw Error(QB_EINVAL, "qb_lanczos_noalloc: max_iter must be in [0, QB_NOALLOC_MAX_ITER = " +
+                                       std::to_string(kNoAllocMaxIter) + "]");
+        *iters = 0;
+        const std::uint64_t n = sec->dim;
+        if (max_iter == 0 || n == 0) return;
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        double* scratch = noalloc_scratch();
+        Scal S{scratch, scratch + kNoAllocMaxIter, scratch + 2 * kNoAllocMaxIter + 1,
+               scratch + 2 * kNoAllocMaxIter + 3, reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxIter + 3 + 4 * kMaxRedBlocks)};
+        // the array keeps the last call's contents: clear the beta history and the counter
+        cuda_check(cudaMemsetAsync(S.beta, 0, (kNoAllocMaxIter + 1) * sizeof(double), st), "scratch clear");
+        cuda_check(cudaMemsetAsync(S.counter, 0, sizeof(unsigned), st), "scratch clear");
+        const std::size_t es = dtype == QB_C64 ? 8 : 16;
+        unsigned char* wk = static_cast<unsigned char*>(work);
+        void* vb[2] = {wk, wk + n * es};
+        double2* w = reinterpret_cast<double2*>(wk + 2 * n * es);
+        cuda_check(cudaMemsetAsync(vb[0], 0, n * es, st), "work clear");
+        const int nb = red_blocks(n);
+        // v_0 = v0 / ||v0|| (v0 is FP64, untouched)
+        k_norm<<<nb, kThreads, 0, st>>>(n, static_cast<const double2*>(v0), S);
+        if (dtype == QB_C64)
+            k_scale_into<float2><<<nb, kThreads, 0, st>>>(n, static_cast<const double2*>(v0), static_cast<float2*>(vb[1]), S.ovl);
+        else
+            k_scale_into<double2><<<nb, kThreads, 0, st>>>(n, static_cast<const double2*>(v0), static_cast<double2*>(vb[1]), S.ovl);
+        cuda_check(cudaGetLastError(), "start");
+        double nrm = 0.0;
+        cuda_check(cudaMemcpyAsync(&nrm, S.ovl, 8, cudaMemcpyDeviceToHost, st), "norm read");
+        cuda_check(cudaStreamSynchronize(st), "start");
+        if (!(nrm > 0.0)) throw Error(QB_EINVAL, "qb_lanczos_noalloc: initial vector has non-positive norm");
+        const int cap = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(max_iter), n));
+        const int local = reorth == QB_REORTH_LOCAL;
+        int cur = 1;
+        for (int j = 0; j < cap; ++j) {
+            void* vc = vb[cur];
+            void* vp = vb[cur ^ 1];
+            launch_walk_mixed(sec, sec, prog, vc, w, dtype, QB_C128, st);
+            if (dtype == QB_C64) {
+                rec_alpha<float2><<<nb, kThreads, 0, st>>>(n, j, w, static_cast<float2*>(vp), static_cast<float2*>(vc), S);
+                rec_beta<float2><<<nb, kThreads, 0, st>>>(n, j, local, w, static_cast<float2*>(vc), S);
+                rec_next<float2><<<nb, kThreads, 0, st>>>(n, j, w, static_cast<float2*>(vc), static_cast<float2*>(vp), S);
+            } else {
+                rec_alpha<double2><<<nb, kThreads, 0, st>>>(n, j, w, static_cast<double2*>(vp), static_cast<double2*>(vc), S);
+                rec_beta<double2><<<nb, kThreads, 0, st>>>(n, j, local, w, static_cast<double2*>(vc), S);
+                rec_next<double2><<<nb, kThreads, 0, st>>>(n, j, w, static_cast<double2*>(vc), static_cast<double2*>(vp), S);
+            }
+            cuda_check(cudaGetLastError(), "recurrence");
+            cur ^= 1;
+        }
+        // straight into the caller's arrays (no staging buffer)
+        cuda_check(cudaMemcpyAsync(alpha, S.alpha, cap * 8, cudaMemcpyDeviceToHost, st), "alpha read");
+        cuda_check(cudaMemcpyAsync(beta, S.beta, (cap + 1) * 8, cudaMemcpyDeviceToHost, st), "beta read");
+        cuda_check(cudaStreamSynchronize(st), "lanczos");
+        int m = 0;
+        beta[0] = 0.0;
+        for (int j = 0; j < cap; ++j) {
+            ++m;
+            if (beta[j + 1] < breakdown_tol) break;
+        }
+        *iters = m;
     });
 }
 
