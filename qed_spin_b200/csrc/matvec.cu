@@ -78,37 +78,53 @@ __device__ __forceinline__ SmemProgram stage(const DProgram& P, const DSector& c
     return out;
 }
 
-// connection (include/ed/ops/row_walk.h:28-52): whether group g acts on s; its target and h.
-__device__ __forceinline__ bool connection(const DProgram& P, u64 s, u32 g, u64& t, cplx& h) {
-    const u64 F = P.group_flip[g];
-    const u64 v = s & F;
+template <class ST> __device__ __forceinline__ int popc(ST x);
+template <> __device__ __forceinline__ int popc<u64>(u64 x) { return __popcll(x); }
+template <> __device__ __forceinline__ int popc<u32>(u32 x) { return __popc(x); }
+
+// The value subgroup of group g that s meets, or -1 (include/ed/ops/row_walk.h:32-43).
+template <class ST> __device__ __forceinline__ int acting_subgroup(const DProgram& P, ST s, u32 g) {
+    const ST F = static_cast<ST>(P.group_flip[g]);
+    const ST v = s & F;
     const int sb = P.group_setbits[g];
-    if (sb >= 0 && __popcll(v) != sb) return false;
+    if (sb >= 0 && popc<ST>(v) != sb) return -1;
     u32 lo = P.group_vbegin[g], hi = P.group_vbegin[g + 1];
     const u32 end = hi;
     while (lo < hi) {
         const u32 mid = lo + ((hi - lo) >> 1);
-        if (P.vsub_val[mid] < v)
+        if (static_cast<ST>(P.vsub_val[mid]) < v)
             lo = mid + 1;
         else
             hi = mid;
     }
-    if (lo == end || P.vsub_val[lo] != v) return false;
-    h = {0.0, 0.0};
-    for (u32 k = P.vsub_tbegin[lo]; k < P.vsub_tbegin[lo + 1]; ++k) {
+    return (lo == end || static_cast<ST>(P.vsub_val[lo]) != v) ? -1 : static_cast<int>(lo);
+}
+
+// h = <s ^ F|O^dagger|s>: the subgroup's terms summed in key order with their signs (row_walk.h:44-50).
+template <class ST> __device__ __forceinline__ cplx subgroup_value(const DProgram& P, ST s, int vi) {
+    cplx h{0.0, 0.0};
+    for (u32 k = P.vsub_tbegin[vi]; k < P.vsub_tbegin[vi + 1]; ++k) {
         const double2 c = P.term_coeff[k];
-        if (__popcll(s & P.term_sign[k]) & 1)
+        if (popc<ST>(s & static_cast<ST>(P.term_sign[k])) & 1)
             h = cadd(h, {-c.x, -c.y});
         else
             h = cadd(h, {c.x, c.y});
     }
-    t = s ^ F;
+    return h;
+}
+
+// connection (include/ed/ops/row_walk.h:28-52): whether group g acts on s; its target and h.
+template <class ST> __device__ __forceinline__ bool connection(const DProgram& P, ST s, u32 g, ST& t, cplx& h) {
+    const int vi = acting_subgroup<ST>(P, s, g);
+    if (vi < 0) return false;
+    h = subgroup_value<ST>(P, s, vi);
+    t = s ^ static_cast<ST>(P.group_flip[g]);
     return true;
 }
 
 // The entry of one connection: column j and value c, or false when the target's orbit cancels.
-template <bool kSame>
-__device__ __forceinline__ bool entry(const DSector& col, const Tables& T, u64 s, long long r, double w, u64 t,
+template <bool kSame, class ST>
+__device__ __forceinline__ bool entry(const DSector& col, const Tables& T, ST s, long long r, double w, ST t,
                                       cplx h, long long& j, cplx& c) {
     if (kSame && t == s) {
         j = r;
@@ -116,7 +132,7 @@ __device__ __forceinline__ bool entry(const DSector& col, const Tables& T, u64 s
         return true;
     }
     double pre, pim;
-    j = index_and_projection(col, T, t, pre, pim);
+    j = index_and_projection<ST>(col, T, t, pre, pim);
     if (j < 0) return false;
     c = rscale(w, cconj(cmul(h, {pre, pim})));
     return true;
@@ -145,104 +161,44 @@ template <int NV> struct VecPtrs {
     void* out[NV];
 };
 
-// Resolve up to B connections of one row at once: every target's canonicalisation first, then all the
-// hash probes, so a thread keeps B independent loads in flight where the single-target walk kept one.
-// j[b] = -1 when connection b is absent or its orbit cancels in the column sector.
-template <int B, bool kSame>
-__device__ __forceinline__ void resolve_batch(const DSector& col, const Tables& T, u64 s, long long r, double w,
-                                              const u64 (&t)[B], const cplx (&h)[B], int nb, long long (&j)[B],
-                                              cplx (&c)[B]) {
-    if (col.lookup != 3) {
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            j[b] = -1;
-            if (b < nb && !entry<kSame>(col, T, s, r, w, t[b], h[b], j[b], c[b])) j[b] = -1;
-        }
-        return;
-    }
-    u64 rb[B];
-    double are[B], aim[B];
-    bool need[B];
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-        j[b] = -1;
-        need[b] = false;
-        if (b >= nb) continue;
-        if (kSame && t[b] == s) {
-            j[b] = r;
-            c[b] = cconj(h[b]);
-        } else if (__popcll(t[b]) == col.n_up) {
-            need[b] = true;
-            rb[b] = canonicalize(col, T, t[b], are[b], aim[b]);
-        }
-    }
-    const u64 mask = (1ULL << col.hash_bits) - 1ULL;
-    u64 slot[B];
-    ulonglong2 e[B];
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-        if (need[b]) {
-            slot[b] = hash_slot(rb[b], col.hash_bits);
-            e[b] = __ldg(col.slots + slot[b]);
-        }
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-        if (!need[b]) continue;
-        while (e[b].x != rb[b] && e[b].x != ~0ULL) {
-            slot[b] = (slot[b] + 1) & mask;
-            e[b] = __ldg(col.slots + slot[b]);
-        }
-        if (e[b].x != rb[b]) continue;   // the target's orbit cancels in this sector
-        const long long jj = static_cast<long long>(e[b].y & 0xFFFFFFFFULL);
-        const double sc = col.n_class ? T.inv_class[static_cast<int>(e[b].y >> 32)] : __ldg(col.inv_norms + jj);
-        j[b] = jj;
-        c[b] = rscale(w, cconj(cmul(h[b], {__dmul_rn(are[b], sc), __dmul_rn(aim[b], sc)})));
-    }
-}
-
-template <int NV, int B, bool kInF32, bool kOutF32, bool kSame>
-__global__ void __launch_bounds__(256, (B >= 4 ? 2 : (B == 2 ? 3 : 4))) walk_rows(DSector row, DSector col, DProgram P,
-                                                                                 bool prog_in_smem, VecPtrs<NV> io) {
+// One thread per row. The row's groups are tested 32 at a time by every lane together (a converged
+// pass that builds the bitmask of the groups acting on the lane's row); the lanes then walk their own
+// acting groups in ascending order -- the diagonal first -- canonicalising one target each per step.
+template <int NV, class ST, bool kInF32, bool kOutF32, bool kSame>
+__global__ void __launch_bounds__(256, 4) walk_rows(DSector row, DSector col, DProgram P, bool prog_in_smem,
+                                                    VecPtrs<NV> io) {
     extern __shared__ __align__(16) unsigned char smem[];
     using St = Store<kInF32>;
     using So = Store<kOutF32>;
     const SmemProgram sp = stage(P, col, smem, prog_in_smem);
     const std::uint64_t r = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = r < row.dim;
-    const u64 s = live ? __ldg(row.reps + r) : 0;
+    const ST s = live ? static_cast<ST>(__ldg(row.reps + r)) : static_cast<ST>(0);
     const double w = live ? __ldg(row.inv_norms + r) : 0.0;
     cplx acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = {0.0, 0.0};
-    u32 g = live ? 0u : sp.P.n_groups;
-    for (;;) {
-        u64 t[B];
-        cplx h[B];
-        int nb = 0;
+    const u32 ng = sp.P.n_groups;
+    for (u32 g0 = 0; g0 < ng; g0 += 32) {
+        const u32 gend = ng < g0 + 32 ? ng : g0 + 32;
+        u32 mask = 0;
+        if (live)
+            for (u32 g = g0; g < gend; ++g)
+                if (acting_subgroup<ST>(sp.P, s, g) >= 0) mask |= 1u << (g - g0);
+        while (__any_sync(0xffffffffu, mask != 0)) {
+            if (mask == 0) continue;
+            const u32 g = g0 + static_cast<u32>(__ffs(mask) - 1);
+            mask &= mask - 1;
+            const int vi = acting_subgroup<ST>(sp.P, s, g);
+            const cplx h = subgroup_value<ST>(sp.P, s, vi);
+            const ST t = s ^ static_cast<ST>(sp.P.group_flip[g]);
+            long long j;
+            cplx c;
+            if (!entry<kSame, ST>(col, sp.T, s, static_cast<long long>(r), w, t, h, j, c)) continue;
 #pragma unroll
-        for (int b = 0; b < B; ++b) {
-            bool have = false;
-            t[b] = 0;
-            h[b] = {0.0, 0.0};
-            while (!have && g < sp.P.n_groups) have = connection(sp.P, s, g++, t[b], h[b]);
-            if (have) nb = b + 1;
+            for (int v = 0; v < NV; ++v)
+                acc[v] = cadd(acc[v], cmul(c, St::load(static_cast<const typename St::T*>(io.in[v]), static_cast<std::size_t>(j))));
         }
-        if (!__any_sync(0xffffffffu, nb > 0)) break;
-        long long j[B];
-        cplx c[B];
-        resolve_batch<B, kSame>(col, sp.T, s, static_cast<long long>(r), w, t, h, nb, j, c);
-        cplx xv[B][NV];
-#pragma unroll
-        for (int b = 0; b < B; ++b)
-            if (j[b] >= 0)
-#pragma unroll
-                for (int v = 0; v < NV; ++v)
-                    xv[b][v] = St::load(static_cast<const typename St::T*>(io.in[v]), static_cast<std::size_t>(j[b]));
-#pragma unroll
-        for (int b = 0; b < B; ++b)
-            if (j[b] >= 0)
-#pragma unroll
-                for (int v = 0; v < NV; ++v) acc[v] = cadd(acc[v], cmul(c[b], xv[b][v]));
     }
     if (!live) return;
 #pragma unroll
@@ -279,8 +235,8 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
         cplx h{0.0, 0.0};
         long long j = -1;
         cplx cv{0.0, 0.0};
-        bool act = live && g < sp.P.n_groups && connection(sp.P, s, g, t, h);
-        if (act) act = entry<kSame>(col, sp.T, s, static_cast<long long>(r), w, t, h, j, cv);
+        bool act = live && g < sp.P.n_groups && connection<u64>(sp.P, s, g, t, h);
+        if (act) act = entry<kSame, u64>(col, sp.T, s, static_cast<long long>(r), w, t, h, j, cv);
         unsigned acting = __ballot_sync(0xffffffffu, act) & team_mask;
         while (acting) {
             const int src = __ffs(acting) - 1;
@@ -312,29 +268,18 @@ template <class K> void set_smem(K kernel, std::size_t bytes) {
                    "smem attribute");
 }
 
-// Targets resolved together per thread in walk_rows (1, 2 or 4): QB_WALK_BATCH, default 1 (measured on
-// B200: batches of 2 and 4 ran 2x and 5x slower, their register pressure outweighing the extra loads in flight).
-int walk_batch() {
-    static int b = [] {
-        const char* e = std::getenv("QB_WALK_BATCH");
-        const int v = e ? std::atoi(e) : 1;
-        return v >= 4 ? 4 : (v >= 2 ? 2 : 1);
-    }();
-    return b;
-}
-
-template <int NV, int B, bool kF32, bool kOutF32>
-void launch_rows_b(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
-                   cudaStream_t st) {
+template <int NV, class ST, bool kF32, bool kOutF32>
+void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
+                    cudaStream_t st) {
     bool in_smem = false;
     const std::size_t smem = smem_for(P, col, in_smem);
     const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
     if (row == col) {
-        auto k = walk_rows<NV, B, kF32, kOutF32, true>;
+        auto k = walk_rows<NV, ST, kF32, kOutF32, true>;
         set_smem(k, smem);
         k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
     } else {
-        auto k = walk_rows<NV, B, kF32, kOutF32, false>;
+        auto k = walk_rows<NV, ST, kF32, kOutF32, false>;
         set_smem(k, smem);
         k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
     }
@@ -349,19 +294,11 @@ void launch_rows_nv(const qb_sector* row, const qb_sector* col, const qb_program
         io.in[v] = ins[v];
         io.out[v] = outs[v];
     }
-    if constexpr (NV == 1) {
-        const int b = walk_batch();
-        if (b == 4)
-            launch_rows_b<1, 4, kF32, kOutF32>(row, col, P, io, st);
-        else if (b == 2)
-            launch_rows_b<1, 2, kF32, kOutF32>(row, col, P, io, st);
-        else
-            launch_rows_b<1, 1, kF32, kOutF32>(row, col, P, io, st);
-    } else if constexpr (NV == 2) {
-        launch_rows_b<2, 2, kF32, kOutF32>(row, col, P, io, st);
-    } else {
-        launch_rows_b<NV, 1, kF32, kOutF32>(row, col, P, io, st);
-    }
+    // 32-bit states when every state fits
+    if (row->N <= 32 && col->N <= 32)
+        launch_rows_st<NV, u32, kF32, kOutF32>(row, col, P, io, st);
+    else
+        launch_rows_st<NV, u64, kF32, kOutF32>(row, col, P, io, st);
 }
 
 template <int kCpl, bool kF32, bool kOutF32>

@@ -26,51 +26,67 @@ struct Tables {
     const u64* pack;          // the sublattice leading-block table when small enough to stage
 };
 
+// States travel as ST: 32-bit for N <= 32 (half the integer instructions of 64-bit shifts, masks and
+// compares), 64-bit otherwise.
+template <class ST> struct StateOps;
+template <> struct StateOps<u64> {
+    __device__ static u64 brev(u64 s) { return __brevll(s); }
+    static constexpr int kBits = 64;
+};
+template <> struct StateOps<u32> {
+    __device__ static u32 brev(u32 s) { return __brev(s); }
+    static constexpr int kBits = 32;
+};
+
+template <class ST> __device__ __forceinline__ ST full_mask(int N) {
+    return N == StateOps<ST>::kBits ? static_cast<ST>(~static_cast<ST>(0)) : static_cast<ST>((static_cast<ST>(1) << N) - 1);
+}
+
 // Image of s under element g (include/ed/basis/compiled_group.h:73-78): new bit i = old bit perm[i], then
 // XOR the flip mask. Chains and tori act by rotations, a reversal, and row rotations; any other group
 // through its byte tables.
-__device__ __forceinline__ u64 apply_elem(const DSector& S, const Tables& T, u64 s, int g) {
+template <class ST>
+__device__ __forceinline__ ST apply_elem(const DSector& S, const Tables& T, ST s, int g) {
     if (S.gkind != 0) {
         const u64 d = T.edesc[g];
         const int kind = static_cast<int>(d & 0xFF);
         const int c = static_cast<int>((d >> 8) & 0xFF);
         const int N = S.N;
-        const u64 full = N == 64 ? ~0ULL : ((1ULL << N) - 1ULL);
-        if (kind == kElemRefl) s = __brevll(s) >> (64 - N);
+        const ST full = full_mask<ST>(N);
+        if (kind == kElemRefl) s = StateOps<ST>::brev(s) >> (StateOps<ST>::kBits - N);
         if (c) s = ((s >> c) | (s << (N - c))) & full;
         if (kind == kElemTorus) {
             const int a = static_cast<int>((d >> 16) & 0xFF);
             if (a) {
-                const u64 lo = T.emask[g];
-                s = ((s >> a) & lo) | ((s << (S.Lx - a)) & ~lo & full);
+                const ST lo = static_cast<ST>(T.emask[g]);
+                s = ((s >> a) & lo) | ((s << (S.Lx - a)) & static_cast<ST>(~lo) & full);
             }
         }
-        return s ^ T.flips[g];
+        return s ^ static_cast<ST>(T.flips[g]);
     }
     const u64* l = S.lut + static_cast<std::size_t>(g) * S.bpw * 256;
-    u64 r = 0;
+    ST r = 0;
 #pragma unroll 8
-    for (int b = 0; b < S.bpw; ++b) r |= __ldg(l + b * 256 + static_cast<int>((s >> (8 * b)) & 0xFFu));
-    return r ^ T.flips[g];
+    for (int b = 0; b < S.bpw; ++b) r |= static_cast<ST>(__ldg(l + b * 256 + static_cast<int>((s >> (8 * b)) & 0xFFu)));
+    return r ^ static_cast<ST>(T.flips[g]);
 }
 
 // A state's bits moved to their key positions.
-__device__ __forceinline__ u64 key_of(const u64* to_key, int bpw, u64 s) {
-    u64 k = 0;
+template <class ST> __device__ __forceinline__ ST key_of(const u64* to_key, int bpw, ST s) {
+    ST k = 0;
 #pragma unroll 8
-    for (int b = 0; b < bpw; ++b) k |= to_key[(b << 8) + static_cast<int>((s >> (8 * b)) & 0xFFu)];
+    for (int b = 0; b < bpw; ++b) k |= static_cast<ST>(to_key[(b << 8) + static_cast<int>((s >> (8 * b)) & 0xFFu)]);
     return k;
 }
 
-__device__ __forceinline__ u32 pattern_of(u64 k, int j, int N, int L) {
+template <class ST> __device__ __forceinline__ u32 pattern_of(ST k, int j, int N, int L) {
     return static_cast<u32>(k >> (N - (j + 1) * L)) & ((1u << L) - 1u);
 }
 
 // The several-blocks case of for_each_candidate: merge the ascending candidate lists of every block that
-// reaches the least leading block (each element maps exactly one block to the lead). Rare; kept out of
-// line so the common path holds no local arrays.
-template <class Fn>
-__device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pack, u64 k, u32 best, Fn& fn) {
+// reaches the least leading block (each element maps exactly one block to the lead).
+template <class ST, class Fn>
+__device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pack, ST k, u32 best, Fn& fn) {
     const int L = S.slc.L, m = S.slc.m, N = S.N;
     u64 sel[8];
     u32 pos[8];
@@ -104,8 +120,8 @@ __device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pa
 
 // fn(g) in ascending order for the elements whose image has the least leading block
 // (sublattice_code.h:102-131); returns that least leading block. One packed load per block.
-template <class Fn>
-__device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* pack, u64 k, Fn&& fn) {
+template <class ST, class Fn>
+__device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* pack, ST k, Fn&& fn) {
     const int L = S.slc.L, m = S.slc.m, N = S.N;
     u32 best = 0xFFFFFFFFu;
     u64 first = 0;
@@ -136,14 +152,14 @@ __device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* p
 }
 
 // Representative of t and the conjugated character sum over the elements that reach it.
-__device__ __forceinline__ u64 canonicalize(const DSector& S, const Tables& T, u64 t, double& acc_re,
-                                            double& acc_im) {
-    u64 rb = ~0ULL, best = ~0ULL;
+template <class ST>
+__device__ __forceinline__ ST canonicalize(const DSector& S, const Tables& T, ST t, double& acc_re, double& acc_im) {
+    ST rb = static_cast<ST>(~static_cast<ST>(0)), best = static_cast<ST>(~static_cast<ST>(0));
     acc_re = 0.0;
     acc_im = 0.0;
     auto visit = [&](int g) {
-        const u64 img = apply_elem(S, T, t, g);
-        const u64 k = S.slc.on ? key_of(T.to_key, S.bpw, img) : img;
+        const ST img = apply_elem<ST>(S, T, t, g);
+        const ST k = S.slc.on ? key_of<ST>(T.to_key, S.bpw, img) : img;
         if (k < best) {
             best = k;
             rb = img;
@@ -157,7 +173,7 @@ __device__ __forceinline__ u64 canonicalize(const DSector& S, const Tables& T, u
         }
     };
     if (S.slc.on) {
-        for_each_candidate(S, T.pack, key_of(T.to_key, S.bpw, t), visit);
+        for_each_candidate<ST>(S, T.pack, key_of<ST>(T.to_key, S.bpw, t), visit);
     } else {
         for (int g = 0; g < S.G; ++g) visit(g);
     }
@@ -229,11 +245,12 @@ __device__ __forceinline__ long long index_of_rep(const DSector& S, u64 rb) {
 }
 
 // index_and_projection: index of t's orbit in S (or -1) and conj(beta_t) * inv_norm[index].
-__device__ __forceinline__ long long index_and_projection(const DSector& S, const Tables& T, u64 t, double& pre,
+template <class ST = u64>
+__device__ __forceinline__ long long index_and_projection(const DSector& S, const Tables& T, ST t, double& pre,
                                                           double& pim) {
-    if (__popcll(t) != S.n_up) return -1;
+    if (__popcll(static_cast<u64>(t)) != S.n_up) return -1;
     double are, aim;
-    const u64 rb = canonicalize(S, T, t, are, aim);
+    const u64 rb = static_cast<u64>(canonicalize<ST>(S, T, t, are, aim));
     long long j;
     double s;
     if (S.lookup == 3) {

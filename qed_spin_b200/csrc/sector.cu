@@ -242,19 +242,19 @@ __device__ __forceinline__ double visit_inv_norm(const DSector& S, const Tables&
     double sre = 0.0, sim = 0.0;
     int cnt = 0;
     if (S.slc.on) {
-        const u64 k = key_of(T.to_key, S.bpw, s);
+        const u64 k = key_of<u64>(T.to_key, S.bpw, s);
         // the least leading block over the blocks vs the state's own (visit_state's early exit)
         u32 least = 0xFFFFFFFFu;
         for (int j = 0; j < S.slc.m; ++j) {
-            const u32 v = static_cast<u32>(T.pack[(static_cast<u32>(j) << S.slc.L) + pattern_of(k, j, S.N, S.slc.L)] &
+            const u32 v = static_cast<u32>(T.pack[(static_cast<u32>(j) << S.slc.L) + pattern_of<u64>(k, j, S.N, S.slc.L)] &
                                            0xFFFFu);
             least = v < least ? v : least;
         }
-        if (least < pattern_of(k, 0, S.N, S.slc.L)) return 0.0;
+        if (least < pattern_of<u64>(k, 0, S.N, S.slc.L)) return 0.0;
         bool rep = true;
-        for_each_candidate(S, T.pack, k, [&](int g) {
+        for_each_candidate<u64>(S, T.pack, k, [&](int g) {
             if (!rep) return;
-            const u64 ik = key_of(T.to_key, S.bpw, apply_elem(S, T, s, g));
+            const u64 ik = key_of<u64>(T.to_key, S.bpw, apply_elem<u64>(S, T, s, g));
             if (ik < k) {
                 rep = false;
             } else if (ik == k) {
@@ -267,7 +267,7 @@ __device__ __forceinline__ double visit_inv_norm(const DSector& S, const Tables&
         if (!rep) return 0.0;
     } else {
         for (int g = 0; g < S.G; ++g) {
-            const u64 img = apply_elem(S, T, s, g);
+            const u64 img = apply_elem<u64>(S, T, s, g);
             if (img < s) return 0.0;
             if (img == s) {
                 const double2 c = T.chars[g];
