@@ -3,14 +3,16 @@
 Workload: the periodic XXZ chain N = 32 (J = 1, Delta = 0.7) in the sector S^z = 0, k = 0, reflection-even,
 spin-flip-even (group D_32 x Z_2, 128 elements; 4,707,969 representatives found on the device). Synthetic
 input: a seeded complex Gaussian vector. One step = one H.v on device-resident vectors with FP32 storage
-(FP64 arithmetic); the FP64-storage matvec and time-to-E0 (FP64 plain vs FP32 storage + FP64 refinement)
-are reported beside it.
+(FP64 arithmetic) through the lane the engine picks for a sector whose merged CSR fits the device: the
+reduced CSR, built once on the device from the row walk (its build time is reported). The on-the-fly walk,
+the FP64-storage applies and time-to-E0 (FP64 plain vs FP32 storage + FP64 refinement) are reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the path has no
 cross-GPU exchange, so the metric is the sum over replicas and the time the max over ranks.
-`--impl reference` times the reference engine's own CPU matvec (oracle/_ref) on the host cores.
+`--impl reference` times the reference engine's own CPU matvec (oracle/_ref) on the host cores: its
+default host lane, the merged reduced CSR (built once, outside the timed region) and its OpenMP spmv.
 """
 from __future__ import annotations
 
@@ -139,63 +141,81 @@ def barrier(world):
         dist.barrier()
 
 
+def _reference_lane(threads):
+    """The reference engine on the workload: its sector, its row program and its merged reduced CSR (the
+    host lane RepSectorMatVec applies through), with the build times."""
+    from oracle import ref as R
+    spec, prog, prods = workload()
+    R.set_threads(threads)
+    t0 = time.time()
+    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+    sector_s = time.time() - t0
+    rp = R.Operator(spec.n_sites, prods).row_program()
+    t0 = time.time()
+    csr = R.Csr(rs, rp)
+    csr_s = time.time() - t0
+    return rs, rp, csr, sector_s, csr_s
+
+
 def run_reference(args, world, rank):
-    """The reference engine's own CPU matvec (oracle/_ref) on the host cores: H.v/s on the same workload."""
+    """The reference engine's own CPU matvec (oracle/_ref) on the host cores: H.v/s on the same workload,
+    through its default host lane (ReducedSymmetryCsr::spmv over the CSR build_sector_csr made)."""
     if rank != 0:
         return None
     from oracle import ref as R
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU engine was not built into oracle/_ref"}))
         return None
-    spec, prog, prods = workload()
     threads = os.cpu_count() or 1
-    R.set_threads(threads)
-    t0 = time.time()
-    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
-    build_s = time.time() - t0
-    rp = R.Operator(spec.n_sites, prods).row_program()
+    rs, rp, csr, sector_s, csr_s = _reference_lane(threads)
     x = R.staged_seed(1, rs.dim)
+    y = np.zeros(rs.dim, np.complex128)
     for _ in range(args.warmup):
-        rs.gather(rp, x)
+        csr.spmv(x, y)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        rs.gather(rp, x)
+        csr.spmv(x, y)
         times.append(time.perf_counter() - t)
     tot = sum(times)
     v = args.steps / tot
     line = {"impl": "reference", "metric": "H.v/s", "value": v, "unit": "H.v/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CONFIG, dim=rs.dim, lane="sector_gather (host walk, OpenMP)"),
+            "config": dict(CONFIG, dim=rs.dim, nnz=csr.nnz, csr_bytes=csr.bytes,
+                           lane="reduced CSR (build_sector_csr + ReducedSymmetryCsr::spmv, OpenMP)"),
             "cpu_baseline": {"value": v, "unit": "H.v/s", "cores": threads, "kind": "reference",
                              "sample": f"{args.steps} full H.v on the {rs.dim}-state sector"},
             "e2e": {"value": v, "unit": "H.v/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_sector_build_s": build_s}
+            "reference_sector_build_s": sector_s, "reference_csr_build_s": csr_s}
     print(json.dumps(line))
     return line
 
 
 def cpu_baseline_sample(dim_gpu):
-    """The reference engine's CPU matvec on a bounded sample: a few full H.v on the host cores."""
+    """The reference engine's CPU matvec on a bounded sample: full H.v through its reduced CSR for about
+    10 s, plus a few through its on-the-fly host walk (sector_gather)."""
     from oracle import ref as R
     if not R.available():
         return None
-    spec, prog, prods = workload()
     threads = os.cpu_count() or 1
-    R.set_threads(threads)
-    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+    rs, rp, csr, sector_s, csr_s = _reference_lane(threads)
     assert rs.dim == dim_gpu
-    rp = R.Operator(spec.n_sites, prods).row_program()
     x = R.staged_seed(1, rs.dim)
-    rs.gather(rp, x)
+    y = np.zeros(rs.dim, np.complex128)
+    csr.spmv(x, y)
     n, t0 = 0, time.perf_counter()
-    while n < 3 or (time.perf_counter() - t0 < 10.0 and n < 20):
-        rs.gather(rp, x)
+    while n < 3 or (time.perf_counter() - t0 < 10.0 and n < 200):
+        csr.spmv(x, y)
         n += 1
     dt = time.perf_counter() - t0
+    t = time.perf_counter()
+    rs.gather(rp, x)
+    walk_s = time.perf_counter() - t
     return {"value": n / dt, "unit": "H.v/s", "cores": threads, "kind": "reference",
-            "sample": f"{n} full H.v (sector_gather, the reference's host walk) on the {rs.dim}-state sector"}
+            "sample": f"{n} full H.v through the reference's reduced CSR (its default host lane) on the "
+                      f"{rs.dim}-state sector",
+            "csr_build_s": csr_s, "sector_build_s": sector_s, "walk_hv_per_s": 1.0 / walk_s}
 
 
 def main():
@@ -205,12 +225,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e0-6x6", action="store_true",
+                    help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
+                         "(FP64, and FP32 storage + FP64 refinement), one JSON line")
     ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36"], default=None,
                     help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing")
+    ap.add_argument("--profile-lane", choices=["walk", "csr"], default="walk",
+                    help="the lane of the profiling run: the on-the-fly walk or the device reduced CSR")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         profile_case(args)
+        return
+    if args.e0_6x6:
+        e0_6x6(args)
         return
 
     world, rank, local = dist_init() if args.impl == "b200" else (int(os.environ.get("WORLD_SIZE", "1")),
@@ -237,18 +265,15 @@ def main():
     n = S.dim
     info = S.info()
 
-    # algorithmic bytes per H.v (8 rep + 8 inv_norm + S_out per row, S_in per emitted entry)
     rng = np.random.default_rng(1)
     x64 = torch.from_numpy(rng.normal(size=n) + 1j * rng.normal(size=n)).to(dev)
     x32 = x64.to(torch.complex64)
     y32 = torch.empty_like(x32)
     y64 = torch.empty_like(x64)
     e_bar = emitted_per_row(S.reps()[0], prog)
+    hbm, peak_kind = peaks()
 
-    def b_alg(S_bytes):
-        return n * (8 + 8 + S_bytes) + n * e_bar * S_bytes
-
-    def time_matvec(x, y, dt, steps, warm):
+    def time_apply(x, y, dt, steps, warm):
         for _ in range(warm):
             D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
         torch.cuda.synchronize()
@@ -263,16 +288,40 @@ def main():
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
         barrier(world)
-        return dist_max(ms, world)
+        return dist_max(ms, world) / steps
+
+    # the on-the-fly walk: 8 rep + 8 inv_norm + S_out per row, S_in per emitted entry
+    def walk_bytes(sb):
+        return n * (8 + 8 + sb) + n * e_bar * sb
+
+    walk_steps = max(5, args.steps // 10)
+    walk32 = time_apply(x32, y32, "c64", walk_steps, 3)
+    walk64 = time_apply(x64, y64, "c128", walk_steps, 3)
+
+    # time to E0 on the plain FP64 lane (the walk), before the CSR exists
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r_plain = D.eigs_lowest(S, P, dtype="c128")
+    t_plain = time.perf_counter() - t
+
+    # the reduced CSR, built on the device from the walk, attached to the program
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    A = D.Csr(S, S, P)
+    torch.cuda.synchronize()
+    csr_build_s = time.perf_counter() - t
+    A.attach(P)
+    cinfo = A.info()
+
+    # the CSR matvec: the CSR streamed once, x read (each element at least once) and y written
+    def csr_bytes(sb):
+        return cinfo["bytes"] + 2 * n * sb
 
     with Clocks(dev) as clk:
-        ms32 = time_matvec(x32, y32, "c64", args.steps, args.warmup)
-    ms64 = time_matvec(x64, y64, "c128", max(10, args.steps // 2), 3)
-    per32 = ms32 / args.steps
-    per64 = ms64 / max(10, args.steps // 2)
-    hbm, peak_kind = peaks()
-    ach32 = b_alg(8) / (per32 * 1e-3) / 1e9
-    ach64 = b_alg(16) / (per64 * 1e-3) / 1e9
+        per32 = time_apply(x32, y32, "c64", args.steps, args.warmup)
+    per64 = time_apply(x64, y64, "c128", max(10, args.steps // 2), 3)
+    ach32 = csr_bytes(8) / (per32 * 1e-3) / 1e9
+    ach64 = csr_bytes(16) / (per64 * 1e-3) / 1e9
 
     # end to end through the public C-ABI: host start vector in, alpha/beta out, K Lanczos steps
     v0 = (rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex128)
@@ -284,7 +333,7 @@ def main():
     e2e_s = time.perf_counter() - t
     e2e_s = dist_max(e2e_s, world)
 
-    # time to E0: FP64 plain lane vs FP32 storage + FP64 refinement
+    # time to E0 on the CSR lane: FP64 storage, and FP32 storage + FP64 refinement
     torch.cuda.synchronize()
     t = time.perf_counter()
     r64 = D.eigs_lowest(S, P, dtype="c128")
@@ -302,30 +351,116 @@ def main():
 
     if rank != 0:
         return
-    value = world * args.steps / (ms32 * 1e-3)
+    value = world * 1e3 / per32
     line = {
         "metric": "H.v/s", "value": value, "unit": "H.v/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per32, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(CONFIG, dim=n, emitted_per_row=e_bar, storage="complex64 vectors, FP64 arithmetic",
-                       lookup=info["lookup"], sublattice=[info["slc_L"], info["slc_m"]],
-                       l2="working set > 126 MB L2 (reps, inv_norms, x, y, lookup ~0.2 GB), no flush",
+        "config": dict(CONFIG, dim=n, lane="device reduced CSR (built from the row walk)", nnz=cinfo["nnz"],
+                       csr_bytes=cinfo["bytes"], n_dict=cinfo["n_dict"], emitted_per_row=e_bar,
+                       storage="complex64 vectors, FP64 arithmetic", lookup=info["lookup"],
+                       sublattice=[info["slc_L"], info["slc_m"]],
+                       l2=f"inputs larger than the 126 MB L2 (CSR {cinfo['bytes'] / 1e6:.0f} MB streamed per step), "
+                          "no flush",
                        parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": hbm, "unit": "GB/s", "frac": ach32 / hbm,
-                     "traffic": None, "peak_kind": peak_kind,
-                     "alg_bytes_per_launch": b_alg(8)},
+                     "traffic": None, "peak_kind": peak_kind, "kernel": "spmv1<complex64>",
+                     "alg_bytes_per_launch": csr_bytes(8)},
         "fp64": {"ms_per_hv": per64, "hv_per_s": 1e3 / per64, "achieved_gbs": ach64, "frac": ach64 / hbm},
+        "csr_build_s": csr_build_s,
+        "walk": {"ms_per_hv_fp32": walk32, "hv_per_s_fp32": 1e3 / walk32, "ms_per_hv_fp64": walk64,
+                 "achieved_gbs_fp32": walk_bytes(8) / (walk32 * 1e-3) / 1e9,
+                 "frac_fp32": walk_bytes(8) / (walk32 * 1e-3) / 1e9 / hbm},
         "e2e": {"value": world * args.steps / e2e_s, "unit": "H.v/s", "h2d_bytes_per_step": 16 * n / args.steps,
-                "d2h_bytes_per_step": 16, "path": "qb_lanczos (host v0 in, alpha/beta out, FP32 storage)"},
-        "time_to_e0": {"fp64_s": t64, "fp64_e0": r64["e0"], "fp64_iters": r64["iters"],
-                       "fp32_refined_s": t32, "fp32_refined_e0": r32["e0"], "fp32_matvecs": r32["matvecs"],
-                       "rel_err": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]), "speedup": t64 / t32},
+                "d2h_bytes_per_step": 16, "path": "qb_lanczos (host v0 in, alpha/beta out, FP32 storage, CSR lane)"},
+        "time_to_e0": {"plain_fp64_walk_s": t_plain, "plain_e0": r_plain["e0"], "plain_iters": r_plain["iters"],
+                       "csr_build_s": csr_build_s,
+                       "csr_fp64_s": t64, "csr_fp64_e0": r64["e0"],
+                       "csr_fp32_refined_s": t32, "csr_fp32_refined_e0": r32["e0"], "fp32_matvecs": r32["matvecs"],
+                       "rel_err_vs_plain": abs(r32["e0"] - r_plain["e0"]) / abs(r_plain["e0"]),
+                       "speedup_vs_plain_incl_build": t_plain / (t32 + csr_build_s)},
         "enumeration_s": enum_s,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
+    A.close()
+
+
+def e0_6x6(args):
+    """Time to E0 on the 6x6 periodic J1-J2 lattice (J1 = 1, J2 = 0.5), S^z = 0, momentum (0, 0) under the 36
+    translations (252,091,362 representatives): the plain FP64 lane (the on-the-fly walk, no CSR) against the
+    device reduced CSR with FP64 storage and with FP32 storage + FP64 refinement; the CSR build is counted."""
+    import torch
+
+    from qed_spin_b200 import build
+    from qed_spin_b200 import device as D
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    build.build()
+    nn, nnn = lat.square_j1j2_bonds(6, 6)
+    spec = lat.square_k0_sector(6, 6, 18)
+    prog = ops.row_program(ops.from_products(36, ops.heisenberg_products(nn, 1.0) + ops.heisenberg_products(nnn, 0.5)))
+    t = time.perf_counter()
+    S = D.Sector(spec)
+    torch.cuda.synchronize()
+    enum_s = time.perf_counter() - t
+    P = D.Program(prog)
+    n = S.dim
+    out = {"workload": "6x6 J1-J2 (J2/J1 = 0.5) Sz=0 k=(0,0), translations only", "dim": n, "enumeration_s": enum_s}
+    stream = torch.cuda.current_stream()
+
+    def per_apply(dt, steps):
+        x = torch.randn(n, dtype=torch.complex64 if dt == "c64" else torch.complex128, device="cuda")
+        y = torch.empty_like(x)
+        D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
+        torch.cuda.synchronize()
+        e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0_.record(stream)
+        for _ in range(steps):
+            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
+        e1_.record(stream)
+        torch.cuda.synchronize()
+        del x, y
+        return e0_.elapsed_time(e1_) / steps
+
+    out["walk_ms_per_hv_fp64"] = per_apply("c128", 2)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r = D.eigs_lowest(S, P, dtype="c128")
+    out["plain_fp64_walk"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
+                              "matvecs": r["matvecs"], "converged": r["converged"]}
+    t = time.perf_counter()
+    A = D.Csr(S, S, P)
+    torch.cuda.synchronize()
+    out["csr_build_s"] = time.perf_counter() - t
+    out["csr"] = A.info()
+    A.attach(P)
+    out["csr_ms_per_hv_fp32"] = per_apply("c64", 5)
+    out["csr_ms_per_hv_fp64"] = per_apply("c128", 5)
+    hbm, kind = peaks()
+    for dt, sb in (("fp32", 8), ("fp64", 16)):
+        ms = out[f"csr_ms_per_hv_{dt}"]
+        alg = out["csr"]["bytes"] + 2 * n * sb
+        # each x load fetches a whole 32-byte DRAM sector when x is far larger than L2
+        sectors = out["csr"]["bytes"] + out["csr"]["nnz"] * 32 + n * sb
+        out[f"roofline_{dt}"] = {"alg_bytes": alg, "alg_frac": alg / (ms * 1e-3) / 1e9 / hbm,
+                                 "sector_bytes_model": sectors, "sector_frac": sectors / (ms * 1e-3) / 1e9 / hbm,
+                                 "peak_gbs": hbm, "peak_kind": kind}
+    t = time.perf_counter()
+    r = D.eigs_lowest(S, P, dtype="c128")
+    out["csr_fp64"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"], "matvecs": r["matvecs"]}
+    t = time.perf_counter()
+    r = D.eigs_lowest(S, P, dtype="c64", refine=True)
+    out["csr_fp32_refined"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
+                               "matvecs": r["matvecs"], "converged": r["converged"]}
+    e_ref = out["plain_fp64_walk"]["e0"]
+    out["rel_err_fp32_refined_vs_plain"] = abs(out["csr_fp32_refined"]["e0"] - e_ref) / abs(e_ref)
+    out["speedup_fp32_refined_incl_build_vs_plain"] = out["plain_fp64_walk"]["s"] / (out["csr_fp32_refined"]["s"]
+                                                                                      + out["csr_build_s"])
+    print(json.dumps(out))
+    A.close()
 
 
 def profile_case(args):
@@ -348,6 +483,10 @@ def profile_case(args):
                                                  + ops.heisenberg_products(nnn, 0.5)))
     S = D.Sector(spec)
     P = D.Program(prog)
+    A = None
+    if args.profile_lane == "csr":
+        A = D.Csr(S, S, P)
+        A.attach(P)
     x = torch.randn(S.dim, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
     for _ in range(args.warmup):
@@ -357,8 +496,9 @@ def profile_case(args):
     for _ in range(args.steps):
         D.matvec(S, S, P, [x], [y], dtype="c64")
     torch.cuda.synchronize()
-    print(json.dumps({"profile_case": args.profile_case, "dim": S.dim, "ms_per_matvec": (time.perf_counter() - t)
-                      / args.steps * 1e3, "sector": S.info()}))
+    print(json.dumps({"profile_case": args.profile_case, "lane": args.profile_lane, "dim": S.dim,
+                      "ms_per_matvec": (time.perf_counter() - t) / args.steps * 1e3, "sector": S.info(),
+                      "csr": A.info() if A is not None else None}))
 
 
 def emitted_per_row(reps: np.ndarray, prog) -> float:

@@ -126,6 +126,41 @@ int qb_matvec_block(const qb_sector* row, const qb_sector* col, const qb_program
 int qb_matvec_host(const qb_sector* row, const qb_sector* col, const qb_program* prog, const double* in_host,
                    double* out_host);
 
+/* ---- the reduced-CSR lane ------------------------------------------------------------------
+ * The merged rows of an operator between two sectors, built once and streamed: columns ascending,
+ * equal columns summed in emission order, exact zeros dropped (build_sector_csr / build_cross_csr,
+ * include/ed/matvec/sector_rows.h:147-404). Values are stored as u8 or u16 ids into a dictionary of the
+ * distinct values when that is the smaller form (ReducedSymmetryCsr, include/ed/matvec/reduced_csr.h:36-75),
+ * else whole. */
+typedef struct qb_csr qb_csr;
+/* Built on the device from the row walk (build_sector_csr_gpu, include/ed/gpu/rep_matvec.h:78-85).
+ * QB_ENOMEM when it would take more than max_bytes (0: no budget) or the device's free memory (the
+ * reference returns null there); QB_EUNSUPPORTED when a row has more than 256 entries before merging or
+ * the column sector has 2^32 states or more. */
+int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* prog, uint64_t max_bytes,
+                 qb_csr** out);
+/* A CSR built on the host (row_ptr: row->dim + 1 entries; col_idx, val: row_ptr[dim] entries, val
+ * interleaved complex128), uploaded as is (upload_csr_gpu, include/ed/gpu/rep_matvec.h:87-91). */
+int qb_csr_upload(const qb_sector* row, const qb_sector* col, const uint64_t* row_ptr, const uint32_t* col_idx,
+                  const double* val, uint64_t max_bytes, qb_csr** out);
+int qb_csr_destroy(qb_csr* csr);
+/* nnz, device bytes, and the dictionary size (-1: values stored whole) (device_csr_info,
+ * include/ed/gpu/rep_matvec.h:98). Any output may be NULL. */
+int qb_csr_info(const qb_csr* csr, uint64_t* nnz, uint64_t* bytes, int* n_dict);
+/* The entries copied to host arrays (download_csr, include/ed/gpu/rep_matvec.h:100-101): row_ptr
+ * (rows + 1), col (nnz), val (2 * nnz doubles). Any output may be NULL. */
+int qb_csr_download(const qb_csr* csr, uint64_t* row_ptr, uint32_t* col, double* val);
+/* out = A in on k vectors (k == 1: one vector; k <= 64: interleaved by row) of dtype, device pointers
+ * (csr_matvec_gpu / csr_matvec_gpu_multi, include/ed/gpu/rep_matvec.h:93-96). Each row is summed in
+ * entry order from zero, as ReducedSymmetryCsr::spmv does (include/ed/matvec/reduced_csr.h:89-102): in
+ * FP64 storage y equals the host CSR's bit for bit, and every vector of a k-vector apply equals its
+ * single apply. */
+int qb_csr_matvec(const qb_csr* csr, const void* in, void* out, int k, int dtype, void* stream);
+/* Routes every apply of prog on the CSR's sector pair (qb_matvec, qb_matvec_block, qb_matvec_host and
+ * the Krylov drivers) through the CSR; NULL detaches. The CSR must outlive the attachment. This is the
+ * lane choice of RepSectorMatVec (device_csr_, src/engine/internal.h:399-434). */
+int qb_program_attach_csr(qb_program* prog, const qb_csr* csr);
+
 /* ---- Krylov recurrences --------------------------------------------------------------------
  * The Lanczos kernel (include/ed/krylov/lanczos.h:266-576) on one sector, device-resident: alpha,
  * beta and every inner product in FP64, vectors stored as dtype. v0 is a host complex128 vector

@@ -67,6 +67,8 @@ def lib():
     L.qref_csr_nnz.argtypes = [vp]
     L.qref_csr_get.argtypes = [vp, _u64p, _u32p, _f64p]
     L.qref_csr_spmv.argtypes = [vp, _f64p, _f64p]
+    L.qref_csr_bytes.restype = C.c_uint64
+    L.qref_csr_bytes.argtypes = [vp]
     L.qref_sample_vector.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _f64p]
     L.qref_staged_seed.argtypes = [C.c_uint64, C.c_uint64, _f64p]
     L.qref_lanczos.argtypes = [vp, vp, _f64p, C.c_int, C.c_int, C.c_double, _f64p, _f64p, C.POINTER(C.c_int)]
@@ -193,7 +195,8 @@ class Sector:
         _check(lib().qref_gather(self.h, prog.h, x.view(np.float64), y.view(np.float64)))
         return y
 
-    def csr(self, prog: Program):
+    def csr(self, prog: Program, x=None):
+        """The merged reduced CSR (row_ptr, col, val); with x, also the reference's CSR spmv of x."""
         L = lib()
         c = L.qref_csr_build(self.h, prog.h)
         nnz = int(L.qref_csr_nnz(c))
@@ -201,8 +204,19 @@ class Sector:
         col = np.zeros(nnz, np.uint32)
         val = np.zeros(2 * nnz, np.float64)
         L.qref_csr_get(c, rp, col, val)
+        y = None
+        if x is not None:
+            x = np.ascontiguousarray(x, dtype=np.complex128)
+            y = np.zeros(self.dim, np.complex128)
+            rc = L.qref_csr_spmv(c, x.view(np.float64), y.view(np.float64))
         L.qref_csr_free(c)
+        if x is not None:
+            _check(rc)
+            return rp, col, val.view(np.complex128), y
         return rp, col, val.view(np.complex128)
+
+    def csr_handle(self, prog: Program) -> "Csr":
+        return Csr(self, prog)
 
     def lanczos(self, prog: Program, v0, max_iter, reorth=0, breakdown_tol=1e-300):
         v0 = np.ascontiguousarray(v0, dtype=np.complex128)
@@ -279,3 +293,35 @@ def set_threads(n: int):
 
 def max_threads() -> int:
     return int(lib().qref_max_threads())
+
+
+class Csr:
+    """The reference's ReducedSymmetryCsr of a program on one sector, kept for repeated spmv."""
+
+    def __init__(self, sector: "Sector", prog: Program):
+        L = lib()
+        self.dim = sector.dim
+        self.h = L.qref_csr_build(sector.h, prog.h)
+        if not self.h:
+            raise RuntimeError(L.qref_last_error().decode())
+
+    @property
+    def nnz(self) -> int:
+        return int(lib().qref_csr_nnz(self.h))
+
+    @property
+    def bytes(self) -> int:
+        return int(lib().qref_csr_bytes(self.h))
+
+    def spmv(self, x: np.ndarray, y: np.ndarray) -> None:
+        _check(lib().qref_csr_spmv(self.h, x.view(np.float64), y.view(np.float64)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                lib().qref_csr_free(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    __del__ = close

@@ -427,6 +427,7 @@ void qref_csr_get(void* c, std::uint64_t* row_ptr, std::uint32_t* col, double* v
         }
     }
 }
+std::uint64_t qref_csr_bytes(void* c) { return static_cast<RefCsr*>(c)->csr.bytes(); }
 int qref_csr_spmv(void* c, const double* in, double* out) {
     return guarded([&] {
         static_cast<RefCsr*>(c)->csr.spmv(reinterpret_cast<const Complex*>(in), reinterpret_cast<Complex*>(out));

@@ -23,6 +23,8 @@ EXPORTS = [
     "qb_sector_info", "qb_index_and_projection",
     "qb_program_create", "qb_program_destroy",
     "qb_matvec", "qb_matvec_block", "qb_matvec_host",
+    "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
+    "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_cf", "qb_lanczos_noalloc",
 ]
 
@@ -89,6 +91,13 @@ def lib():
     L.qb_matvec.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
     L.qb_matvec_block.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
     L.qb_matvec_host.argtypes = [vp, vp, vp, vp, vp]
+    L.qb_csr_build.argtypes = [vp, vp, vp, u64, C.POINTER(vp)]
+    L.qb_csr_upload.argtypes = [vp, vp, vp, vp, vp, u64, C.POINTER(vp)]
+    L.qb_csr_destroy.argtypes = [vp]
+    L.qb_csr_info.argtypes = [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(i)]
+    L.qb_csr_download.argtypes = [vp, vp, vp, vp]
+    L.qb_csr_matvec.argtypes = [vp, vp, vp, i, i, vp]
+    L.qb_program_attach_csr.argtypes = [vp, vp]
     L.qb_lanczos.argtypes = [vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i)]
     L.qb_eigs_lowest.argtypes = [vp, vp, i, i, i, C.POINTER(d), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]

@@ -1061,27 +1061,49 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         double best = theta;
         bool ok = false;
         for (int c = 0; c < 8 && !ok; ++c) {
-            Recurrence F(sec, prog, QB_C128, cyc);
-            F.start_from_device(x.p);
-            // the short FP64 cycle keeps its basis (the restart vector is built from it)
-            ScanOut f = run_scan(F, cyc, QB_REORTH_NONE, false, 1e-300, true);
-            total_mv += f.matvecs;
-            const int mm = static_cast<int>(f.alpha.size());
-            std::vector<double> ee(std::max(1, mm - 1));
-            for (int i = 0; i + 1 < mm; ++i) ee[i] = f.beta[i + 1];
-            double l2, h2;
-            gershgorin(f.alpha.data(), ee.data(), mm, l2, h2);
-            const double th = kth_eigenvalue(f.alpha.data(), ee.data(), mm, 0, l2, h2);
-            const std::vector<double> zz = inverse_iteration(f.alpha.data(), ee.data(), mm, th);
-            const double bound = std::abs(f.beta[mm]) * std::abs(zz[mm - 1]);
-            best = th;
-            if (bound <= 1e-7 * scale) {
-                ok = true;
-                break;
+            // the short FP64 cycle keeps its basis for the restart vector when it fits comfortably; otherwise
+            // the cycle runs twice and the second pass accumulates the restart vector
+            cudaMemGetInfo(&free_b, &total_b);
+            const bool keep_f = static_cast<double>(cyc + 4) * nb * 16.0 < 0.5 * static_cast<double>(free_b);
+            std::vector<double> zz;
+            int mm = 0;
+            {
+                Recurrence F(sec, prog, QB_C128, cyc);
+                F.start_from_device(x.p);
+                ScanOut f = run_scan(F, cyc, QB_REORTH_NONE, false, 1e-300, keep_f);
+                total_mv += f.matvecs;
+                mm = static_cast<int>(f.alpha.size());
+                std::vector<double> ee(std::max(1, mm - 1));
+                for (int i = 0; i + 1 < mm; ++i) ee[i] = f.beta[i + 1];
+                double l2, h2;
+                gershgorin(f.alpha.data(), ee.data(), mm, l2, h2);
+                const double th = kth_eigenvalue(f.alpha.data(), ee.data(), mm, 0, l2, h2);
+                zz = inverse_iteration(f.alpha.data(), ee.data(), mm, th);
+                const double bound = std::abs(f.beta[mm]) * std::abs(zz[mm - 1]);
+                best = th;
+                if (bound <= 1e-7 * scale) {
+                    ok = true;
+                    break;
+                }
+                if (keep_f) {
+                    cuda_check(cudaMemsetAsync(x.p, 0, nb * 16, F.st), "zero");
+                    for (int j = 0; j < mm; ++j) F.accumulate(x.p, zz[j], F.basis[j]);
+                    cuda_check(cudaStreamSynchronize(F.st), "refine");
+                    continue;
+                }
             }
-            cuda_check(cudaMemsetAsync(x.p, 0, nb * 16, F.st), "zero");
-            for (int j = 0; j < mm; ++j) F.accumulate(x.p, zz[j], F.basis[j]);
-            cuda_check(cudaStreamSynchronize(F.st), "refine");
+            // second pass from the same start: the same vectors, bit for bit
+            Recurrence F2(sec, prog, QB_C128, mm);
+            F2.start_from_device(x.p);   // synchronises; x is free to be overwritten from here
+            cuda_check(cudaMemsetAsync(x.p, 0, nb * 16, F2.st), "zero");
+            for (int j = 0; j < mm; ++j) {
+                F2.accumulate(x.p, zz[j], F2.vbuf[F2.cur].p);
+                if (j + 1 < mm) {
+                    F2.step(j, QB_REORTH_NONE);
+                    ++total_mv;
+                }
+            }
+            cuda_check(cudaStreamSynchronize(F2.st), "refine second pass");
         }
         *e0 = best;
         if (converged) *converged = ok ? 1 : 0;

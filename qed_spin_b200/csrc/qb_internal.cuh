@@ -184,11 +184,35 @@ struct qb_sector {
     std::uint64_t device_bytes() const;
 };
 
+struct qb_csr;
+
 struct qb_program {
     qb::DevBuf<unsigned char> blob;   // every array back to back (8-byte aligned), staged as one copy
     qb::DProgram view;
     double norm_bound = 0.0;          // sum of |coeff|
+    const qb_csr* csr = nullptr;      // the attached reduced CSR (qb_program_attach_csr), or none
 };
+
+// The merged reduced CSR of an operator between two sectors (csr.cu).
+struct qb_csr {
+    const qb_sector* row = nullptr;
+    const qb_sector* col = nullptr;
+    std::uint64_t rows = 0, nnz = 0;
+    int id_bytes = 0;                 // 1: u8 dictionary ids, 2: u16 ids, 0: full values
+    int n_dict = 0;
+    qb::DevBuf<unsigned long long> row_ptr;
+    qb::DevBuf<std::uint32_t> col_idx;
+    qb::DevBuf<unsigned char> ids;    // nnz x id_bytes
+    qb::DevBuf<double2> vals;         // the dictionary (n_dict) or every value (nnz)
+    std::uint64_t bytes() const {
+        return row_ptr.bytes() + col_idx.bytes() + ids.bytes() + vals.bytes();
+    }
+};
+
+namespace qb {
+// y = A x on k vectors (k == 1: one vector; else interleaved by row), x as dtype_in, y as dtype_out.
+void csr_spmv(const qb_csr* A, const void* in, void* out, int k, int dtype_in, int dtype_out, cudaStream_t st);
+}  // namespace qb
 
 namespace qb {
 

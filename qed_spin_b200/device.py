@@ -57,7 +57,7 @@ class Sector:
                 lib().qb_sector_destroy(self.h)
             except Exception:   # interpreter shutdown: the library is already gone
                 pass
-            self.h = C.c_void_p()
+            self.h = None   # (no module globals here: this also runs at interpreter shutdown)
 
     __del__ = close
 
@@ -114,9 +114,81 @@ class Program:
                 lib().qb_program_destroy(self.h)
             except Exception:   # interpreter shutdown: the library is already gone
                 pass
-            self.h = C.c_void_p()
+            self.h = None   # (no module globals here: this also runs at interpreter shutdown)
 
     __del__ = close
+
+
+class Csr:
+    """The merged reduced CSR of a program between two sectors, on the device.
+
+    Built from the row walk on the device (`Csr(row, col, prog)`) or uploaded from host arrays
+    (`Csr.upload(row, col, row_ptr, col, val)`). `attach(prog)` routes every apply of `prog` on this
+    sector pair through it.
+    """
+
+    def __init__(self, row: Sector, col: Sector, prog: Program = None, max_bytes: int = 0, _handle=None):
+        self.row, self.col = row, col
+        self._attached = []
+        if _handle is not None:
+            self.h = _handle
+            return
+        h = C.c_void_p()
+        check(lib().qb_csr_build(row.h, col.h, prog.h, int(max_bytes), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def upload(cls, row: Sector, col: Sector, row_ptr, col_idx, val, max_bytes: int = 0) -> "Csr":
+        rp = np.ascontiguousarray(row_ptr, np.uint64)
+        ci = np.ascontiguousarray(col_idx, np.uint32)
+        v = np.ascontiguousarray(val, np.complex128)
+        h = C.c_void_p()
+        check(lib().qb_csr_upload(row.h, col.h, rp.ctypes.data, ci.ctypes.data, v.view(np.float64).ctypes.data,
+                                  int(max_bytes), C.byref(h)))
+        return cls(row, col, _handle=h)
+
+    def info(self) -> dict:
+        nnz, nb, nd = C.c_uint64(), C.c_uint64(), C.c_int()
+        check(lib().qb_csr_info(self.h, C.byref(nnz), C.byref(nb), C.byref(nd)))
+        return {"nnz": nnz.value, "bytes": nb.value, "n_dict": nd.value}
+
+    def download(self):
+        nnz = self.info()["nnz"]
+        rp = np.zeros(self.row.dim + 1, np.uint64)
+        ci = np.zeros(nnz, np.uint32)
+        v = np.zeros(2 * nnz, np.float64)
+        check(lib().qb_csr_download(self.h, rp.ctypes.data, ci.ctypes.data, v.ctypes.data))
+        return rp, ci, v.view(np.complex128)
+
+    def matvec(self, x, out, k: int = 1, dtype="c128", stream=None):
+        """out = A x on device tensors (k > 1: k vectors interleaved by row)."""
+        check(lib().qb_csr_matvec(self.h, x.data_ptr(), out.data_ptr(), k, _dt(dtype), _stream_ptr(stream)))
+
+    def attach(self, prog: Program):
+        check(lib().qb_program_attach_csr(prog.h, self.h))
+        prog._csr = self
+        self._attached.append(prog)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            try:
+                for p in self._attached:
+                    if getattr(p, "_csr", None) is self and p.h and p.h.value:
+                        lib().qb_program_attach_csr(p.h, None)
+                        p._csr = None
+                lib().qb_csr_destroy(self.h)
+            except Exception:   # interpreter shutdown: the library is already gone
+                pass
+            self.h = None   # (no module globals here: this also runs at interpreter shutdown)
+            self._attached = []
+
+    __del__ = close
+
+
+def detach_csr(prog: Program):
+    """Routes prog's applies back to the row walk."""
+    check(lib().qb_program_attach_csr(prog.h, None))
+    prog._csr = None
 
 
 def _stream_ptr(stream):

@@ -10,7 +10,7 @@ Writes
                 (tests/python/golden/refs/api-2026-09/cpu.json.gz, tier "exact" 1e-10), for the chain models
                 whose fixed-S^z spectra the sector tests reassemble, plus the N = 12 Heisenberg ring E0.
   fixtures.npz  outputs of the reference engine itself on small seeded cases: representatives and 1/norms,
-                row programs, y = H x, the merged CSR pattern, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
+                row programs, y = H x, the merged CSR pattern and its spmv of x, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
                 curves and continued-fraction spectra.
 """
 from __future__ import annotations
@@ -91,7 +91,8 @@ def main(ref_root: str):
         x = R.staged_seed(1234, rs.dim)
         fx[f"{name}/x"] = x
         fx[f"{name}/y"] = rs.gather(rp, x)
-        rowp, col, val = rs.csr(rp)
+        rowp, col, val, ycsr = rs.csr(rp, x)
+        fx[f"{name}/csr_y"] = ycsr
         fx[f"{name}/csr_row_ptr"] = rowp
         fx[f"{name}/csr_col"] = col
         fx[f"{name}/csr_val"] = val

@@ -46,7 +46,7 @@ def test_gather_and_sparsity_bit_exact(fixtures, name):
     rp, col, val = S.csr(P)
     assert np.array_equal(rp, fixtures[f"{name}/csr_row_ptr"])
     assert np.array_equal(col, fixtures[f"{name}/csr_col"])
-    np.testing.assert_allclose(val, fixtures[f"{name}/csr_val"], rtol=0, atol=1e-14)
+    assert np.array_equal(val.view(np.uint64), fixtures[f"{name}/csr_val"].view(np.uint64))
 
 
 @pytest.mark.parametrize("name", NAMES)
