@@ -20,7 +20,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -52,62 +51,100 @@ def workload():
     return spec, prog, prods
 
 
+# DRAM bytes (read + write) of one spmv1<complex64> launch on this workload, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch, cold L2).
+SPMV1_CHAIN32_DRAM_BYTES = 596.873472e6 + 38.907392e6
+
 CONFIG = {"workload": "XXZ chain N=32 J=1 Delta=0.7, Sz=0 k=0 reflection-even flip-even (D32 x Z2)",
           "n_sites": 32, "group_size": 128}
 
 
 class Clocks:
-    """nvidia-smi clock / throttle samples taken while the timed region runs."""
+    """SM clock, power and clock-event-reason samples (NVML, read only) taken every 10 ms while the timed
+    region runs, plus one sample just before it and one just after, so a short region still has samples."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/qb_clocks_{os.getpid()}.csv"
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.stop = None
+        self.thread = None
+        self.h = None
+        d = os.environ.get("QB_CLOCKS_DIR")   # keeps the raw samples when set
+        self.path = os.path.join(d, f"clocks_gpu{cuda_index}.csv") if d and os.path.isdir(d) else None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.cuda_index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _sample(self):
+        import pynvml
+        h = self.h
+        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+        try:
+            reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            reasons = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        try:
+            power = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+        except Exception:
+            power = None
+        self.samples.append((time.time(), sm, reasons, power))
 
     def __enter__(self):
+        import threading
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
-                                         stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            self.h = self._handle()
+            import pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self._sample()
+            self.stop = threading.Event()
+
+            def run():
+                while not self.stop.wait(0.01):
+                    self._sample()
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+        except Exception as e:
+            self.h = None
+            self.error = str(e)
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-            self.fh.close()
+        if self.h is None:
+            return
+        self.stop.set()
+        self.thread.join()
+        self._sample()
+        if self.path:
+            with open(self.path, "w") as fh:
+                fh.write("unix_time,sm_mhz,reasons_mask,power_w\n")
+                for t, sm, r, pw in self.samples:
+                    fh.write(f"{t:.3f},{sm},{r:#x},{pw}\n")
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        try:
-            for line in open(self.path):
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    sm.append(float(f[1]))
-                    mx = float(f[2])
-                except ValueError:
-                    continue
-                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-                for n, v in zip(names, f[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
-        except FileNotFoundError:
-            pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "unavailable": getattr(self, "error", "no NVML")}
+        sm = [x[1] for x in self.samples]
+        reasons = set()
+        for _, _, r, _ in self.samples:
+            for bit, name in self.REASONS.items():
+                if r & bit:
+                    reasons.add(name)
+        pw = [x[3] for x in self.samples if x[3] is not None]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_median": statistics.median(pw) if pw else None, "source": "NVML"}
 
 
 def dist_init():
@@ -221,7 +258,7 @@ def cpu_baseline_sample(dim_gpu):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -364,7 +401,8 @@ def main():
                           "no flush",
                        parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": hbm, "unit": "GB/s", "frac": ach32 / hbm,
-                     "traffic": None, "peak_kind": peak_kind, "kernel": "spmv1<complex64>",
+                     "traffic": SPMV1_CHAIN32_DRAM_BYTES, "traffic_source": "ncu capture of one spmv1 launch on this workload",
+                     "peak_kind": peak_kind, "kernel": "spmv1<complex64>",
                      "alg_bytes_per_launch": csr_bytes(8)},
         "fp64": {"ms_per_hv": per64, "hv_per_s": 1e3 / per64, "achieved_gbs": ach64, "frac": ach64 / hbm},
         "csr_build_s": csr_build_s,

@@ -240,18 +240,16 @@ __device__ __forceinline__ double2 csr_value(const unsigned char* ids, int id_by
     return __ldg(vals + e);
 }
 
-// One vector: a thread per row, its entries taken kBatch at a time (the columns and ids of the batch, then
-// its x loads, all in flight together) and added in entry order. The sum is the reference's
-// (ReducedSymmetryCsr::spmv, include/ed/matvec/reduced_csr.h:89-102: acc = 0, then acc += value * x in
-// entry order), so y equals the host CSR's bit for bit. The x loads are random: with x in L2 the kernel is
-// bound by L2 sector requests, beyond it by the DRAM sectors they fetch (32 bytes per 8- or 16-byte element).
+// One vector: a thread per row. The row's entries are read in aligned windows of 4 (one 16-byte load of
+// columns, one 4- or 8-byte load of value ids; the column and id arrays are padded to a multiple of 4
+// entries, so a window never leaves them); the window's entries outside the row are skipped, the others'
+// x loads issued together and their products added in entry order. The sum is the reference's
+// (ReducedSymmetryCsr::spmv, include/ed/matvec/reduced_csr.h:89-102: acc = 0, then acc += value * x in entry
+// order), so y equals the host CSR's bit for bit. The x loads are random: with x in L2 the kernel is bound
+// by L1/L2 sector traffic, beyond it by the DRAM sectors they fetch (32 bytes per 8- or 16-byte element).
 constexpr int kRowsPerBlock = 256;
 constexpr int kBatch = kPerLd;
-
-__device__ __forceinline__ unsigned csr_id(const unsigned char* ids, int id_bytes, u64 e) {
-    return id_bytes == 1 ? static_cast<unsigned>(__ldg(ids + e))
-                         : static_cast<unsigned>(__ldg(reinterpret_cast<const unsigned short*>(ids) + e));
-}
+static_assert(kBatch == 4, "the 16-byte column windows hold 4 entries");
 
 template <bool kInF32, bool kOutF32>
 __global__ void __launch_bounds__(kRowsPerBlock) spmv1(u64 rows, const unsigned long long* __restrict__ row_ptr,
@@ -270,28 +268,34 @@ __global__ void __launch_bounds__(kRowsPerBlock) spmv1(u64 rows, const unsigned 
     const u64 r = static_cast<u64>(blockIdx.x) * kRowsPerBlock + threadIdx.x;
     if (r >= rows) return;
     cplx acc{0.0, 0.0};
-    const u64 e1 = row_ptr[r + 1];
-    for (u64 e = row_ptr[r]; e < e1; e += kBatch) {
-        u32 cj[kBatch];
-        unsigned vid[kBatch];
+    const u64 e0 = row_ptr[r], e1 = row_ptr[r + 1];
+    for (u64 w = e0 & ~3ULL; w < e1; w += 4) {
+        const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + w));
+        const u32 cj[4] = {c4.x, c4.y, c4.z, c4.w};
+        unsigned vid[4] = {0, 0, 0, 0};
+        if (id_bytes == 1) {
+            const unsigned i4 = __ldg(reinterpret_cast<const unsigned*>(ids + w));
 #pragma unroll
-        for (int q = 0; q < kBatch; ++q) {
-            cj[q] = 0;
-            vid[q] = 0;
-            if (e + q < e1) {
-                cj[q] = __ldg(col + e + q);
-                if (id_bytes) vid[q] = csr_id(ids, id_bytes, e + q);
-            }
+            for (int q = 0; q < 4; ++q) vid[q] = (i4 >> (8 * q)) & 0xFFu;
+        } else if (id_bytes == 2) {
+            const uint2 i2 = __ldg(reinterpret_cast<const uint2*>(ids + 2 * w));
+            vid[0] = i2.x & 0xFFFFu;
+            vid[1] = i2.x >> 16;
+            vid[2] = i2.y & 0xFFFFu;
+            vid[3] = i2.y >> 16;
         }
-        typename Li::T xv[kBatch];
+        bool on[4];
+        typename Li::T xv[4];
 #pragma unroll
-        for (int q = 0; q < kBatch; ++q)
-            if (e + q < e1) xv[q] = __ldg(in + cj[q]);
+        for (int q = 0; q < 4; ++q) {
+            on[q] = w + q >= e0 && w + q < e1;
+            if (on[q]) xv[q] = __ldg(in + cj[q]);
+        }
 #pragma unroll
-        for (int q = 0; q < kBatch; ++q)
-            if (e + q < e1) {
+        for (int q = 0; q < 4; ++q)
+            if (on[q]) {
                 const double2 v = id_bytes == 1 ? dict[vid[q]]
-                                                : (id_bytes == 2 ? __ldg(vals + vid[q]) : __ldg(vals + e + q));
+                                                : (id_bytes == 2 ? __ldg(vals + vid[q]) : __ldg(vals + w + q));
                 acc = cadd(acc, cmul({v.x, v.y}, Li::load(xv, q)));
             }
     }
@@ -401,6 +405,10 @@ struct BitsHash {
     }
 };
 
+// The column and id arrays hold a multiple of 4 entries (at least 4): the matvec reads them in aligned
+// windows of 4.
+u64 padded(u64 nnz) { return ((nnz + 3) & ~3ULL) + (nnz == 0 ? 4 : 0); }
+
 // The id width of a dictionary of n values over nnz entries: 1 (u8) up to 256 values, 2 (u16) up to 65536,
 // 0 (whole values) beyond, or when the dictionary form is not the smaller one (build_cross_csr,
 // include/ed/matvec/sector_rows.h:363-366).
@@ -509,11 +517,11 @@ int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* p
         int id_bytes = dict_id_bytes(dict.size(), A->nnz);
         if (overflow) id_bytes = 0;
         check_budget(row->dim, A->nnz, id_bytes, dict.size(), max_bytes);
-        A->col_idx.alloc(A->nnz);
+        A->col_idx.alloc(padded(A->nnz));
         for (int attempt = 0; attempt < 2; ++attempt) {
             if (id_bytes) {
                 cuda_check(cudaMemcpy(dids.p, hid.data(), nslots * 4, cudaMemcpyHostToDevice), "dict ids");
-                A->ids.alloc(A->nnz * id_bytes);
+                A->ids.alloc(padded(A->nnz) * id_bytes);
                 A->vals.upload(dict);
                 A->n_dict = static_cast<int>(dict.size());
             } else {
@@ -568,9 +576,10 @@ int qb_csr_upload(const qb_sector* row, const qb_sector* col, const uint64_t* ro
         A->nnz = nnz;
         A->id_bytes = id_bytes;
         A->row_ptr.upload(reinterpret_cast<const unsigned long long*>(row_ptr), rows + 1);
-        A->col_idx.upload(col_idx, nnz);
+        A->col_idx.alloc(padded(nnz));
+        if (nnz) cuda_check(cudaMemcpy(A->col_idx.p, col_idx, nnz * 4, cudaMemcpyHostToDevice), "upload");
         if (id_bytes) {
-            std::vector<unsigned char> ids(nnz * id_bytes);
+            std::vector<unsigned char> ids(padded(nnz) * id_bytes, 0);
             for (u64 e = 0; e < nnz; ++e) {
                 if (id_bytes == 1)
                     ids[e] = static_cast<unsigned char>(id[e]);
