@@ -262,6 +262,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ftlm", action="store_true", help="leave the batched FTLM measurement out of the line")
+    ap.add_argument("--ftlm", action="store_true",
+                    help="batched FTLM over the 600 blocks of the XXZ chain N=24 (every S^z x 24 momenta), one "
+                         "JSON line: samples/s against the plain single-sample path and the reference CPU engine")
     ap.add_argument("--e0-6x6", action="store_true",
                     help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
                          "(FP64, and FP32 storage + FP64 refinement), one JSON line")
@@ -276,6 +280,9 @@ def main():
         return
     if args.e0_6x6:
         e0_6x6(args)
+        return
+    if args.ftlm:
+        ftlm_config(args)
         return
 
     world, rank, local = dist_init() if args.impl == "b200" else (int(os.environ.get("WORLD_SIZE", "1")),
@@ -385,6 +392,13 @@ def main():
             cpu = cpu_baseline_sample(n)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"unavailable": str(e)}
+    # the batched FTLM workload (every block of the N = 24 chain), rank 0 at N = 1
+    ftlm = None
+    if rank == 0 and world == 1 and not args.no_ftlm:
+        try:
+            ftlm = ftlm_measure(args, with_cpu=not args.no_cpu_baseline)
+        except Exception as e:
+            ftlm = {"unavailable": str(e)}
 
     if rank != 0:
         return
@@ -421,9 +435,104 @@ def main():
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "ftlm": ftlm,
     }
     print(json.dumps(line))
     A.close()
+
+
+FTLM_N, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED = 24, 40, 100, 20240601
+
+
+def ftlm_workload():
+    """XXZ chain N = 24 (J = 1, Delta = 0.5, field h = 0.1 as -h sum S^z): every S^z sector x the 24
+    translation momenta (the non-empty ones), 40 temperatures linspace(0.1, 4)."""
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    N = FTLM_N
+    prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.5) + ops.zeeman_z_products(N, 0.1)
+    specs = [lat.chain_sector(N, n_up, k) for n_up in range(N + 1) for k in range(N)]
+    betas = 1.0 / np.linspace(0.1, 4.0, 40)
+    return specs, prods, ops.row_program(ops.from_products(N, prods)), betas
+
+
+def ftlm_reference_sample(threads):
+    """The reference engine's sampled thermal blocks on the host cores, on a bounded stratified sample: the
+    k = 0 block of every S^z sector with 4 samples each at depth 100 (a sample's cost depends only on its
+    block, so samples/s carries over to the whole 600-block workload)."""
+    from oracle import ref as R
+    _, prods, _, betas = ftlm_workload()
+    R.set_threads(threads)
+    from qed_spin_b200 import lattice as lat
+    blocks = [lat.chain_sector(FTLM_N, n_up, 0) for n_up in range(FTLM_N + 1)]
+    rs = [R.Sector(s.n_sites, s.n_up, s.perms, s.chars, flips=s.flips, slc_mode=-1) for s in blocks]
+    rp = R.Operator(FTLM_N, prods).row_program()
+    dims = [r.dim for r in rs]
+    t = time.perf_counter()
+    R.ftlm_blocks(rs, rp, 4, FTLM_DEPTH, FTLM_SEED, betas)
+    dt = time.perf_counter() - t
+    # whole-workload estimate: each S^z sector's 24 blocks have about its k = 0 block's dimension
+    return {"value": 4 * len(rs) / dt, "unit": "samples/s", "cores": threads, "kind": "reference",
+            "sample": f"k=0 block of each of the 25 S^z sectors (dims {min(dims)}..{max(dims)}), 4 samples, depth "
+                      f"{FTLM_DEPTH}, CSR lane, the reference's block scheduling; {dt:.1f} s"}
+
+
+def ftlm_config(args):
+    print(json.dumps(ftlm_measure(args, with_cpu=not args.no_cpu_baseline)))
+
+
+def ftlm_measure(args, with_cpu=True):
+    """Batched FTLM over the 554 non-empty blocks of the N = 24 chain: samples/s of the FP64 and FP32-storage
+    lanes, the plain single-sample path on a stratified subset, and the reference engine on the host cores."""
+    import torch
+
+    from qed_spin_b200 import build
+    from qed_spin_b200 import device as D
+    build.build()
+    specs, prods, prog, betas = ftlm_workload()
+    t = time.perf_counter()
+    secs = [D.Sector(s) for s in specs]
+    secs = [s for s in secs if s.dim > 0]
+    torch.cuda.synchronize()
+    enum_s = time.perf_counter() - t
+    P = D.Program(prog)
+    n_blocks = len(secs)
+    dims = np.array([s.dim for s in secs])
+    out = {"workload": "XXZ chain N=24 J=1 Delta=0.5 h=0.1, every Sz x 24 momenta, 40 samples, depth 100, 40 T",
+           "blocks": n_blocks, "dim_total": int(dims.sum()), "dim_max": int(dims.max()), "enumeration_s": enum_s}
+    res = {}
+    for dtype in ("c128", "c64"):
+        D.ftlm_blocks(secs[-8:], P, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas, dtype=dtype)   # warm-up
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = D.ftlm_blocks(secs, P, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas, dtype=dtype)
+        dt = time.perf_counter() - t
+        res[dtype] = r
+        out[f"batched_{dtype}"] = {"s": dt, "samples_per_s": n_blocks * FTLM_SAMPLES / dt, "phases": r["stats"]}
+    tot64, tot32 = res["c128"]["total"], res["c64"]["total"]
+    out["fp32_vs_fp64_max_rel"] = {k: float(np.max(np.abs(tot32[k] - tot64[k]) / np.maximum(np.abs(tot64[k]), 1e-12)))
+                                   for k in ("lnZ", "E", "C")}
+    i1 = int(np.argmin(np.abs(1.0 / betas - 1.0)))
+    out["thermo_T1"] = {"T": float(1.0 / betas[i1]), "E_per_site": float(tot64["E"][i1] / FTLM_N),
+                        "C_per_site": float(tot64["C"][i1] / FTLM_N), "S_per_site": float(tot64["S"][i1] / FTLM_N)}
+    # the plain path: one sample at a time, FP64, the on-the-fly walk, on a stratified subset (the k = 0 block
+    # of every S^z sector, one sample each)
+    from qed_spin_b200 import lattice as lat
+    sub = [D.Sector(lat.chain_sector(FTLM_N, n_up, 0)) for n_up in range(FTLM_N + 1)]
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for s in sub:
+        D.ftlm_blocks([s], P, 1, FTLM_DEPTH, FTLM_SEED, betas, use_csr=False)
+    dt = time.perf_counter() - t
+    out["plain_fp64_walk"] = {"samples_per_s": len(sub) / dt,
+                              "sample": "k=0 block of each S^z sector, 1 sample each, one call per sample"}
+    out["speedup_batched_fp64_vs_plain"] = out["batched_c128"]["samples_per_s"] / out["plain_fp64_walk"]["samples_per_s"]
+    if with_cpu:
+        try:
+            out["cpu_baseline"] = ftlm_reference_sample(os.cpu_count() or 1)
+        except Exception as e:
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
 
 
 def e0_6x6(args):

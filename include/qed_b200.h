@@ -183,6 +183,25 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
 int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth, uint64_t seed, const double* betas,
             int n_beta, int dtype, double* lnZ, double* E, double* V, double* e_min);
 
+/* FTLM over many blocks, the sampled per-block path of the thermal driver (src/engine/thermal.cpp:155-340
+ * over the blocks of one call): every block uses the call's base seed, so sample s of block b is the first
+ * dim_b draws of sample_engine(seed, s) (thermal.cpp:363, sample_seed.h:37-89); one table of those streams,
+ * drawn once, serves every block. Blocks run largest first on a few streams; each block's samples advance
+ * together as one block matvec, on the block's reduced CSR (built inside the call) when use_csr != 0 and it
+ * fits, else on the row walk. Outputs per block b and beta t at [b * n_beta + t]: lnZ, E, V; e_min[b].
+ * stats (NULL or 4 doubles): seconds spent drawing the samples, building the CSRs, running the recurrences,
+ * and forming the curves (the per-block build / apply times the thermal driver reports). */
+int qb_ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int samples, int depth,
+                   uint64_t seed, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ, double* E,
+                   double* V, double* e_min, double* stats);
+
+/* The blocks' curves combined in log space (src/engine/thermal.cpp:599-641): lnZ = logsumexp_b(ln w_b +
+ * lnZ_b), E = sum_b p_b E_b, C = beta^2 sum_b p_b (V_b + (E_b - E)^2) (the law of total variance), S = lnZ +
+ * beta E, F = -lnZ / beta. weights: per-block multiplicities (NULL: all 1). Inputs [b * n_beta + t]. */
+int qb_thermal_combine(int n_blocks, const double* weights, const double* lnZ, const double* E, const double* V,
+                       const double* betas, int n_beta, double* lnZ_out, double* E_out, double* C_out, double* S_out,
+                       double* F_out);
+
 /* The T = 0 continued fraction from a host complex128 vector phi on one sector
  * (cf_spectral_from_vector, include/ed/dynamics/cf.h:104-160): Lanczos without reorthogonalisation to
  * `depth`, breakdown at `tolerance`, S(w) = -Im G(w + i eta)/pi with G weighted by ||phi||^2; shift: the

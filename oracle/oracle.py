@@ -237,20 +237,32 @@ def staged_seed(seed: int, n: int):
     return out.view(np.complex128)
 
 
-def combine_blocks(curves, betas):
-    """Log-space combine of per-block FTLM curves into the whole system's thermodynamics
-    (the driver's combine, docs/architecture.md:231-232): lnZ = logsumexp_b lnZ_b,
-    E = sum_b w_b E_b, C = beta^2 (sum_b w_b (V_b + E_b^2) - E^2), S = lnZ + beta E."""
-    betas = np.asarray(betas)
-    lnZ = np.stack([c["lnZ"] for c in curves])
-    E = np.stack([c["E"] for c in curves])
-    V = np.stack([c["V"] for c in curves])
-    m = lnZ.max(axis=0)
-    w = np.exp(lnZ - m)
-    Z = w.sum(axis=0)
-    w = w / Z
-    tot_lnZ = m + np.log(Z)
-    tot_E = (w * E).sum(axis=0)
-    tot_C = betas ** 2 * ((w * (V + E ** 2)).sum(axis=0) - tot_E ** 2)
-    tot_S = tot_lnZ + betas * tot_E
-    return dict(lnZ=tot_lnZ, E=tot_E, C=tot_C, S=tot_S)
+def combine_blocks(curves, betas, weights=None):
+    """Log-space combine of per-block FTLM curves into the whole system's thermodynamics (the thermal
+    driver's combine, src/engine/thermal.cpp:608-641): p_b = w_b exp(lnZ_b - max), lnZ = max + ln sum p_b,
+    E = sum p_b E_b / Z, C = beta^2 sum p_b (V_b + (E_b - E)^2) / Z (law of total variance), S = lnZ + beta E,
+    F = -lnZ / beta. Sums run over the blocks in order, as there."""
+    betas = np.asarray(betas, np.float64)
+    nb = len(curves)
+    w = np.ones(nb) if weights is None else np.asarray(weights, np.float64)
+    out = {k: np.zeros(len(betas)) for k in ("lnZ", "E", "C", "S", "F")}
+    for i, bt in enumerate(betas):
+        mx = max(np.log(w[b]) + curves[b]["lnZ"][i] for b in range(nb))
+        p = [np.exp(np.log(w[b]) + curves[b]["lnZ"][i] - mx) for b in range(nb)]
+        z = 0.0
+        e = 0.0
+        for b in range(nb):
+            z += p[b]
+            e += p[b] * curves[b]["E"][i]
+        e /= z
+        var = 0.0
+        for b in range(nb):
+            d = curves[b]["E"][i] - e
+            var += p[b] * (curves[b]["V"][i] + d * d)
+        var /= z
+        out["lnZ"][i] = mx + np.log(z)
+        out["E"][i] = e
+        out["C"][i] = bt * bt * var
+        out["S"][i] = out["lnZ"][i] + bt * e
+        out["F"][i] = -out["lnZ"][i] / bt
+    return out

@@ -67,6 +67,8 @@ def lib():
     L.qref_csr_nnz.argtypes = [vp]
     L.qref_csr_get.argtypes = [vp, _u64p, _u32p, _f64p]
     L.qref_csr_spmv.argtypes = [vp, _f64p, _f64p]
+    L.qref_ftlm_blocks.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint64, _f64p, C.c_int, _f64p, _f64p,
+                                   _f64p, _f64p]
     L.qref_csr_bytes.restype = C.c_uint64
     L.qref_csr_bytes.argtypes = [vp]
     L.qref_sample_vector.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _f64p]
@@ -325,3 +327,15 @@ class Csr:
             self.h = None
 
     __del__ = close
+
+
+def ftlm_blocks(sectors, prog: "Program", samples: int, depth: int, seed: int, betas) -> dict:
+    """The reference's sampled thermal blocks on the host (its CSR lane and block scheduling): per-block
+    curves [n_blocks, n_beta] and e_min [n_blocks]."""
+    betas = np.ascontiguousarray(betas, np.float64)
+    nb, nt = len(sectors), len(betas)
+    arr = (C.c_void_p * nb)(*[s.h for s in sectors])
+    lnZ, E, V = (np.zeros(nb * nt) for _ in range(3))
+    gs = np.zeros(nb)
+    _check(lib().qref_ftlm_blocks(arr, prog.h, nb, samples, depth, seed, betas, nt, lnZ, E, V, gs))
+    return {"lnZ": lnZ.reshape(nb, nt), "E": E.reshape(nb, nt), "V": V.reshape(nb, nt), "e_min": gs}

@@ -571,6 +571,60 @@ int qref_ftlm(void* sec, void* prog, int samples, int depth, std::uint64_t seed,
     });
 }
 
+// The sampled thermal blocks of one call on the host, scheduled as the reference's thermal driver schedules
+// them (src/engine/thermal.cpp:397-541): each block applies H through its merged reduced CSR (build_sector_csr,
+// the host default lane), every block draws its samples from the call's base seed; blocks below 2^16 states
+// (kHostPoolMaxDim, include/ed/core/device.h:67) run afterwards concurrently, one thread each (dynamic
+// schedule), the larger ones one at a time on the full thread team. Per-block curves [b * nb + t].
+int qref_ftlm_blocks(void* const* secs, void* prog, int n_blocks, int samples, int depth, std::uint64_t seed,
+                     const double* betas, int nb, double* lnZ, double* E, double* V, double* gs) {
+    return guarded([&] {
+        const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
+        const double tol = ed::numerics::kBreakdownRel * ed::numerics::scale_or_one(program_norm_bound(*P));
+        auto run = [&](int b) {
+            auto* S = static_cast<RefSector*>(secs[b]);
+            const auto pol = S->rd.make_policy();
+            const auto csr = ed::matvec::build_sector_csr(P->view(), pol, S->rd.dim());
+            auto apply = [&csr](const Complex* in, Complex* out, std::size_t) { csr.spmv(in, out); };
+            ed::thermal::FtlmOptions o;
+            o.num_samples = static_cast<std::size_t>(samples);
+            o.krylov_dim = static_cast<std::size_t>(depth);
+            o.breakdown_tol = tol;
+            o.betas.assign(betas, betas + nb);
+            o.random_seed = seed;
+            ed::matvec::CpuBackend be;
+            auto r = ed::thermal::ftlm_kernel(be, apply, S->rd.dim(), o);
+            std::copy(r.curves.lnZ.begin(), r.curves.lnZ.end(), lnZ + static_cast<std::size_t>(b) * nb);
+            std::copy(r.curves.E.begin(), r.curves.E.end(), E + static_cast<std::size_t>(b) * nb);
+            std::copy(r.curves.V.begin(), r.curves.V.end(), V + static_cast<std::size_t>(b) * nb);
+            gs[b] = r.ground_state_estimate;
+        };
+        constexpr std::uint64_t kPoolMaxDim = std::uint64_t{1} << 16;
+        std::vector<int> small;
+        for (int b = 0; b < n_blocks; ++b) {
+            if (static_cast<RefSector*>(secs[b])->rd.dim() >= kPoolMaxDim)
+                run(b);
+            else
+                small.push_back(b);
+        }
+        std::string failure;
+        {
+            const ed::parallel::ThreadBudgetScope serial_inside(omp_get_max_threads(), 1);
+#pragma omp parallel for schedule(dynamic, 1)
+            for (long long q = 0; q < static_cast<long long>(small.size()); ++q) {
+                try {
+                    const ed::parallel::ThreadBudgetScope one(1, 1);
+                    run(small[static_cast<std::size_t>(q)]);
+                } catch (const std::exception& e) {
+#pragma omp critical(qref_thermal_failure)
+                    if (failure.empty()) failure = e.what();
+                }
+            }
+        }
+        if (!failure.empty()) throw std::runtime_error(failure);
+    });
+}
+
 // The T = 0 continued fraction from a host vector phi (cf_spectral_from_vector, include/ed/dynamics/cf.h:104-160).
 // shift: NaN lets the kernel use the tridiagonal's lowest value.
 int qref_cf(void* sec, void* prog, const double* phi, int depth, const double* omega, int nw, double eta,

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -49,7 +50,8 @@ __device__ __forceinline__ u64 value_key(cplx v) {
 }
 
 struct Dict {
-    u64* keys;        // 2^kDictBits
+    u64* keys;        // mask + 1 slots (a power of two, at most 2^kDictBits)
+    u64 mask;
     double2* vals;
     u32* ids;         // slot -> dictionary id (fill pass)
     int* overflow;    // set past 65536 values, or when two values share a key
@@ -59,10 +61,10 @@ struct Dict {
 // One merged value into the dictionary set (the values pass).
 __device__ __forceinline__ void dict_insert(const Dict& D, cplx v) {
     if (*static_cast<volatile int*>(D.overflow)) return;   // whole values: the set is no longer needed
-    const u64 mask = (1ULL << kDictBits) - 1ULL;
+    const u64 mask = D.mask;
     const u64 key = value_key(v);
     u64 h = key & mask;
-    for (int probe = 0; probe <= (1 << kDictBits); ++probe) {
+    for (u64 probe = 0; probe <= mask; ++probe) {
         const u64 old = atomicCAS(reinterpret_cast<unsigned long long*>(D.keys + h), kEmpty, key);
         if (old == kEmpty) {
             D.vals[h] = make_double2(v.re, v.im);
@@ -75,11 +77,11 @@ __device__ __forceinline__ void dict_insert(const Dict& D, cplx v) {
     *D.overflow = 1;
 }
 
-// The dictionary id of a merged value (the fill pass; the set holds at most 65536 of its 2^17 slots, so the
+// The dictionary id of a merged value (the fill pass; the set is at most half full when ids are used, so the
 // probe ends at the key or an empty slot). A different value under the same key raises the overflow flag:
 // the caller then stores every value whole.
 __device__ __forceinline__ u32 dict_id(const Dict& D, cplx v) {
-    const u64 mask = (1ULL << kDictBits) - 1ULL;
+    const u64 mask = D.mask;
     const u64 key = value_key(v);
     u64 h = key & mask;
     while (D.keys[h] != key && D.keys[h] != kEmpty) h = (h + 1) & mask;
@@ -91,6 +93,70 @@ __device__ __forceinline__ u32 dict_id(const Dict& D, cplx v) {
     }
     return D.ids[h];
 }
+
+// The occupied slots of the value set numbered in slot order: ids[slot], the values compacted into dict (at
+// most kMaxDict), and the count. One CTA of 1024 threads walks the slots 1024 at a time.
+constexpr int kMaxDict = 65536;
+__global__ void __launch_bounds__(1024) dict_compact(const u64* keys, const double2* vals, u64 nslots, u32* ids,
+                                                     double2* dict, int* count) {
+    __shared__ u32 warp_n[32], warp_off[32];
+    __shared__ u32 base, round_n;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (u64 s0 = 0; s0 < nslots; s0 += 1024) {
+        const u64 slot = s0 + threadIdx.x;
+        const bool occ = slot < nslots && keys[slot] != kEmpty;
+        const unsigned bal = __ballot_sync(0xffffffffu, occ);
+        if (lane == 0) warp_n[w] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            u32 acc = 0;
+            for (int i = 0; i < 32; ++i) {
+                warp_off[i] = acc;
+                acc += warp_n[i];
+            }
+            round_n = acc;
+        }
+        __syncthreads();
+        if (occ) {
+            const u32 id = base + warp_off[w] + __popc(bal & ((1u << lane) - 1u));
+            ids[slot] = id;
+            if (id < static_cast<u32>(kMaxDict)) dict[id] = vals[slot];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) base += round_n;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = static_cast<int>(base);
+}
+
+// The device's default memory pool keeps up to 256 MB of freed scratch between builds (the default releases
+// everything at each synchronisation, which makes many small builds pay for fresh allocations).
+void keep_pool_scratch() {
+    static std::once_flag once[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::call_once(once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+        std::uint64_t keep = 256ULL << 20;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    });
+}
+
+// Stream-ordered scratch from the device's memory pool (freed in stream order).
+template <class T> struct PoolBuf {
+    T* p = nullptr;
+    explicit PoolBuf(std::size_t count) {
+        if (count) cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), nullptr), "cudaMallocAsync");
+    }
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    ~PoolBuf() {
+        if (p) cudaFreeAsync(p, nullptr);
+    }
+};
 
 // A warp per row (the reference's csr_count / csr_fill, src/gpu/rep_matvec.cu:933-989, likewise deal a row's
 // groups to the lanes of a warp). Lane l tests groups l, l + 32, ...; the acting ones' entries land in the
@@ -384,7 +450,6 @@ void run_pass(const qb_sector* row, const qb_sector* col, const qb_program* P, i
     k<<<blocks, 32 * kBuildWarps, smem>>>(row->view(), col->view(), P->view, in_smem, stage_bytes, pass, counts,
                                           row_ptr, col_out, ids, id_bytes, full, D, too_long);
     cuda_check(cudaGetLastError(), "CSR build pass");
-    cuda_check(cudaDeviceSynchronize(), "CSR build pass");
 }
 
 template <class ST>
@@ -467,73 +532,77 @@ int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* p
             return;
         }
         const bool narrow = row->N <= 32 && col->N <= 32;
-        DevBuf<int> flags(3);
-        cuda_check(cudaMemset(flags.p, 0, 12), "flags clear");
-        DevBuf<unsigned long long> counts(row->dim);
-        Dict D{nullptr, nullptr, nullptr, flags.p + 1, reinterpret_cast<u32*>(flags.p + 2)};
-        auto passes = [&](int pass, unsigned char* ids, int id_bytes, double2* full) {
-            if (narrow)
-                build_passes<u32>(row, col, prog, pass, counts.p, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
-                                  flags.p);
-            else
-                build_passes<u64>(row, col, prog, pass, counts.p, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
-                                  flags.p);
-        };
-        passes(0, nullptr, 0, nullptr);
-        int too_long = 0;
-        cuda_check(cudaMemcpy(&too_long, flags.p, 4, cudaMemcpyDeviceToHost), "flags read");
-        if (too_long) throw Error(QB_EUNSUPPORTED, "CSR: a row has more than 256 entries before merging");
-        // row_ptr = exclusive scan of the counts, then the total
-        std::size_t tmp = 0;
-        cub::DeviceScan::InclusiveSum(nullptr, tmp, counts.p, A->row_ptr.p + 1, static_cast<int>(row->dim));
-        DevBuf<unsigned char> tmpb(std::max<std::size_t>(tmp, 1));
-        cub::DeviceScan::InclusiveSum(tmpb.p, tmp, counts.p, A->row_ptr.p + 1, static_cast<int>(row->dim));
-        cuda_check(cudaGetLastError(), "CSR scan");
+        keep_pool_scratch();
+        // flags: [0] a row past 256 entries, [1] dictionary overflow, [2] values inserted, [3] dictionary size
+        PoolBuf<int> flags(4);
+        cuda_check(cudaMemsetAsync(flags.p, 0, 16, nullptr), "flags clear");
+        int hflags[4] = {0, 0, 0, 0};
+        Dict D{nullptr, 0, nullptr, nullptr, flags.p + 1, reinterpret_cast<u32*>(flags.p + 2)};
+        {
+            PoolBuf<unsigned long long> counts(row->dim);
+            auto passes = [&](int pass, unsigned char* ids, int id_bytes, double2* full) {
+                if (narrow)
+                    build_passes<u32>(row, col, prog, pass, counts.p, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full,
+                                      D, flags.p);
+                else
+                    build_passes<u64>(row, col, prog, pass, counts.p, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full,
+                                      D, flags.p);
+            };
+            passes(0, nullptr, 0, nullptr);
+            // row_ptr[1:] = inclusive scan of the counts
+            std::size_t tmp = 0;
+            cub::DeviceScan::InclusiveSum(nullptr, tmp, counts.p, A->row_ptr.p + 1, static_cast<int>(row->dim));
+            PoolBuf<unsigned char> tmpb(std::max<std::size_t>(tmp, 1));
+            cub::DeviceScan::InclusiveSum(tmpb.p, tmp, counts.p, A->row_ptr.p + 1, static_cast<int>(row->dim));
+            cuda_check(cudaGetLastError(), "CSR scan");
+        }
         cuda_check(cudaMemcpy(&A->nnz, A->row_ptr.p + row->dim, 8, cudaMemcpyDeviceToHost), "nnz read");
-        counts.release();
-        // the dictionary
-        const std::size_t nslots = std::size_t{1} << kDictBits;
-        DevBuf<u64> keys(nslots);
-        DevBuf<double2> dvals(nslots);
-        DevBuf<u32> dids(nslots);
-        cuda_check(cudaMemset(keys.p, 0xFF, nslots * 8), "dict clear");
+        cuda_check(cudaMemcpy(hflags, flags.p, 16, cudaMemcpyDeviceToHost), "flags read");
+        if (hflags[0]) throw Error(QB_EUNSUPPORTED, "CSR: a row has more than 256 entries before merging");
+        // the value set: at most half full while it can still become a dictionary
+        u64 nslots = 1024;
+        while (nslots < 2 * A->nnz && nslots < (1ULL << kDictBits)) nslots <<= 1;
+        PoolBuf<u64> keys(nslots);
+        PoolBuf<double2> dvals(nslots);
+        PoolBuf<u32> dids(nslots);
+        PoolBuf<double2> dict(kMaxDict);
+        cuda_check(cudaMemsetAsync(keys.p, 0xFF, nslots * 8, nullptr), "dict clear");
         D.keys = keys.p;
+        D.mask = nslots - 1;
         D.vals = dvals.p;
         D.ids = dids.p;
+        auto passes = [&](int pass, unsigned char* ids, int id_bytes, double2* full) {
+            if (narrow)
+                build_passes<u32>(row, col, prog, pass, nullptr, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
+                                  flags.p);
+            else
+                build_passes<u64>(row, col, prog, pass, nullptr, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
+                                  flags.p);
+        };
         passes(1, nullptr, 0, nullptr);
-        std::vector<u64> hk(nslots);
-        std::vector<double2> hv(nslots);
-        int overflow = 0;
-        cuda_check(cudaMemcpy(hk.data(), keys.p, nslots * 8, cudaMemcpyDeviceToHost), "dict read");
-        cuda_check(cudaMemcpy(hv.data(), dvals.p, nslots * 16, cudaMemcpyDeviceToHost), "dict read");
-        cuda_check(cudaMemcpy(&overflow, flags.p + 1, 4, cudaMemcpyDeviceToHost), "dict read");
-        std::vector<u32> hid(nslots, 0);
-        std::vector<double2> dict;
-        for (std::size_t i = 0; i < nslots; ++i)
-            if (hk[i] != kEmpty) {
-                hid[i] = static_cast<u32>(dict.size());
-                dict.push_back(hv[i]);
-            }
-        int id_bytes = dict_id_bytes(dict.size(), A->nnz);
-        if (overflow) id_bytes = 0;
-        check_budget(row->dim, A->nnz, id_bytes, dict.size(), max_bytes);
+        dict_compact<<<1, 1024>>>(keys.p, dvals.p, nslots, dids.p, dict.p, flags.p + 3);
+        cuda_check(cudaGetLastError(), "dictionary");
+        cuda_check(cudaMemcpy(hflags, flags.p, 16, cudaMemcpyDeviceToHost), "dictionary read");
+        const std::size_t n_dict = static_cast<std::size_t>(hflags[3]);
+        int id_bytes = hflags[1] ? 0 : dict_id_bytes(n_dict, A->nnz);
+        check_budget(row->dim, A->nnz, id_bytes, n_dict, max_bytes);
         A->col_idx.alloc(padded(A->nnz));
         for (int attempt = 0; attempt < 2; ++attempt) {
             if (id_bytes) {
-                cuda_check(cudaMemcpy(dids.p, hid.data(), nslots * 4, cudaMemcpyHostToDevice), "dict ids");
                 A->ids.alloc(padded(A->nnz) * id_bytes);
-                A->vals.upload(dict);
-                A->n_dict = static_cast<int>(dict.size());
+                A->vals.alloc(n_dict);
+                cuda_check(cudaMemcpy(A->vals.p, dict.p, n_dict * 16, cudaMemcpyDeviceToDevice), "dictionary copy");
+                A->n_dict = static_cast<int>(n_dict);
             } else {
                 A->ids.release();
                 A->vals.alloc(A->nnz);
                 A->n_dict = 0;
             }
             A->id_bytes = id_bytes;
-            cuda_check(cudaMemset(flags.p + 1, 0, 4), "flags clear");
+            cuda_check(cudaMemsetAsync(flags.p + 1, 0, 4, nullptr), "flags clear");
             passes(2, A->ids.p, id_bytes, A->vals.p);
-            cuda_check(cudaMemcpy(&overflow, flags.p + 1, 4, cudaMemcpyDeviceToHost), "fill read");
-            if (!overflow || id_bytes == 0) break;
+            cuda_check(cudaMemcpy(hflags, flags.p, 16, cudaMemcpyDeviceToHost), "fill read");
+            if (!hflags[1] || id_bytes == 0) break;
             id_bytes = 0;   // a key collision: store every value whole
             A->ids.release();
             check_budget(row->dim, A->nnz, 0, 0, max_bytes);

@@ -24,6 +24,8 @@
 //   qb_cf           the T = 0 continued fraction (include/ed/dynamics/cf.h:39-160).
 // =============================================================================
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -32,6 +34,8 @@
 #include <mutex>
 #include <numeric>
 #include <random>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "qb_internal.cuh"
@@ -940,6 +944,338 @@ ScanOut run_scan(Recurrence& R, int max_iter, int reorth, bool gate, double brea
 
 double norm_bound(const qb_program* p) { return p->norm_bound > 0.0 ? p->norm_bound : 1.0; }
 
+// ---- FTLM: sample tables, the block recurrence of one sector's samples, the curves ----
+// The sample vectors of a call: sample s of every block is the first n_b draws of sample_engine(seed, s)
+// (the reference gives every block of a thermal call the same base seed, src/engine/thermal.cpp:363, and
+// draws a block's vector as gaussian_vector(n_b, gen), include/ed/thermal/sample_seed.h:84-89). So one table
+// of k streams, as long as the largest block, holds every block's samples as prefixes; a block normalises its
+// prefix. The table is drawn on host threads with the reference's own generator and distribution.
+std::vector<std::complex<double>> sample_table(std::uint64_t seed, int k, std::uint64_t len) {
+    std::vector<std::complex<double>> G(static_cast<std::size_t>(k) * len);
+    auto draw = [&](int s) {
+        std::mt19937 gen = sample_engine(seed, static_cast<std::uint64_t>(s));
+        std::normal_distribution<double> nd(0.0, 1.0);
+        std::complex<double>* g = G.data() + static_cast<std::size_t>(s) * len;
+        for (std::uint64_t i = 0; i < len; ++i) {
+            const double im = nd(gen);   // the imaginary part is drawn first (see gaussian_fill)
+            const double re = nd(gen);
+            g[i] = std::complex<double>(re, im);
+        }
+    };
+    const int nt = std::max(1, std::min<int>(k, static_cast<int>(std::thread::hardware_concurrency())));
+    std::vector<std::thread> pool;
+    std::atomic<int> next{0};
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (int s = next++; s < k; s = next++) draw(s);
+        });
+    for (auto& t : pool) t.join();
+    return G;
+}
+
+// One CTA per sample: 1 / ||G[s][0, n)|| by a fixed-order tree sum (the reference normalises with dznrm2).
+__global__ void k_sample_norms(std::uint64_t n, const double2* G, std::uint64_t ld, double* inv) {
+    __shared__ double sm[32];
+    const double2* g = G + static_cast<std::size_t>(blockIdx.x) * ld;
+    double v[1] = {0.0};
+    for (std::uint64_t i = threadIdx.x; i < n; i += blockDim.x) v[0] += g[i].x * g[i].x + g[i].y * g[i].y;
+    block_reduce<1>(v, sm);
+    if (threadIdx.x == 0) inv[blockIdx.x] = v[0] > 0.0 ? 1.0 / sqrt(v[0]) : 0.0;
+}
+
+// w[i][s] = G[s][i] / ||G[s][0, n)||, the block's samples interleaved by row.
+__global__ void k_sample_start(std::uint64_t n, int k, const double2* G, std::uint64_t ld, const double* inv,
+                               double2* w) {
+    const std::uint64_t total = n * k;
+    for (std::uint64_t t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const int s = static_cast<int>(t % k);
+        const std::uint64_t i = t / k;
+        const double2 g = G[static_cast<std::size_t>(s) * ld + i];
+        w[t] = make_double2(g.x * inv[s], g.y * inv[s]);
+    }
+}
+
+// The scratch of one stream's block recurrences, grown to the largest block it runs.
+struct BlockBufs {
+    DevBuf<double2> w;
+    DevBuf<unsigned char> vb[2];
+    DevBuf<double> alpha, beta, ovl, part, inv;
+    DevBuf<unsigned> cnt;
+    void ensure(std::uint64_t n, int k, int cap, std::size_t es) {
+        const std::size_t nk = static_cast<std::size_t>(n) * k;
+        if (w.n < nk) w.alloc(nk);
+        for (auto& b : vb)
+            if (b.n < nk * es) b.alloc(nk * es);
+        if (alpha.n < static_cast<std::size_t>(cap) * k) alpha.alloc(static_cast<std::size_t>(cap) * k);
+        if (beta.n < static_cast<std::size_t>(cap + 1) * k) beta.alloc(static_cast<std::size_t>(cap + 1) * k);
+        if (ovl.n == 0) ovl.alloc(2 * kMaxCols);
+        if (part.n == 0) part.alloc(static_cast<std::size_t>(3) * kMaxCols * kMaxRedBlocks);
+        if (inv.n == 0) inv.alloc(kMaxCols);
+        if (cnt.n == 0) cnt.alloc(1);
+    }
+};
+
+// The lock-step recurrence of one block's k sample columns (ftlm_kernel's per-sample Lanczos with the
+// local reorthogonalisation, include/ed/thermal/ftlm.h:277-480), from the unit start columns in B.w
+// (FP64, interleaved by row), cap steps; queues alpha [cap][k] and beta [cap + 1][k] into host memory on st.
+// The matvec runs on the block's reduced CSR when one is given, else on the row walk.
+void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr* csr, int k, int cap, double tol,
+                      int dtype, BlockBufs& B, cudaStream_t st, double* h_alpha, double* h_beta) {
+    const std::uint64_t n = sec->dim;
+    const std::size_t nk = static_cast<std::size_t>(n) * k;
+    const std::size_t es = dtype == QB_C64 ? 8 : 16;
+    cuda_check(cudaMemsetAsync(B.vb[0].p, 0, nk * es, st), "zero");
+    if (dtype == QB_C64)
+        k_cast_from<float2><<<red_blocks(nk), kThreads, 0, st>>>(nk, B.w.p, reinterpret_cast<float2*>(B.vb[1].p));
+    else
+        cuda_check(cudaMemcpyAsync(B.vb[1].p, B.w.p, nk * 16, cudaMemcpyDeviceToDevice, st), "copy");
+    cuda_check(cudaMemsetAsync(B.beta.p, 0, static_cast<std::size_t>(cap + 1) * k * 8, st), "zero");
+    cuda_check(cudaMemsetAsync(B.cnt.p, 0, 4, st), "zero");
+    BScal S{B.alpha.p, B.beta.p, B.ovl.p, B.part.p, B.cnt.p};
+    int cur = 1;
+    const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kMaxRedBlocks)));
+    const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
+    for (int j = 0; j < cap; ++j) {
+        void* vc = B.vb[cur].p;
+        void* vp = B.vb[cur ^ 1].p;
+        if (csr)
+            csr_spmv(csr, vc, B.w.p, k, dtype, QB_C128, st);
+        else if (k == 1)
+            launch_walk_mixed(sec, sec, prog, vc, B.w.p, dtype, QB_C128, st);   // one sample: the plain walk
+        else
+            launch_block_mixed(sec, sec, prog, vc, B.w.p, k, dtype, QB_C128, st);
+        if (dtype == QB_C64) {
+            if (k <= 32) {
+                brec_alpha<float2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, B.w.p, (float2*)vp, (float2*)vc, S);
+                brec_beta<float2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, 1, B.w.p, (float2*)vc, S);
+            } else {
+                brec_alpha<float2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, B.w.p, (float2*)vp, (float2*)vc, S);
+                brec_beta<float2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, 1, B.w.p, (float2*)vc, S);
+            }
+            brec_next<float2><<<red_blocks(nk), kThreads, 0, st>>>(n, k, j, tol, B.w.p, (float2*)vc, (float2*)vp, S);
+        } else {
+            if (k <= 32) {
+                brec_alpha<double2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, B.w.p, (double2*)vp, (double2*)vc, S);
+                brec_beta<double2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, 1, B.w.p, (double2*)vc, S);
+            } else {
+                brec_alpha<double2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, B.w.p, (double2*)vp, (double2*)vc, S);
+                brec_beta<double2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, 1, B.w.p, (double2*)vc, S);
+            }
+            brec_next<double2><<<red_blocks(nk), kThreads, 0, st>>>(n, k, j, tol, B.w.p, (double2*)vc, (double2*)vp, S);
+        }
+        cuda_check(cudaGetLastError(), "ftlm step");
+        cur ^= 1;
+    }
+    cuda_check(cudaMemcpyAsync(h_alpha, B.alpha.p, static_cast<std::size_t>(cap) * k * 8, cudaMemcpyDeviceToHost, st),
+               "alpha");
+    cuda_check(cudaMemcpyAsync(h_beta, B.beta.p, static_cast<std::size_t>(cap + 1) * k * 8, cudaMemcpyDeviceToHost, st),
+               "beta");
+}
+
+// A block's curves from its samples' alpha / beta: each sample's run up to its breakdown, its Ritz values and
+// first-component weights, moments about its lowest level (sample_moments, ftlm.h:165-192), then the samples
+// combined (combine_samples, ftlm.h:199-235): lnZ = ln n + ln<Z> - beta e_ref, E, V.
+void block_curves(const double* ha, const double* hb, int k, int cap, double tol, std::uint64_t n,
+                  const double* betas, int n_beta, double* lnZ, double* E, double* V, double* e_min) {
+    struct Mom {
+        double e_min;
+        std::vector<double> Z, E1, E2;
+    };
+    std::vector<Mom> mom;
+    double gs = std::numeric_limits<double>::infinity();
+    for (int s = 0; s < k; ++s) {
+        std::vector<double> a, b;
+        b.push_back(0.0);
+        for (int j = 0; j < cap; ++j) {
+            a.push_back(ha[static_cast<std::size_t>(j) * k + s]);
+            b.push_back(hb[static_cast<std::size_t>(j + 1) * k + s]);
+            if (b.back() < tol) break;
+        }
+        std::vector<double> d(a), e(a.size() > 1 ? a.size() - 1 : 1, 0.0), vals, z0;
+        for (std::size_t i = 0; i + 1 < a.size(); ++i) e[i] = b[i + 1];
+        eig_first_row(d, e, vals, z0);
+        Mom mo;
+        mo.e_min = std::numeric_limits<double>::infinity();
+        std::vector<double> wts(vals.size());
+        for (std::size_t i = 0; i < vals.size(); ++i) {
+            wts[i] = z0[i] * z0[i];
+            if (wts[i] > 0.0) mo.e_min = std::min(mo.e_min, vals[i]);
+        }
+        if (!std::isfinite(mo.e_min)) mo.e_min = *std::min_element(vals.begin(), vals.end());
+        for (int t = 0; t < n_beta; ++t) {
+            double zz = 0.0, e1 = 0.0, e2 = 0.0;
+            for (std::size_t i = 0; i < vals.size(); ++i) {
+                const double x = vals[i] - mo.e_min;
+                const double bb = wts[i] * std::exp(-betas[t] * x);
+                zz += bb;
+                e1 += x * bb;
+                e2 += x * x * bb;
+            }
+            mo.Z.push_back(zz);
+            mo.E1.push_back(e1);
+            mo.E2.push_back(e2);
+        }
+        gs = std::min(gs, mo.e_min);
+        mom.push_back(std::move(mo));
+    }
+    double e_ref = mom.front().e_min;
+    for (const auto& m : mom) e_ref = std::min(e_ref, m.e_min);
+    const double ln_n = std::log(static_cast<double>(n));
+    for (int t = 0; t < n_beta; ++t) {
+        const double beta = betas[t];
+        double zz = 0.0, e1 = 0.0, e2 = 0.0;
+        for (const auto& m : mom) {
+            const double dd = m.e_min - e_ref, r = std::exp(-beta * dd);
+            zz += m.Z[t] * r;
+            e1 += (m.E1[t] + dd * m.Z[t]) * r;
+            e2 += (m.E2[t] + 2.0 * dd * m.E1[t] + dd * dd * m.Z[t]) * r;
+        }
+        zz /= k;
+        e1 /= k;
+        e2 /= k;
+        if (zz > 1e-300) {
+            const double m1 = e1 / zz, m2 = e2 / zz;
+            lnZ[t] = ln_n + std::log(zz) - beta * e_ref;
+            E[t] = e_ref + m1;
+            V[t] = std::max(m2 - m1 * m1, 0.0);
+        } else {
+            lnZ[t] = -beta * e_ref;
+            E[t] = e_ref;
+            V[t] = 0.0;
+        }
+    }
+    *e_min = gs;
+}
+
+// Pinned host memory owned by a host object.
+template <class T> struct PinnedBuf {
+    T* p = nullptr;
+    std::size_t n = 0;
+    explicit PinnedBuf(std::size_t count) : n(count) {
+        if (count) cuda_check(cudaMallocHost(reinterpret_cast<void**>(&p), count * sizeof(T)), "cudaMallocHost");
+    }
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// FTLM over many blocks (qb_ftlm_blocks; one block: qb_ftlm).
+void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int k, int depth,
+                 std::uint64_t seed, const double* betas, int n_beta, int dtype, bool use_csr, double* lnZ, double* E,
+                 double* V, double* e_min, double* stats) {
+    using clock = std::chrono::steady_clock;
+    auto secs_since = [](clock::time_point t0) { return std::chrono::duration<double>(clock::now() - t0).count(); };
+    auto t_phase = clock::now();
+    double st_draw = 0.0, st_csr = 0.0, st_rec = 0.0, st_curves = 0.0;
+    if (k < 1 || k > kMaxCols) throw Error(QB_EINVAL, "samples must be in [1, 64]");
+    if (depth < 2) throw Error(QB_EINVAL, "depth must be >= 2");
+    if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "bad dtype");
+    if (n_blocks < 1 || !secs || !progs) throw Error(QB_EINVAL, "no blocks");
+    std::uint64_t len = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        if (!secs[b] || !progs[b]) throw Error(QB_EINVAL, "null block");
+        if (secs[b]->dim == 0) throw Error(QB_EINVAL, "empty sector");
+        len = std::max(len, secs[b]->dim);
+    }
+    const std::size_t es = dtype == QB_C64 ? 8 : 16;
+    // the samples of every block: one table, drawn once
+    const std::vector<std::complex<double>> G = sample_table(seed, k, len);
+    DevBuf<double2> dG(G.size());
+    cuda_check(cudaMemcpy(dG.p, G.data(), G.size() * 16, cudaMemcpyHostToDevice), "samples upload");
+    st_draw = secs_since(t_phase);
+    // blocks, largest first, dealt round robin to a few streams so small blocks overlap
+    std::vector<int> order(n_blocks);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return secs[a]->dim > secs[b]->dim; });
+    const int ns = std::min(n_blocks, 4);
+    std::vector<cudaStream_t> streams(ns);
+    for (auto& st : streams) cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    struct StreamGuard {
+        std::vector<cudaStream_t>& s;
+        ~StreamGuard() {
+            for (auto st : s)
+                if (st) cudaStreamDestroy(st);
+        }
+    } guard{streams};
+    std::vector<BlockBufs> bufs(ns);
+    std::vector<int> caps(n_blocks);
+    std::vector<std::size_t> a_off(n_blocks), b_off(n_blocks);
+    std::size_t a_tot = 0, b_tot = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        caps[b] = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(depth), secs[b]->dim));
+        a_off[b] = a_tot;
+        b_off[b] = b_tot;
+        a_tot += static_cast<std::size_t>(caps[b]) * k;
+        b_tot += static_cast<std::size_t>(caps[b] + 1) * k;
+    }
+    PinnedBuf<double> ha(a_tot), hb(b_tot);
+    std::vector<double> tol(n_blocks);
+    // every block's reduced CSR, built before the recurrences (a build synchronises the device); a block
+    // whose CSR does not fit runs on the walk
+    struct Csrs {
+        std::vector<qb_csr*> h;
+        ~Csrs() {
+            for (auto* c : h)
+                if (c) qb_csr_destroy(c);
+        }
+    } csrs{std::vector<qb_csr*>(n_blocks, nullptr)};
+    t_phase = clock::now();
+    if (use_csr)
+        for (int b = 0; b < n_blocks; ++b)
+            if (qb_csr_build(secs[b], secs[b], progs[b], 0, &csrs.h[b]) != QB_OK) csrs.h[b] = nullptr;
+    st_csr = secs_since(t_phase);
+    t_phase = clock::now();
+    for (int i = 0; i < n_blocks; ++i) {
+        const int b = order[i];
+        const int si = i % ns;
+        cudaStream_t st = streams[si];
+        const qb_sector* sec = secs[b];
+        const std::uint64_t n = sec->dim;
+        tol[b] = 64.0 * std::numeric_limits<double>::epsilon() * norm_bound(progs[b]);
+        // the buffers grow on the host's side of the stream: wait for the stream's previous block first
+        BlockBufs& B = bufs[si];
+        const bool grow = B.w.n < static_cast<std::size_t>(n) * k || B.alpha.n < static_cast<std::size_t>(caps[b]) * k;
+        if (grow) cuda_check(cudaStreamSynchronize(st), "stream");
+        B.ensure(n, k, caps[b], es);
+        k_sample_norms<<<k, kThreads, 0, st>>>(n, dG.p, len, B.inv.p);
+        k_sample_start<<<red_blocks(static_cast<std::uint64_t>(n) * k), kThreads, 0, st>>>(n, k, dG.p, len, B.inv.p,
+                                                                                            B.w.p);
+        block_recurrence(sec, progs[b], csrs.h[b], k, caps[b], tol[b], dtype, B, st, ha.p + a_off[b], hb.p + b_off[b]);
+    }
+    for (auto st : streams) cuda_check(cudaStreamSynchronize(st), "ftlm blocks");
+    st_rec = secs_since(t_phase);
+    t_phase = clock::now();
+    // the curves, on host threads
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    const int nt = std::max(1, std::min<int>(n_blocks, static_cast<int>(std::thread::hardware_concurrency())));
+    std::vector<std::string> errs(nt);
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            try {
+                for (int b = next++; b < n_blocks; b = next++)
+                    block_curves(ha.p + a_off[b], hb.p + b_off[b], k, caps[b], tol[b], secs[b]->dim, betas, n_beta,
+                                 lnZ + static_cast<std::size_t>(b) * n_beta, E + static_cast<std::size_t>(b) * n_beta,
+                                 V + static_cast<std::size_t>(b) * n_beta, e_min + b);
+            } catch (const std::exception& e) {
+                errs[t] = e.what();
+            }
+        });
+    for (auto& t : pool) t.join();
+    for (const auto& e : errs)
+        if (!e.empty()) throw Error(QB_EINVAL, e);
+    st_curves = secs_since(t_phase);
+    if (stats) {
+        stats[0] = st_draw;
+        stats[1] = st_csr;
+        stats[2] = st_rec;
+        stats[3] = st_curves;
+    }
+}
+
 // ---- the allocation-free Lanczos (qb_lanczos_noalloc) ----
 // Its scratch -- the alpha / beta history, the local-projection overlap, the block partials of the
 // deterministic reductions and the last-block counter -- lives in this file-scope device array, held by
@@ -1116,150 +1452,58 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
     return qb::guarded([&] {
         using namespace qb;
         if (!sec || !prog || !betas || !lnZ || !E || !V || !e_min) throw Error(QB_EINVAL, "null argument");
-        if (samples < 1 || samples > kMaxCols) throw Error(QB_EINVAL, "samples must be in [1, 64]");
-        if (depth < 2) throw Error(QB_EINVAL, "depth must be >= 2");
-        if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "bad dtype");
-        const std::uint64_t n = sec->dim;
-        if (n == 0) throw Error(QB_EINVAL, "empty sector");
-        const int k = samples;
-        const int cap = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(depth), n));
-        const double tol = 64.0 * std::numeric_limits<double>::epsilon() * norm_bound(prog);
-        const std::size_t es = dtype == QB_C64 ? 8 : 16;
-        // the sample vectors, interleaved by row
-        std::vector<std::complex<double>> host(n * k);
-        for (int s = 0; s < k; ++s) {
-            std::mt19937 gen = sample_engine(seed, static_cast<std::uint64_t>(s));
-            std::normal_distribution<double> nd(0.0, 1.0);
-            double n2 = 0.0;
-            for (std::uint64_t i = 0; i < n; ++i) {
-                const double im = nd(gen);   // the imaginary part is drawn first (see gaussian_fill)
-                const double re = nd(gen);
-                host[i * k + s] = std::complex<double>(re, im);
+        const qb_sector* secs[1] = {sec};
+        const qb_program* progs[1] = {prog};
+        // the program's own lane: its attached CSR for this sector, else the walk
+        ftlm_blocks(secs, progs, 1, samples, depth, seed, betas, n_beta, dtype, false, lnZ, E, V, e_min, nullptr);
+    });
+}
+
+int qb_ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int samples, int depth,
+                   uint64_t seed, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ, double* E,
+                   double* V, double* e_min, double* stats) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!betas || !lnZ || !E || !V || !e_min) throw Error(QB_EINVAL, "null argument");
+        ftlm_blocks(secs, progs, n_blocks, samples, depth, seed, betas, n_beta, dtype, use_csr != 0, lnZ, E, V, e_min,
+                    stats);
+    });
+}
+
+int qb_thermal_combine(int n_blocks, const double* weights, const double* lnZ, const double* E, const double* V,
+                       const double* betas, int n_beta, double* lnZ_out, double* E_out, double* C_out, double* S_out,
+                       double* F_out) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (n_blocks < 1 || !lnZ || !E || !V || !betas || !lnZ_out || !E_out || !C_out || !S_out || !F_out)
+            throw Error(QB_EINVAL, "null argument");
+        std::vector<double> p(n_blocks);
+        for (int i = 0; i < n_beta; ++i) {
+            auto at = [&](const double* a, int b) { return a[static_cast<std::size_t>(b) * n_beta + i]; };
+            double mx = -std::numeric_limits<double>::infinity();
+            for (int b = 0; b < n_blocks; ++b)
+                mx = std::max(mx, std::log(weights ? weights[b] : 1.0) + at(lnZ, b));
+            double z = 0.0, e = 0.0;
+            for (int b = 0; b < n_blocks; ++b) {
+                p[b] = std::exp(std::log(weights ? weights[b] : 1.0) + at(lnZ, b) - mx);
+                z += p[b];
+                e += p[b] * at(E, b);
             }
-            for (std::uint64_t i = 0; i < n; ++i) n2 += std::norm(host[i * k + s]);
-            const double inv = 1.0 / std::sqrt(n2);
-            for (std::uint64_t i = 0; i < n; ++i) host[i * k + s] *= inv;
+            e /= z;
+            // the law of total variance: each block's variance plus the spread of the block means
+            double var = 0.0;
+            for (int b = 0; b < n_blocks; ++b) {
+                const double d = at(E, b) - e;
+                var += p[b] * (at(V, b) + d * d);
+            }
+            var /= z;
+            const double bt = betas[i];
+            lnZ_out[i] = mx + std::log(z);
+            E_out[i] = e;
+            C_out[i] = bt * bt * var;
+            S_out[i] = lnZ_out[i] + bt * e;
+            F_out[i] = -lnZ_out[i] / bt;
         }
-        (void)0;
-        DevBuf<double2> w(n * k);
-        DevBuf<unsigned char> vb[2];
-        vb[0].alloc(n * k * es);
-        vb[1].alloc(n * k * es);
-        cudaStream_t st = nullptr;
-        cuda_check(cudaMemcpy(w.p, host.data(), n * k * 16, cudaMemcpyHostToDevice), "samples upload");
-        cuda_check(cudaMemset(vb[0].p, 0, n * k * es), "zero");
-        if (dtype == QB_C64)
-            k_cast_from<float2><<<red_blocks(n * k), kThreads>>>(n * k, w.p, reinterpret_cast<float2*>(vb[1].p));
-        else
-            cuda_check(cudaMemcpy(vb[1].p, w.p, n * k * 16, cudaMemcpyDeviceToDevice), "copy");
-        DevBuf<double> d_alpha(static_cast<std::size_t>(cap) * k), d_beta(static_cast<std::size_t>(cap + 1) * k),
-            d_ovl(2 * kMaxCols), d_part(static_cast<std::size_t>(3) * kMaxCols * kMaxRedBlocks);
-        DevBuf<unsigned> d_cnt(1);
-        cuda_check(cudaMemset(d_beta.p, 0, (cap + 1) * k * 8), "zero");
-        cuda_check(cudaMemset(d_cnt.p, 0, 4), "zero");
-        BScal S{d_alpha.p, d_beta.p, d_ovl.p, d_part.p, d_cnt.p};
-        int cur = 1;
-        const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kMaxRedBlocks)));
-        const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
-        for (int j = 0; j < cap; ++j) {
-            void* vc = vb[cur].p;
-            void* vp = vb[cur ^ 1].p;
-            launch_block_mixed(sec, sec, prog, vc, w.p, k, dtype, QB_C128, st);
-            if (dtype == QB_C64) {
-                if (k <= 32) {
-                    brec_alpha<float2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, w.p, (float2*)vp, (float2*)vc, S);
-                    brec_beta<float2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, 1, w.p, (float2*)vc, S);
-                } else {
-                    brec_alpha<float2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, w.p, (float2*)vp, (float2*)vc, S);
-                    brec_beta<float2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, 1, w.p, (float2*)vc, S);
-                }
-                brec_next<float2><<<red_blocks(n * k), kThreads, 0, st>>>(n, k, j, tol, w.p, (float2*)vc, (float2*)vp, S);
-            } else {
-                if (k <= 32) {
-                    brec_alpha<double2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, w.p, (double2*)vp, (double2*)vc, S);
-                    brec_beta<double2, 1><<<rb, kThreads, bsm, st>>>(n, k, j, 1, w.p, (double2*)vc, S);
-                } else {
-                    brec_alpha<double2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, w.p, (double2*)vp, (double2*)vc, S);
-                    brec_beta<double2, 2><<<rb, kThreads, bsm, st>>>(n, k, j, 1, w.p, (double2*)vc, S);
-                }
-                brec_next<double2><<<red_blocks(n * k), kThreads, 0, st>>>(n, k, j, tol, w.p, (double2*)vc, (double2*)vp, S);
-            }
-            cuda_check(cudaGetLastError(), "ftlm step");
-            cur ^= 1;
-        }
-        std::vector<double> ha(static_cast<std::size_t>(cap) * k), hb(static_cast<std::size_t>(cap + 1) * k);
-        cuda_check(cudaMemcpy(ha.data(), d_alpha.p, ha.size() * 8, cudaMemcpyDeviceToHost), "alpha");
-        cuda_check(cudaMemcpy(hb.data(), d_beta.p, hb.size() * 8, cudaMemcpyDeviceToHost), "beta");
-        // per sample: its run up to its breakdown, Ritz values and weights, moments (ftlm.h:165-192)
-        struct Mom {
-            double e_min;
-            std::vector<double> Z, E1, E2;
-        };
-        std::vector<Mom> mom;
-        double gs = std::numeric_limits<double>::infinity();
-        for (int s = 0; s < k; ++s) {
-            std::vector<double> a, b;
-            b.push_back(0.0);
-            for (int j = 0; j < cap; ++j) {
-                a.push_back(ha[static_cast<std::size_t>(j) * k + s]);
-                b.push_back(hb[static_cast<std::size_t>(j + 1) * k + s]);
-                if (b.back() < tol) break;
-            }
-            std::vector<double> d(a), e(a.size() > 1 ? a.size() - 1 : 1, 0.0), vals, z0;
-            for (std::size_t i = 0; i + 1 < a.size(); ++i) e[i] = b[i + 1];
-            eig_first_row(d, e, vals, z0);
-            Mom mo;
-            mo.e_min = std::numeric_limits<double>::infinity();
-            std::vector<double> wts(vals.size());
-            for (std::size_t i = 0; i < vals.size(); ++i) {
-                wts[i] = z0[i] * z0[i];
-                if (wts[i] > 0.0) mo.e_min = std::min(mo.e_min, vals[i]);
-            }
-            if (!std::isfinite(mo.e_min)) mo.e_min = *std::min_element(vals.begin(), vals.end());
-            for (int t = 0; t < n_beta; ++t) {
-                double zz = 0.0, e1 = 0.0, e2 = 0.0;
-                for (std::size_t i = 0; i < vals.size(); ++i) {
-                    const double x = vals[i] - mo.e_min;
-                    const double bb = wts[i] * std::exp(-betas[t] * x);
-                    zz += bb;
-                    e1 += x * bb;
-                    e2 += x * x * bb;
-                }
-                mo.Z.push_back(zz);
-                mo.E1.push_back(e1);
-                mo.E2.push_back(e2);
-            }
-            gs = std::min(gs, mo.e_min);
-            mom.push_back(std::move(mo));
-        }
-        // combine_samples (ftlm.h:199-235)
-        double e_ref = mom.front().e_min;
-        for (const auto& m : mom) e_ref = std::min(e_ref, m.e_min);
-        const double ln_n = std::log(static_cast<double>(n));
-        for (int t = 0; t < n_beta; ++t) {
-            const double beta = betas[t];
-            double zz = 0.0, e1 = 0.0, e2 = 0.0;
-            for (const auto& m : mom) {
-                const double dd = m.e_min - e_ref, r = std::exp(-beta * dd);
-                zz += m.Z[t] * r;
-                e1 += (m.E1[t] + dd * m.Z[t]) * r;
-                e2 += (m.E2[t] + 2.0 * dd * m.E1[t] + dd * dd * m.Z[t]) * r;
-            }
-            zz /= k;
-            e1 /= k;
-            e2 /= k;
-            if (zz > 1e-300) {
-                const double m1 = e1 / zz, m2 = e2 / zz;
-                lnZ[t] = ln_n + std::log(zz) - beta * e_ref;
-                E[t] = e_ref + m1;
-                V[t] = std::max(m2 - m1 * m1, 0.0);
-            } else {
-                lnZ[t] = -beta * e_ref;
-                E[t] = e_ref;
-                V[t] = 0.0;
-            }
-        }
-        *e_min = gs;
     });
 }
 

@@ -247,6 +247,39 @@ def ftlm(sec: Sector, prog: Program, samples: int, depth: int, seed: int, betas,
     return dict(lnZ=lnZ, E=E, V=V, e_min=em.value)
 
 
+def ftlm_blocks(sectors, progs, samples: int, depth: int, seed: int, betas, dtype="c128", use_csr=True) -> dict:
+    """FTLM over many blocks (each a Sector; progs: one Program for all, or one per block). Returns the
+    per-block curves [n_blocks, n_beta] (lnZ, E, V), e_min [n_blocks], and their log-space combination
+    (lnZ, E, C, S, F over beta) under "total"."""
+    nb = len(sectors)
+    if isinstance(progs, Program):
+        progs = [progs] * nb
+    betas = np.ascontiguousarray(betas, np.float64)
+    nt = len(betas)
+    sh = (C.c_void_p * nb)(*[s.h.value for s in sectors])
+    ph = (C.c_void_p * nb)(*[p.h.value for p in progs])
+    lnZ, E, V = (np.zeros((nb, nt)) for _ in range(3))
+    e_min = np.zeros(nb)
+    stats = np.zeros(4)
+    check(lib().qb_ftlm_blocks(sh, ph, nb, samples, depth, seed, betas.ctypes.data, nt, _dt(dtype), int(bool(use_csr)),
+                               lnZ.ctypes.data, E.ctypes.data, V.ctypes.data, e_min.ctypes.data, stats.ctypes.data))
+    return {"lnZ": lnZ, "E": E, "V": V, "e_min": e_min, "total": thermal_combine(lnZ, E, V, betas),
+            "stats": dict(zip(("draw_s", "csr_build_s", "recurrence_s", "curves_s"), stats.tolist()))}
+
+
+def thermal_combine(lnZ, E, V, betas, weights=None) -> dict:
+    """Per-block curves [n_blocks, n_beta] combined in log space (the reference thermal driver's combine)."""
+    lnZ, E, V = (np.ascontiguousarray(a, np.float64) for a in (lnZ, E, V))
+    betas = np.ascontiguousarray(betas, np.float64)
+    nb, nt = lnZ.shape
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    out = {k: np.zeros(nt) for k in ("lnZ", "E", "C", "S", "F")}
+    check(lib().qb_thermal_combine(nb, None if w is None else w.ctypes.data, lnZ.ctypes.data, E.ctypes.data,
+                                   V.ctypes.data, betas.ctypes.data, nt, out["lnZ"].ctypes.data, out["E"].ctypes.data,
+                                   out["C"].ctypes.data, out["S"].ctypes.data, out["F"].ctypes.data))
+    return out
+
+
 def cf(sec: Sector, prog: Program, phi: np.ndarray, depth: int, omega, eta: float, shift: float = float("nan"),
        tolerance: float = 1e-12):
     phi = np.ascontiguousarray(phi, np.complex128)

@@ -1,0 +1,97 @@
+"""Batched FTLM over many blocks against the oracle, through the C-ABI.
+
+The blocks are every (S^z, momentum) sector of an XXZ chain in a field: the decomposition the thermal driver
+samples (config 3 at N = 12). Each block's curves are checked against the oracle's FTLM of that block with the
+call's base seed (tolerances written per test: 1e-8 relative for FP64 storage, 2e-4 for FP32), and the combined
+thermodynamics against the oracle's log-space combine.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qed_spin_b200 import lattice as lat
+from qed_spin_b200 import operators as ops
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+N = 12
+SEED = 20240601
+BETAS = 1.0 / np.linspace(0.1, 4.0, 40)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    from qed_spin_b200 import build
+    build.build()
+
+
+def _blocks():
+    specs = []
+    for n_up in range(N + 1):
+        for k in range(N):
+            spec = lat.chain_sector(N, n_up, k)
+            if O.Sector(spec).dim > 0:
+                specs.append(spec)
+    prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.5) + ops.zeeman_z_products(N, 0.1)
+    return specs, ops.row_program(ops.from_products(N, prods))
+
+
+@pytest.fixture(scope="module")
+def oracle_curves():
+    specs, prog = _blocks()
+    P = O.Program(prog)
+    curves = [O.Sector(s).ftlm(P, 8, 30, SEED, BETAS) for s in specs]
+    return specs, prog, curves
+
+
+@pytest.mark.parametrize("dtype,use_csr", [("c128", True), ("c128", False), ("c64", True)])
+def test_blocks_match_oracle(oracle_curves, dtype, use_csr):
+    from qed_spin_b200 import device as D
+    specs, prog, curves = oracle_curves
+    secs = [D.Sector(s) for s in specs]
+    P = D.Program(prog)
+    r = D.ftlm_blocks(secs, P, 8, 30, SEED, BETAS, dtype=dtype, use_csr=use_csr)
+    tol = 1e-8 if dtype == "c128" else 2e-4
+    assert len(curves) == r["lnZ"].shape[0] > 100
+    for b, c in enumerate(curves):
+        for key in ("lnZ", "E", "V"):
+            ref = np.asarray(c[key])
+            np.testing.assert_allclose(r[key][b], ref, rtol=tol, atol=tol * max(np.abs(ref).max(), 1e-3),
+                                       err_msg=f"block {b} {key}")
+        assert abs(r["e_min"][b] - c["e_min"]) <= tol * max(1.0, abs(c["e_min"]))
+    tot = O.combine_blocks(curves, BETAS)
+    for key in ("lnZ", "E", "C", "S", "F"):
+        np.testing.assert_allclose(r["total"][key], tot[key], rtol=tol, atol=tol * np.abs(tot[key]).max(),
+                                   err_msg=key)
+
+
+def test_combine_matches_oracle(oracle_curves):
+    """The C combine equals the oracle's restatement of the thermal driver's (1e-13 relative)."""
+    from qed_spin_b200 import device as D
+    _, _, curves = oracle_curves
+    lnZ = np.stack([c["lnZ"] for c in curves])
+    E = np.stack([c["E"] for c in curves])
+    V = np.stack([c["V"] for c in curves])
+    w = np.linspace(1.0, 2.0, len(curves))
+    got = D.thermal_combine(lnZ, E, V, BETAS, weights=w)
+    ref = O.combine_blocks(curves, BETAS, weights=w)
+    for key in got:
+        np.testing.assert_allclose(got[key], ref[key], rtol=1e-13, atol=1e-13 * np.abs(ref[key]).max())
+
+
+def test_one_block_call_equals_batch(oracle_curves):
+    """qb_ftlm on a block equals that block inside the batch (the same start vectors and recurrence)."""
+    from qed_spin_b200 import device as D
+    specs, prog, _ = oracle_curves
+    pick = [len(specs) // 2, len(specs) // 3]
+    secs = [D.Sector(specs[i]) for i in pick]
+    P = D.Program(prog)
+    r = D.ftlm_blocks(secs, P, 8, 30, SEED, BETAS, use_csr=False)
+    for j, s in enumerate(secs):
+        one = D.ftlm(s, P, 8, 30, SEED, BETAS)
+        for key in ("lnZ", "E", "V"):
+            np.testing.assert_array_equal(one[key], r[key][j])
