@@ -177,6 +177,32 @@ int qb_lanczos(const qb_sector* sec, const qb_program* prog, const double* v0_ho
 int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, int dtype, int refine, double* e0,
                    int* iters, int* converged, int* matvecs);
 
+/* The certified lowest eigenpair of a sector with its vector (gs_vector / gs_lanczos,
+ * src/engine/block_solve.cpp:697-845): a Paige-gated recurrence without reorthogonalisation from
+ * staged_seed(0x51ED900D), the Ritz vector from the kept basis or a replay, restarted from it until
+ * ||H u - E u|| <= 1e-9 * (sum |coeff|), at most 5 attempts of 600 steps (max_steps > 0 caps all of them).
+ * vec_device (n complex128, device) and vec_host (2n doubles) may each be NULL. */
+int qb_ground_state(const qb_sector* sec, const qb_program* prog, int max_steps, double* e0, double* residual,
+                    int* certified, void* vec_device, double* vec_host, int* matvecs);
+
+/* The k > 1 lane (krylov_schur_lane, src/engine/block_solve.cpp:433-510, over krylov_schur_kernel,
+ * include/ed/krylov/krylov_schur.h:95-330): thick-restart Krylov-Schur with full CGS2 from
+ * staged_seed(0x51ED0B70), cycles of min(2k + 60, 2p + 20, n) vectors keeping p = k + max(k/2, 8), lock
+ * tolerance 1e-10 * scale, fresh deflated starts after an invariant subspace, and the degeneracy probe.
+ * values: the k lowest, ascending (NaN past n_found). max_iter: matvec budget (0: max(200k, 2000)).
+ * vecs_device: NULL, or k device pointers (each n complex128, or NULL) for the eigenvectors. */
+int qb_eigs_k(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, double* values, int* n_found,
+              int* converged, int* matvecs, void* const* vecs_device);
+
+/* T = 0 dynamics of an operator O from sector src to sector tgt (src/engine/dynamics.cpp:442-566): the
+ * certified ground state psi0 of h_src, phi = O psi0 (op: the cross row program, rows in tgt, columns in
+ * src), and the continued fraction of h_tgt from phi (cf_spectral_from_vector, include/ed/dynamics/cf.h:104-160)
+ * at depth max(depth, 2), shifted by E0, tolerance 64 eps * scale. S: n_omega values; conv_change: the
+ * half-depth change of the fraction. */
+int qb_dynamics_t0(const qb_sector* src, const qb_program* h_src, const qb_sector* tgt, const qb_program* h_tgt,
+                   const qb_program* op, int depth, const double* omega, int n_omega, double eta, double* S, double* e0,
+                   double* conv_change, int* certified);
+
 /* FTLM on one block (ftlm_kernel, include/ed/thermal/ftlm.h:277-480; sample vectors of
  * include/ed/thermal/sample_seed.h:37-89): all samples advance together as one block matvec.
  * Outputs per beta: lnZ, E, V; and the lowest weighted Ritz value. */

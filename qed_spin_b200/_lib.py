@@ -26,7 +26,7 @@ EXPORTS = [
     "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
-    "qb_lanczos_noalloc",
+    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0",
 ]
 
 
@@ -102,6 +102,9 @@ def lib():
     L.qb_lanczos.argtypes = [vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i)]
     L.qb_eigs_lowest.argtypes = [vp, vp, i, i, i, C.POINTER(d), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]
+    L.qb_ground_state.argtypes = [vp, vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i), vp, vp, C.POINTER(i)]
+    L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
+    L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
     L.qb_ftlm_blocks.argtypes = [vp, vp, i, i, i, u64, vp, i, i, i, vp, vp, vp, vp, vp]
     L.qb_thermal_combine.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]
     L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]

@@ -237,6 +237,43 @@ def eigs_lowest(sec: Sector, prog: Program, max_iter: int = 0, dtype="c128", ref
     return dict(e0=e.value, iters=it.value, converged=bool(cv.value), matvecs=mv.value)
 
 
+def ground_state(sec: Sector, prog: Program, max_steps: int = 0, vector: bool = True) -> dict:
+    """The certified lowest eigenpair: energy, residual, certified, matvecs, and the vector (host complex128)."""
+    e0, res, cert, mv = C.c_double(), C.c_double(), C.c_int(), C.c_int()
+    vec = np.zeros(sec.dim, np.complex128) if vector else None
+    check(lib().qb_ground_state(sec.h, prog.h, max_steps, C.byref(e0), C.byref(res), C.byref(cert), None,
+                                None if vec is None else vec.ctypes.data, C.byref(mv)))
+    return {"e0": e0.value, "residual": res.value, "certified": bool(cert.value), "matvecs": mv.value, "vector": vec}
+
+
+def eigs(sec: Sector, prog: Program, k: int, max_iter: int = 0, vectors: bool = False) -> dict:
+    """The k lowest levels: the k = 1 scan lane for k == 1, thick-restart Krylov-Schur for k > 1."""
+    if k == 1 and not vectors:
+        r = eigs_lowest(sec, prog, max_iter)
+        return {"values": np.array([r["e0"]]), "converged": r["converged"], "matvecs": r["matvecs"]}
+    vals = np.zeros(k)
+    nf, cv, mv = C.c_int(), C.c_int(), C.c_int()
+    import torch
+    vecs = [torch.empty(sec.dim, dtype=torch.complex128, device="cuda") for _ in range(k)] if vectors else None
+    ptrs = (C.c_void_p * k)(*[v.data_ptr() for v in vecs]) if vectors else None
+    check(lib().qb_eigs_k(sec.h, prog.h, k, max_iter, vals.ctypes.data, C.byref(nf), C.byref(cv), C.byref(mv), ptrs))
+    out = {"values": vals[: nf.value], "converged": bool(cv.value), "matvecs": mv.value}
+    if vectors:
+        out["vectors"] = [v.cpu().numpy() for v in vecs[: nf.value]]
+    return out
+
+
+def dynamics_t0(src: Sector, h_src: Program, tgt: Sector, h_tgt: Program, op: Program, depth: int, omega,
+                eta: float) -> dict:
+    """T = 0 dynamics of the cross-sector operator `op` (rows in tgt, columns in src): S(omega), E0."""
+    omega = np.ascontiguousarray(omega, np.float64)
+    S = np.zeros(len(omega))
+    e0, ch, cert = C.c_double(), C.c_double(), C.c_int()
+    check(lib().qb_dynamics_t0(src.h, h_src.h, tgt.h, h_tgt.h, op.h, depth, omega.ctypes.data, len(omega), eta,
+                               S.ctypes.data, C.byref(e0), C.byref(ch), C.byref(cert)))
+    return {"S": S, "e0": e0.value, "conv_change": ch.value, "certified": bool(cert.value)}
+
+
 def ftlm(sec: Sector, prog: Program, samples: int, depth: int, seed: int, betas, dtype="c128") -> dict:
     betas = np.ascontiguousarray(betas, np.float64)
     nb = len(betas)

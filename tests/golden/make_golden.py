@@ -10,7 +10,7 @@ Writes
                 (tests/python/golden/refs/api-2026-09/cpu.json.gz, tier "exact" 1e-10), for the chain models
                 whose fixed-S^z spectra the sector tests reassemble, plus the N = 12 Heisenberg ring E0.
   fixtures.npz  outputs of the reference engine itself on small seeded cases: representatives and 1/norms,
-                row programs, y = H x, the merged CSR pattern and its spmv of x, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
+                row programs, y = H x, the merged CSR pattern and its spmv of x, the k = 4 lane's levels, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
                 curves and continued-fraction spectra.
 """
 from __future__ import annotations
@@ -101,6 +101,8 @@ def main(ref_root: str):
         fx[f"{name}/lz_beta"] = b
         e0, it, cv = rs.scan_lowest(rp)
         fx[f"{name}/e0"] = np.array([e0, it, cv], np.float64)
+        ks, ks_cv, ks_ap = rs.ks_lowest(rp, 4)
+        fx[f"{name}/ks4"] = ks   # the k = 4 lane: the reference's krylov_schur_kernel
         betas = 1.0 / np.linspace(0.1, 4.0, 40)
         f = rs.ftlm(rp, 8, 60, 20240601, betas)
         for k in ("lnZ", "E", "V"):
