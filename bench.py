@@ -266,6 +266,11 @@ def main():
     ap.add_argument("--ftlm", action="store_true",
                     help="batched FTLM over the 600 blocks of the XXZ chain N=24 (every S^z x 24 momenta), one "
                          "JSON line: samples/s against the plain single-sample path and the reference CPU engine")
+    ap.add_argument("--serve", action="store_true",
+                    help="the served request stream (Poisson arrivals of eigs / S^z(q) dynamics requests on chains "
+                         "N = 16..30): p50/p99 latency and solves/s of the server against one solve at a time")
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--no-serve", action="store_true", help="leave the served-stream measurement out of the line")
     ap.add_argument("--e0-6x6", action="store_true",
                     help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
                          "(FP64, and FP32 storage + FP64 refinement), one JSON line")
@@ -283,6 +288,9 @@ def main():
         return
     if args.ftlm:
         ftlm_config(args)
+        return
+    if args.serve:
+        print(json.dumps(serve_measure(args)))
         return
 
     world, rank, local = dist_init() if args.impl == "b200" else (int(os.environ.get("WORLD_SIZE", "1")),
@@ -392,6 +400,13 @@ def main():
             cpu = cpu_baseline_sample(n)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"unavailable": str(e)}
+    # the served request stream, rank 0 at N = 1
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        try:
+            serve = serve_measure(args)
+        except Exception as e:
+            serve = {"unavailable": str(e)}
     # the batched FTLM workload (every block of the N = 24 chain), rank 0 at N = 1
     ftlm = None
     if rank == 0 and world == 1 and not args.no_ftlm:
@@ -436,6 +451,7 @@ def main():
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
         "ftlm": ftlm,
+        "serve": serve,
     }
     print(json.dumps(line))
     A.close()
@@ -532,6 +548,100 @@ def ftlm_measure(args, with_cpu=True):
             out["cpu_baseline"] = ftlm_reference_sample(os.cpu_count() or 1)
         except Exception as e:
             out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
+def serve_requests(n: int, seed: int = 7):
+    """The served stream's requests: periodic chains with N uniform in 16..30 and n_up = N // 2 (S^z = 0 for
+    even N, -1/2 for odd), H = J sum S_i.S_{i+1} + K sum S_i.(S_{i+1} x S_{i+2}) with J ~ U[0.5, 1.5] and
+    K ~ U[0, 0.3] drawn per request (uniform over the bonds, so translations stay a symmetry); half eigs (k
+    uniform in 1..4 in a uniform momentum sector), half T = 0 dynamics of S^z(q) from the lowest state of the
+    k = 0 sector, q = 2 pi m / N with m uniform, Krylov 200, 400 frequencies in [-0.5, 6], eta = 0.05."""
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    rng = np.random.default_rng(seed)
+    omega = np.linspace(-0.5, 6.0, 400)
+    out = []
+    for _ in range(n):
+        N = int(rng.integers(16, 31))
+        J = float(rng.uniform(0.5, 1.5))
+        K = float(rng.uniform(0.0, 0.3))
+        prods = ops.heisenberg_products(lat.chain_bonds(N), J) + ops.chiral_products(
+            [(i, (i + 1) % N, (i + 2) % N) for i in range(N)], K)
+        h = ops.row_program(ops.from_products(N, prods))
+        if rng.random() < 0.5:
+            k = int(rng.integers(1, 5))
+            mom = int(rng.integers(0, N))
+            out.append({"kind": "eigs", "N": N, "spec": lat.chain_sector(N, N // 2, mom), "h": h, "k": k})
+        else:
+            m = int(rng.integers(0, N))
+            src, tgt = lat.chain_sector(N, N // 2, 0), lat.chain_sector(N, N // 2, m)
+            op = ops.cross_row_program(ops.from_products(N, ops.sz_q_products(N, 2 * np.pi * m / N)), tgt, src)
+            out.append({"kind": "dynamics", "N": N, "src": src, "tgt": tgt, "h": h, "op": op, "omega": omega})
+    return out
+
+
+def serve_run(reqs, arrivals, max_active):
+    """Submits each request at its arrival time (seconds from the start) to a server with max_active slots;
+    returns the per-request latencies (done - arrival) and the makespan."""
+    import threading
+
+    from qed_spin_b200 import device as D
+    srv = D.Server(max_active=max_active)
+    t0 = srv.clock()
+    tickets = [None] * len(reqs)
+
+    def submitter():
+        for i, (r, ta) in enumerate(zip(reqs, arrivals)):
+            dt = ta - (srv.clock() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            if r["kind"] == "eigs":
+                tickets[i] = srv.submit_eigs(r["spec"], r["h"], r["k"])
+            else:
+                tickets[i] = srv.submit_dynamics(r["src"], r["tgt"], r["h"], r["op"], 200, r["omega"], 0.05)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    results = []
+    for i in range(len(reqs)):
+        while tickets[i] is None:
+            time.sleep(0.0005)
+        results.append(srv.wait(tickets[i]))
+    th.join()
+    lat_s = np.array([res["t_done"] - t0 - ta for res, ta in zip(results, arrivals)])
+    span = max(res["t_done"] for res in results) - t0
+    srv.close()
+    return lat_s, span, results
+
+
+def serve_measure(args):
+    import torch
+
+    from qed_spin_b200 import build
+    build.build()
+    n = args.serve_requests
+    reqs = serve_requests(n)
+    # warm-up: one of each kind
+    serve_run(reqs[:2], [0.0, 0.0], 2)
+    # the service time of one solve at a time, back to back
+    lat1, span1, _ = serve_run(reqs, [0.0] * n, 1)
+    mean_service = span1 / n
+    rate = 0.9 / mean_service   # 90% offered load for one solve at a time
+    rng = np.random.default_rng(11)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = {"workload": "served stream: chains N=16..30, J~U[0.5,1.5], K~U[0,0.3]; half eigs k=1..4, half S^z(q) "
+                       "T=0 dynamics (Krylov 200, 400 omega, eta 0.05); Poisson arrivals",
+           "requests": n, "mean_service_s_one_at_a_time": mean_service, "arrival_rate_per_s": rate}
+    for name, slots in (("plain_one_at_a_time", 1), ("served_continuous_batching", 8)):
+        lat, span, res = serve_run(reqs, arrivals, slots)
+        torch.cuda.synchronize()
+        out[name] = {"slots": slots, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                     "p99_ms": 1e3 * float(np.percentile(lat, 99)), "solves_per_s": n / span,
+                     "makespan_s": span, "unconverged": int(sum(1 for r in res if not r["converged"]))}
+    # capacity: the whole stream submitted at once
+    lat8, span8, _ = serve_run(reqs, [0.0] * n, 8)
+    out["saturated_solves_per_s"] = {"one_at_a_time": n / span1, "served": n / span8}
     return out
 
 

@@ -2,8 +2,10 @@
  * include/qed_b200.h -- the C-ABI of the B200 symmetry-sector matvec and its Krylov recurrences.
  *
  * The drop-in boundary for the reference engine's device lane: plain C types, opaque handles,
- * integer status codes, an explicit CUDA stream (NULL: the legacy default stream, the one the
- * reference's device lane orders its work on). Nothing here throws across the ABI.
+ * integer status codes, an explicit CUDA stream. NULL means the calling thread's default stream: the
+ * library is built with per-thread default streams, and that stream synchronises with the legacy
+ * default stream the reference's device lane orders its work on, so the lane's ordering holds; solves
+ * driven from different host threads overlap on the device. Nothing here throws across the ABI.
  *
  * Conventions.
  *   - A basis state is a uint64 bit string, a SET bit an UP spin (include/ed/ops/term.h:27-34 in the
@@ -253,6 +255,48 @@ int qb_cf(const qb_sector* sec, const qb_program* prog, const double* phi_host, 
 int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void* v0, void* work, int max_iter,
                        int reorth, double breakdown_tol, int dtype, double* alpha, double* beta, int* iters,
                        void* stream);
+
+/* ---- the request server ---------------------------------------------------------------------
+ * Eigs and T = 0 dynamics solves of sectors of different sizes served on one GPU with continuous
+ * batching: requests queue in arrival order; a worker admits the head when one of max_active slots is
+ * free and the request's estimated HBM footprint (sectors, reduced CSRs, Krylov vectors) fits what is
+ * left of hbm_budget (0: 80% of the free memory); a request larger than the budget runs alone. Admitted
+ * requests run concurrently, each on its worker's own stream. No reference counterpart: the reference
+ * serves one call at a time through its verbs (python/qed/_verbs). */
+typedef struct qb_server qb_server;
+enum { QB_REQ_EIGS = 0, QB_REQ_DYNAMICS = 1 };
+#define QB_SERVER_MAX_LEVELS 16
+typedef struct {
+    int kind;                 /* QB_REQ_EIGS or QB_REQ_DYNAMICS */
+    qb_sector_desc sector;    /* eigs: the sector; dynamics: the source sector */
+    qb_program_desc h;        /* the Hamiltonian's row program (compile_operator(H^dagger)) */
+    int k;                    /* eigs: levels wanted, 1..16 (k = 1: the scan lane; k > 1: Krylov-Schur) */
+    qb_sector_desc target;    /* dynamics: the target sector */
+    qb_program_desc op;       /* dynamics: the operator's cross row program (rows in target, columns in source) */
+    int krylov;               /* dynamics: continued-fraction depth */
+    const double* omega;      /* dynamics: n_omega frequencies */
+    int n_omega;
+    double eta;
+} qb_request;
+typedef struct {
+    int status;               /* QB_OK, or the error of the solve (qb_last_error then describes it) */
+    int n_values;
+    double values[QB_SERVER_MAX_LEVELS];   /* eigs: the levels ascending; dynamics: E0 */
+    int converged;            /* eigs: converged; dynamics: the ground state certified */
+    int matvecs;
+    double e0, conv_change;   /* dynamics */
+    double t_submit, t_admit, t_done;      /* seconds on the server's clock (qb_server_clock) */
+    uint64_t footprint;       /* the bytes the request was admitted with */
+} qb_result;
+/* The request's descriptors are copied: the caller's arrays may be freed when submit returns. */
+int qb_server_create(int max_active, uint64_t hbm_budget, qb_server** out);
+int qb_server_submit(qb_server* s, const qb_request* r, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a ticket; QB_ETIMEOUT when it is not done. A returned result
+ * releases the ticket. S: NULL or n_omega doubles for a dynamics request's spectrum. */
+int qb_server_wait(qb_server* s, uint64_t ticket, int timeout_ms, qb_result* out, double* S);
+int qb_server_clock(qb_server* s, double* seconds);
+/* Finishes the admitted requests and drops the queued ones; call it once no thread waits on a ticket. */
+int qb_server_destroy(qb_server* s);
 
 #ifdef __cplusplus
 }

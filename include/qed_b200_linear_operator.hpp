@@ -111,7 +111,8 @@ public:
     [[nodiscard]] std::string description() const override { return "B200SectorMatVec"; }
     [[nodiscard]] bool has_device_kernel() const override { return true; }
 
-    // Device pointers of complex128, on the legacy default stream (the reference's device lane).
+    // Device pointers of complex128, on the calling thread's default stream (it synchronises with the
+    // legacy default stream the reference's device lane orders its work on).
     [[nodiscard]] MatvecFn bind_cuda() const override {
         auto row = row_, col = col_;
         auto prog = prog_;

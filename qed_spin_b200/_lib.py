@@ -27,6 +27,7 @@ EXPORTS = [
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
     "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0",
+    "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
 ]
 
 
@@ -44,6 +45,25 @@ class ProgramDesc(C.Structure):
         ("group_vbegin", C.c_void_p), ("n_vsub", C.c_uint32), ("vsub_val", C.c_void_p),
         ("vsub_tbegin", C.c_void_p), ("n_terms", C.c_uint32), ("term_sign", C.c_void_p),
         ("term_coeff", C.c_void_p),
+    ]
+
+
+QB_REQ_EIGS, QB_REQ_DYNAMICS = 0, 1
+QB_SERVER_MAX_LEVELS = 16
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("sector", SectorDesc), ("h", ProgramDesc), ("k", C.c_int), ("target", SectorDesc),
+        ("op", ProgramDesc), ("krylov", C.c_int), ("omega", C.c_void_p), ("n_omega", C.c_int), ("eta", C.c_double),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("n_values", C.c_int), ("values", C.c_double * QB_SERVER_MAX_LEVELS),
+        ("converged", C.c_int), ("matvecs", C.c_int), ("e0", C.c_double), ("conv_change", C.c_double),
+        ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double), ("footprint", C.c_uint64),
     ]
 
 
@@ -105,6 +125,11 @@ def lib():
     L.qb_ground_state.argtypes = [vp, vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i), vp, vp, C.POINTER(i)]
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
+    L.qb_server_create.argtypes = [i, u64, C.POINTER(vp)]
+    L.qb_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(u64)]
+    L.qb_server_wait.argtypes = [vp, u64, i, C.POINTER(Result), vp]
+    L.qb_server_clock.argtypes = [vp, C.POINTER(d)]
+    L.qb_server_destroy.argtypes = [vp]
     L.qb_ftlm_blocks.argtypes = [vp, vp, i, i, i, u64, vp, i, i, i, vp, vp, vp, vp, vp]
     L.qb_thermal_combine.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]
     L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]

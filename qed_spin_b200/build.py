@@ -19,8 +19,11 @@ BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# --default-stream per-thread: work the library issues on the NULL stream goes to the calling thread's default
+# stream, so solves driven from different host threads (the request server's workers) overlap on the device;
+# that stream still synchronises with the legacy default stream.
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-         "-Xcompiler", "-Wall", "-Wno-deprecated-gpu-targets"]
+         "-Xcompiler", "-Wall", "-Wno-deprecated-gpu-targets", "--default-stream", "per-thread"]
 
 
 def _nvcc() -> str:

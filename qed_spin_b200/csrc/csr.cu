@@ -492,6 +492,7 @@ void check_budget(u64 rows, u64 nnz, int id_bytes, std::size_t n_dict, uint64_t 
                                    std::to_string(max_bytes));
     std::size_t free_b = 0, total_b = 0;
     cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    free_b += idle_cached_bytes();
     if (need > free_b) throw Error(QB_ENOMEM, "CSR: " + std::to_string(need) + " bytes, " + std::to_string(free_b) +
                                                   " free on the device");
 }

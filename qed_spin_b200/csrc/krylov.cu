@@ -448,8 +448,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         const bool mixed = dtype == QB_C64 && refine;
         // FP32 storage keeps its Krylov basis when it fits comfortably (the Ritz vector for the
         // refinement); otherwise the scan runs twice (the second pass accumulates the Ritz vector).
-        std::size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        const std::size_t free_b = available_bytes();
         const bool keep = mixed && static_cast<double>(mi + 2) * nb * 8.0 < 0.5 * static_cast<double>(free_b);
         auto Rp = std::make_unique<Recurrence>(sec, prog, dtype, mi);
         Recurrence& R = *Rp;
@@ -500,8 +499,7 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
         for (int c = 0; c < 8 && !ok; ++c) {
             // the short FP64 cycle keeps its basis for the restart vector when it fits comfortably; otherwise
             // the cycle runs twice and the second pass accumulates the restart vector
-            cudaMemGetInfo(&free_b, &total_b);
-            const bool keep_f = static_cast<double>(cyc + 4) * nb * 16.0 < 0.5 * static_cast<double>(free_b);
+            const bool keep_f = static_cast<double>(cyc + 4) * nb * 16.0 < 0.5 * static_cast<double>(available_bytes());
             std::vector<double> zz;
             int mm = 0;
             {

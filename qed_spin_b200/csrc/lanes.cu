@@ -196,8 +196,7 @@ GsOut gs_vector(const qb_sector* sec, const qb_program* prog, double2* u, int ma
     const int nb = red_blocks(n);
     for (int attempt = 0; attempt <= kGsRestarts && left > 0; ++attempt) {
         const int cap = std::min(per_attempt, left);
-        std::size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        const std::size_t free_b = available_bytes();
         const bool keep = static_cast<double>(cap + 6) * n * 16.0 < 0.5 * static_cast<double>(free_b);
         std::vector<double> alpha, beta{0.0};
         int m = 0;
@@ -301,8 +300,7 @@ KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std:
     const std::size_t m = std::max<std::size_t>(1, std::min<std::size_t>({per_cycle, 2 * p_want + 20, static_cast<std::size_t>(n)}));
     const std::size_t p_keep = std::min(p_want, m > 1 ? m - 1 : std::size_t{1});
     {
-        std::size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        const std::size_t free_b = available_bytes();
         const double need = static_cast<double>(m + 2 + p_keep + k) * n * 16.0;
         if (need > 0.9 * static_cast<double>(free_b))
             throw Error(QB_ENOMEM, "eigs: a Krylov-Schur cycle of " + std::to_string(m) + " vectors of dimension " +
@@ -311,7 +309,7 @@ KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std:
     DevBuf<double2> V((m + 1) * n), w(n), U(std::max<std::size_t>(p_keep, k) * n);
     DevBuf<double> dS(static_cast<std::size_t>(m) * m);
     DevBuf<void*> dptr(m + 2 * k + 2);
-    DevBuf<double2> dcoef(m + 2 * k + 2);
+    DevBuf<double2> dcoef(m + 2 * k + 2), dpart(static_cast<std::size_t>(kMaxRedBlocks) + m + 2 * k + 2);
     Reducer red;
     const int nb = red_blocks(n);
     auto col = [&](std::size_t j) { return V.p + j * n; };
@@ -337,8 +335,8 @@ KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std:
         cuda_check(cudaMemcpy(dptr.p, b.data(), b.size() * sizeof(void*), cudaMemcpyHostToDevice), "basis");
         std::vector<double2> h(b.size());
         for (int pass = 0; pass < 2; ++pass) {
-            k_dot_many<double2><<<static_cast<unsigned>(b.size()), kThreads>>>(
-                n, reinterpret_cast<const double2* const*>(dptr.p), x, dcoef.p, nullptr);
+            dot_many<double2>(n, static_cast<int>(b.size()), reinterpret_cast<const double2* const*>(dptr.p), x, dcoef.p,
+                              dpart.p, nullptr, nullptr);
             k_axpy_many<double2><<<nb, kThreads>>>(n, static_cast<int>(b.size()),
                                                    reinterpret_cast<const double2* const*>(dptr.p), dcoef.p, x, nullptr);
             cuda_check(cudaGetLastError(), "cgs2");

@@ -42,6 +42,12 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string& m);
 
+// The device bytes the calling thread's solves may plan their optional buffers with (a kept Krylov basis):
+// the free device memory, or less when the thread has an allowance (a request server's worker sets one to
+// the footprint it admitted the request with; 0: none).
+std::size_t available_bytes();
+void set_thread_allowance(std::size_t bytes);
+
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;
     const int code = (e == cudaErrorMemoryAllocation) ? QB_ENOMEM : (e == cudaErrorNoDevice ? QB_ENODEV : QB_ECUDA);
@@ -65,7 +71,14 @@ template <class F> int guarded(F&& f) {
     }
 }
 
-// A device allocation owned by a host object.
+// Device memory from the library's cache of released blocks (alloc.cu): dev_free records an event on the
+// calling thread's stream and the block is reused once it completes, so releasing never synchronises the device.
+void* dev_alloc(std::size_t bytes);
+void dev_free(void* p, std::size_t bytes);
+std::size_t idle_cached_bytes();
+
+// A device allocation owned by a host object (released on the thread whose stream last used it, or after a
+// synchronisation).
 template <class T> struct DevBuf {
     T* p = nullptr;
     std::size_t n = 0;
@@ -86,11 +99,11 @@ template <class T> struct DevBuf {
     void alloc(std::size_t count) {
         release();
         if (count == 0) return;
-        cuda_check(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)), "cudaMalloc");
+        p = static_cast<T*>(dev_alloc(count * sizeof(T)));
         n = count;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p, n * sizeof(T));
         p = nullptr;
         n = 0;
     }

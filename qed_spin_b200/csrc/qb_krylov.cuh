@@ -223,21 +223,55 @@ __global__ void k_norm_to(std::uint64_t n, const double2* w, Scal S, double* slo
     if (last_block_total<1>(v, S.partials, S.counter, sm, tot)) *slot = sqrt(tot[0]);
 }
 
-// coeff[k] = -<V_k, w>, one block per basis vector.
+// coeff[k] = -<V_k, w>: a grid of (chunk, basis vector) blocks writes partial sums, and k_dot_sum adds each
+// vector's partials in chunk order (deterministic for a given chunk count).
 template <class T>
-__global__ void k_dot_many(std::uint64_t n, const T* const* basis, const double2* w, double2* coeff, const int* flag) {
+__global__ void k_dot_part(std::uint64_t n, const T* const* basis, const double2* w, double2* part, int chunks,
+                           const int* flag) {
     if (flag && *flag == 0) return;
     __shared__ double sm[4 * 32];
-    const T* v = basis[blockIdx.x];
+    const T* v = basis[blockIdx.y];
+    const std::uint64_t per = (n + chunks - 1) / chunks;
+    const std::uint64_t lo = static_cast<std::uint64_t>(blockIdx.x) * per;
+    const std::uint64_t hi = lo + per < n ? lo + per : n;
     double acc[2] = {0.0, 0.0};
-    for (std::uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    for (std::uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const double2 b = V<T>::ld(v, i);
         const double2 y = w[i];
         acc[0] += b.x * y.x + b.y * y.y;
         acc[1] += b.x * y.y - b.y * y.x;
     }
     block_reduce<2>(acc, sm);
-    if (threadIdx.x == 0) coeff[blockIdx.x] = make_double2(-acc[0], -acc[1]);
+    if (threadIdx.x == 0) part[static_cast<std::size_t>(blockIdx.y) * chunks + blockIdx.x] = make_double2(acc[0], acc[1]);
+}
+
+__global__ void k_dot_sum(int m, int chunks, const double2* part, double2* coeff, const int* flag) {
+    if (flag && *flag == 0) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    double sx = 0.0, sy = 0.0;
+    for (int c = 0; c < chunks; ++c) {
+        const double2 p = part[static_cast<std::size_t>(k) * chunks + c];
+        sx += p.x;
+        sy += p.y;
+    }
+    coeff[k] = make_double2(-sx, -sy);
+}
+
+// The chunk count of a dot_many over m vectors of length n: about kMaxRedBlocks blocks in all.
+int dot_chunks(std::uint64_t n, int m) {
+    const std::uint64_t by_len = (n + 4095) / 4096;
+    const int by_grid = std::max(1, kMaxRedBlocks / std::max(1, m));
+    return static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>(by_len, by_grid)));
+}
+
+// coeff[0..m) = -<V_k, w>; part holds at least m * dot_chunks(n, m) entries.
+template <class T>
+void dot_many(std::uint64_t n, int m, const T* const* basis, const double2* w, double2* coeff, double2* part,
+              const int* flag, cudaStream_t st) {
+    const int chunks = dot_chunks(n, m);
+    k_dot_part<T><<<dim3(chunks, m), kThreads, 0, st>>>(n, basis, w, part, chunks, flag);
+    k_dot_sum<<<(m + 127) / 128, 128, 0, st>>>(m, chunks, part, coeff, flag);
 }
 
 // w += sum_k coeff[k] V_k, each element accumulated in k order.
@@ -710,7 +744,7 @@ struct Recurrence {
     DevBuf<unsigned char> basis_block;          // kept Lanczos vectors, back to back (optional)
     std::vector<unsigned char*> basis;
     DevBuf<void*> d_basis;                      // their device pointers (full reorthogonalisation)
-    DevBuf<double2> d_coeff;
+    DevBuf<double2> d_coeff, d_part;
     DevBuf<double> d_norms;                     // [0] before, [1] after
     DevBuf<int> d_flag;
     cudaEvent_t ev = nullptr;
@@ -772,6 +806,7 @@ struct Recurrence {
         if (d_basis.n < static_cast<std::size_t>(max_iter + 1)) {
             d_basis.alloc(max_iter + 1);
             d_coeff.alloc(max_iter + 1);
+            d_part.alloc(static_cast<std::size_t>(kMaxRedBlocks) + max_iter + 1);
             d_norms.alloc(2);
             d_flag.alloc(1);
         }
@@ -787,10 +822,10 @@ struct Recurrence {
             double* before = d_norms.p;
             k_norm_to<<<nb, kThreads, 0, st>>>(n, w.p, scal(), before, flag);
             if (dtype == QB_C64) {
-                k_dot_many<float2><<<m, kThreads, 0, st>>>(n, reinterpret_cast<const float2* const*>(d_basis.p), w.p, d_coeff.p, flag);
+                dot_many<float2>(n, m, reinterpret_cast<const float2* const*>(d_basis.p), w.p, d_coeff.p, d_part.p, flag, st);
                 k_axpy_many<float2><<<nb, kThreads, 0, st>>>(n, m, reinterpret_cast<const float2* const*>(d_basis.p), d_coeff.p, w.p, flag);
             } else {
-                k_dot_many<double2><<<m, kThreads, 0, st>>>(n, reinterpret_cast<const double2* const*>(d_basis.p), w.p, d_coeff.p, flag);
+                dot_many<double2>(n, m, reinterpret_cast<const double2* const*>(d_basis.p), w.p, d_coeff.p, d_part.p, flag, st);
                 k_axpy_many<double2><<<nb, kThreads, 0, st>>>(n, m, reinterpret_cast<const double2* const*>(d_basis.p), d_coeff.p, w.p, flag);
             }
             k_norm_to<<<nb, kThreads, 0, st>>>(n, w.p, scal(), d_norms.p + 1, flag);

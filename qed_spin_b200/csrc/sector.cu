@@ -25,6 +25,15 @@ namespace qb {
 thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
 
+thread_local std::size_t g_allowance = 0;
+void set_thread_allowance(std::size_t bytes) { g_allowance = bytes; }
+std::size_t available_bytes() {
+    std::size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    free_b += idle_cached_bytes();   // released blocks the cache would hand out again
+    return g_allowance ? std::min(free_b, g_allowance) : free_b;
+}
+
 namespace {
 
 // -------------------------------------------------------------------------------------------
@@ -516,8 +525,6 @@ void build_lookup(qb_sector& s, int want) {
     }
     const auto C = pascal();
     const u64 ranks = C[s.N * 65 + s.n_up];
-    std::size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
     const double table_bytes = 4.0 * static_cast<double>(ranks);
     // buckets: ~one per representative, at most 2^24
     std::vector<u64> ends(2);
@@ -587,7 +594,7 @@ void build_lookup(qb_sector& s, int want) {
                                                                               s.bucket_off.p);
         cuda_check(cudaGetLastError(), "buckets");
     }
-    cuda_check(cudaDeviceSynchronize(), "lookup build");
+    cuda_check(cudaStreamSynchronize(nullptr), "lookup build");
 }
 
 }  // namespace
@@ -693,7 +700,7 @@ int qb_sector_create(const qb_sector_desc* d, qb_sector** out) {
                                                    s->inv_norms.p);
             cuda_check(cudaGetLastError(), "enumeration (write)");
         }
-        cuda_check(cudaDeviceSynchronize(), "enumeration");
+        cuda_check(cudaStreamSynchronize(nullptr), "enumeration");
         build_lookup(*s, d->lookup);
         *out = s.release();
     });

@@ -326,3 +326,94 @@ def cf(sec: Sector, prog: Program, phi: np.ndarray, depth: int, omega, eta: floa
     check(lib().qb_cf(sec.h, prog.h, phi.ctypes.data, depth, omega.ctypes.data, len(omega), eta, shift, tolerance,
                       S.ctypes.data, C.byref(sh)))
     return S, sh.value
+
+
+def _sector_desc(spec, keep: list, lookup: int = 0) -> "_lib.SectorDesc":
+    perms = np.ascontiguousarray(spec.perms, np.int32)
+    chars = np.ascontiguousarray(np.asarray(spec.chars, np.complex128)).view(np.float64)
+    flips = None if spec.flips is None else np.ascontiguousarray(spec.flips, np.uint64)
+    keep += [perms, chars, flips]
+    return _lib.SectorDesc(spec.n_sites, spec.n_up, perms.shape[0], perms.ctypes.data,
+                           None if flips is None else flips.ctypes.data, chars.ctypes.data, -1, lookup)
+
+
+def _program_desc(prog: HostProgram, keep: list) -> "_lib.ProgramDesc":
+    a = [
+        np.ascontiguousarray(prog.group_flip, np.uint64),
+        np.ascontiguousarray(prog.group_setbits, np.int32),
+        np.ascontiguousarray(prog.group_vbegin, np.uint32),
+        np.ascontiguousarray(prog.vsub_val, np.uint64),
+        np.ascontiguousarray(prog.vsub_tbegin, np.uint32),
+        np.ascontiguousarray(prog.term_sign, np.uint64),
+        np.ascontiguousarray(np.asarray(prog.term_coeff, np.complex128)).view(np.float64),
+    ]
+    keep += a
+    return _lib.ProgramDesc(len(a[0]), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, len(a[3]),
+                            a[3].ctypes.data, a[4].ctypes.data, len(a[5]), a[5].ctypes.data, a[6].ctypes.data)
+
+
+class Server:
+    """The request server (qb_server_*): eigs and T = 0 dynamics requests served concurrently on the device
+    with admission by HBM footprint. submit() returns a ticket at once; wait() returns the result."""
+
+    def __init__(self, max_active: int = 8, hbm_budget: int = 0):
+        h = C.c_void_p()
+        check(lib().qb_server_create(max_active, hbm_budget, C.byref(h)))
+        self.h = h
+        self.n_omega = {}
+
+    def submit_eigs(self, spec, prog: HostProgram, k: int) -> int:
+        keep = []
+        r = _lib.Request()
+        r.kind = _lib.QB_REQ_EIGS
+        r.sector = _sector_desc(spec, keep)
+        r.h = _program_desc(prog, keep)
+        r.k = k
+        t = C.c_uint64()
+        check(lib().qb_server_submit(self.h, C.byref(r), C.byref(t)))
+        return t.value
+
+    def submit_dynamics(self, src, tgt, h: HostProgram, op: HostProgram, krylov: int, omega, eta: float) -> int:
+        keep = []
+        omega = np.ascontiguousarray(omega, np.float64)
+        keep.append(omega)
+        r = _lib.Request()
+        r.kind = _lib.QB_REQ_DYNAMICS
+        r.sector = _sector_desc(src, keep)
+        r.target = _sector_desc(tgt, keep)
+        r.h = _program_desc(h, keep)
+        r.op = _program_desc(op, keep)
+        r.krylov = krylov
+        r.omega = omega.ctypes.data
+        r.n_omega = len(omega)
+        r.eta = eta
+        t = C.c_uint64()
+        check(lib().qb_server_submit(self.h, C.byref(r), C.byref(t)))
+        self.n_omega[t.value] = len(omega)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        res = _lib.Result()
+        no = self.n_omega.pop(ticket, 0)
+        S = np.zeros(no) if no else None
+        check(lib().qb_server_wait(self.h, ticket, timeout_ms, C.byref(res), None if S is None else S.ctypes.data))
+        if res.status != _lib.QB_OK:
+            check(res.status)
+        return {"values": np.array(res.values[: res.n_values]), "converged": bool(res.converged),
+                "matvecs": res.matvecs, "e0": res.e0, "conv_change": res.conv_change, "S": S,
+                "t_submit": res.t_submit, "t_admit": res.t_admit, "t_done": res.t_done, "footprint": res.footprint}
+
+    def clock(self) -> float:
+        t = C.c_double()
+        check(lib().qb_server_clock(self.h, C.byref(t)))
+        return t.value
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            try:
+                lib().qb_server_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    __del__ = close
