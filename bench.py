@@ -148,34 +148,18 @@ class Clocks:
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    from qed_spin_b200 import replicas
+    return replicas.init("nccl")
 
 
 def dist_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from qed_spin_b200 import replicas
+    return replicas.max_over_ranks(x, world)
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from qed_spin_b200 import replicas
+    replicas.barrier(world)
 
 
 def _reference_lane(threads):
@@ -415,9 +399,12 @@ def main():
         except Exception as e:
             ftlm = {"unavailable": str(e)}
 
+    from qed_spin_b200 import replicas
     if rank != 0:
+        A.close()
+        replicas.finish(world)
         return
-    value = world * 1e3 / per32
+    value = replicas.whole_job_rate(1.0, world, per32 * 1e-3)
     line = {
         "metric": "H.v/s", "value": value, "unit": "H.v/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per32, "higher_is_better": True, "scaling": "weak",
@@ -453,8 +440,9 @@ def main():
         "ftlm": ftlm,
         "serve": serve,
     }
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
     A.close()
+    replicas.finish(world)
 
 
 FTLM_N, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED = 24, 40, 100, 20240601
