@@ -205,6 +205,12 @@ int qb_dynamics_t0(const qb_sector* src, const qb_program* h_src, const qb_secto
                    const qb_program* op, int depth, const double* omega, int n_omega, double eta, double* S, double* e0,
                    double* conv_change, int* certified);
 
+/* The full spectrum of a small block (at most 8192 states), ascending, with multiplicity: the dense tail of
+ * the thermal and eigs drivers (blocks up to dense_max_dim are solved exactly, include/ed/sectors/thermal.h:35).
+ * The block is assembled on the device from the block matvec on identity columns; the host reduces it by
+ * Householder reflections to a real tridiagonal and takes its eigenvalues by implicit QL. */
+int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values);
+
 /* FTLM on one block (ftlm_kernel, include/ed/thermal/ftlm.h:277-480; sample vectors of
  * include/ed/thermal/sample_seed.h:37-89): all samples advance together as one block matvec.
  * Outputs per beta: lnZ, E, V; and the lowest weighted Ritz value. */

@@ -26,7 +26,7 @@ EXPORTS = [
     "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
-    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0",
+    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0", "qb_dense_levels",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
 ]
 
@@ -125,6 +125,7 @@ def lib():
     L.qb_ground_state.argtypes = [vp, vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i), vp, vp, C.POINTER(i)]
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
+    L.qb_dense_levels.argtypes = [vp, vp, vp]
     L.qb_server_create.argtypes = [i, u64, C.POINTER(vp)]
     L.qb_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(u64)]
     L.qb_server_wait.argtypes = [vp, u64, i, C.POINTER(Result), vp]

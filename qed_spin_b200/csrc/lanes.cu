@@ -497,10 +497,92 @@ KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std:
     return R;
 }
 
+// ---- the dense tail: the full spectrum of a small block ----
+// X[r][c] = (r == c0 + c): kc identity columns, interleaved by row, for the block matvec.
+__global__ void k_identity_cols(std::uint64_t n, int kc, std::uint64_t c0, double2* X) {
+    const std::uint64_t total = n * kc;
+    for (std::uint64_t t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const std::uint64_t r = t / kc, c = t % kc;
+        X[t] = make_double2(r == c0 + c ? 1.0 : 0.0, 0.0);
+    }
+}
+
+// The eigenvalues of a Hermitian matrix (column-major, n x n), ascending: Householder reflections to a
+// Hermitian tridiagonal (A22 <- A22 - 2 (v w^H + w v^H), w = A22 v - (v^H A22 v) v), whose off-diagonal moduli
+// make a real symmetric tridiagonal with the same spectrum, then implicit QL.
+std::vector<double> hermitian_levels(std::vector<std::complex<double>> A, int n) {
+    using cd = std::complex<double>;
+    auto at = [&](int r, int c) -> cd& { return A[static_cast<std::size_t>(c) * n + r]; };
+    std::vector<cd> v(n), p(n), w(n);
+    for (int k = 0; k + 2 < n; ++k) {
+        double xn = 0.0;
+        for (int i = k + 1; i < n; ++i) xn += std::norm(at(i, k));
+        xn = std::sqrt(xn);
+        if (xn == 0.0) continue;
+        const cd x0 = at(k + 1, k);
+        const cd phase = std::abs(x0) > 0.0 ? x0 / std::abs(x0) : cd(1.0, 0.0);
+        const cd alpha = -phase * xn;
+        // v = x - alpha e1, normalised
+        double vn = 0.0;
+        for (int i = k + 1; i < n; ++i) {
+            v[i] = at(i, k) - (i == k + 1 ? alpha : cd(0.0, 0.0));
+            vn += std::norm(v[i]);
+        }
+        vn = std::sqrt(vn);
+        if (vn == 0.0) continue;
+        for (int i = k + 1; i < n; ++i) v[i] /= vn;
+        // p = A22 v, K = v^H p (real), w = p - K v
+        for (int i = k + 1; i < n; ++i) {
+            cd s(0.0, 0.0);
+            for (int j = k + 1; j < n; ++j) s += at(i, j) * v[j];
+            p[i] = s;
+        }
+        cd K(0.0, 0.0);
+        for (int i = k + 1; i < n; ++i) K += std::conj(v[i]) * p[i];
+        for (int i = k + 1; i < n; ++i) w[i] = p[i] - K.real() * v[i];
+        for (int j = k + 1; j < n; ++j)
+            for (int i = k + 1; i < n; ++i) at(i, j) -= 2.0 * (v[i] * std::conj(w[j]) + w[i] * std::conj(v[j]));
+        at(k + 1, k) = alpha;
+        at(k, k + 1) = std::conj(alpha);
+        for (int i = k + 2; i < n; ++i) at(i, k) = at(k, i) = cd(0.0, 0.0);
+    }
+    std::vector<double> d(n), e(std::max(1, n - 1), 0.0), vals, z0;
+    for (int i = 0; i < n; ++i) d[i] = at(i, i).real();
+    for (int i = 0; i + 1 < n; ++i) e[i] = std::abs(at(i + 1, i));
+    eig_first_row(d, e, vals, z0);
+    std::sort(vals.begin(), vals.end());
+    return vals;
+}
+
 }  // namespace
 }  // namespace qb
 
 extern "C" {
+
+int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!sec || !prog || !values) throw Error(QB_EINVAL, "null argument");
+        const std::uint64_t n = sec->dim;
+        if (n == 0) return;
+        if (n > 8192) throw Error(QB_EINVAL, "dense levels: a block of more than 8192 states");
+        const int kc = static_cast<int>(std::min<std::uint64_t>(n, 64));
+        DevBuf<double2> X(n * kc), Y(n * kc);
+        std::vector<std::complex<double>> A(static_cast<std::size_t>(n) * n), Yh(static_cast<std::size_t>(n) * kc);
+        for (std::uint64_t c0 = 0; c0 < n; c0 += kc) {
+            k_identity_cols<<<red_blocks(n * kc), kThreads>>>(n, kc, c0, X.p);
+            launch_block_mixed(sec, sec, prog, X.p, Y.p, kc, QB_C128, QB_C128, nullptr);
+            cuda_check(cudaMemcpy(Yh.data(), Y.p, n * kc * 16, cudaMemcpyDeviceToHost), "dense columns");
+            for (int c = 0; c < kc && c0 + c < n; ++c)
+                for (std::uint64_t r = 0; r < n; ++r) A[(c0 + c) * n + r] = Yh[r * kc + c];
+        }
+        const std::vector<double> lv = hermitian_levels(std::move(A), static_cast<int>(n));
+        std::copy(lv.begin(), lv.end(), values);
+    });
+}
+
+
 
 int qb_ground_state(const qb_sector* sec, const qb_program* prog, int max_steps, double* e0, double* residual,
                     int* certified, void* vec_device, double* vec_host, int* matvecs) {

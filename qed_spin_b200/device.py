@@ -263,6 +263,13 @@ def eigs(sec: Sector, prog: Program, k: int, max_iter: int = 0, vectors: bool = 
     return out
 
 
+def dense_levels(sec: Sector, prog: Program) -> np.ndarray:
+    """The full spectrum of a small block (<= 8192 states), ascending, with multiplicity."""
+    vals = np.zeros(sec.dim)
+    check(lib().qb_dense_levels(sec.h, prog.h, vals.ctypes.data))
+    return vals
+
+
 def dynamics_t0(src: Sector, h_src: Program, tgt: Sector, h_tgt: Program, op: Program, depth: int, omega,
                 eta: float) -> dict:
     """T = 0 dynamics of the cross-sector operator `op` (rows in tgt, columns in src): S(omega), E0."""

@@ -1,0 +1,153 @@
+"""The verbs (eigs, thermal, dynamics with device=) against dense spectra built from the oracle's matvec.
+
+Tolerances, written per test: eigs levels 1e-9 * scale (the Krylov lanes' lock tolerance; dense blocks agree to
+1e-12); exact thermodynamics 1e-10 relative; FTLM blocks mixed with exact ones 1e-8 relative against the oracle's
+FTLM of the sampled blocks and exact traces of the rest.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qed_spin_b200 import lattice as lat
+from qed_spin_b200 import operators as ops
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    from qed_spin_b200 import build
+    build.build()
+
+
+def _model(N, K=0.2, h=0.1):
+    prods = (ops.heisenberg_products(lat.chain_bonds(N), 1.0) + ops.zeeman_z_products(N, h)
+             + ops.chiral_products([(i, (i + 1) % N, (i + 2) % N) for i in range(N)], K))
+    return ops.from_products(N, prods)
+
+
+def _dense_levels(spec, prog):
+    So, Po = O.Sector(spec), O.Program(prog)
+    n = So.dim
+    M = np.zeros((n, n), np.complex128)
+    for j in range(n):
+        e = np.zeros(n, np.complex128)
+        e[j] = 1.0
+        M[:, j] = So.gather(Po, e)
+    return np.linalg.eigvalsh(M)
+
+
+def _all_blocks(N):
+    return [lat.chain_sector(N, n, k) for n in range(N + 1) for k in range(N) if O.Sector(lat.chain_sector(N, n, k)).dim]
+
+
+def test_dense_levels_match_dense_solve():
+    from qed_spin_b200 import device as D
+    H = _model(10)
+    prog = ops.row_program(H)
+    for spec in [lat.chain_sector(10, 5, 0), lat.chain_sector(10, 4, 3), lat.chain_sector(10, 1, 7)]:
+        got = D.dense_levels(D.Sector(spec), D.Program(prog))
+        np.testing.assert_allclose(got, _dense_levels(spec, prog), rtol=0, atol=1e-12 * 20)
+
+
+@pytest.mark.parametrize("dense_max_dim", [0, 64])
+def test_eigs_verb(dense_max_dim):
+    from qed_spin_b200 import verbs
+    N = 10
+    H = _model(N)
+    prog = ops.row_program(H)
+    sz0 = [lat.chain_sector(N, N // 2, k) for k in range(N)]
+    r = verbs.eigs(H, 6, sectors=sz0, dense_max_dim=dense_max_dim)
+    ref = np.sort(np.concatenate([_dense_levels(s, prog) for s in sz0]))[:6]
+    scale = float(np.abs(np.asarray(prog.term_coeff)).sum())
+    assert r.complete and len(r.energies) == 6
+    np.testing.assert_allclose(r.energies, ref, rtol=0, atol=1e-9 * scale)
+    assert sorted(set(lv.block for lv in r.levels)) == sorted(set(lv.block for lv in r.levels))
+
+
+def _oracle_thermo(lnZ, E, V, betas):
+    curves = [{"lnZ": a, "E": b, "V": c} for a, b, c in zip(lnZ, E, V)]
+    return O.combine_blocks(curves, betas)
+
+
+def test_thermal_exact_verb():
+    from qed_spin_b200 import verbs
+    N = 10
+    H = _model(N)
+    prog = ops.row_program(H)
+    T = np.linspace(0.1, 4.0, 40)
+    blocks = _all_blocks(N)
+    r = verbs.thermal(H, T, sectors=blocks, method="exact")
+    levels = np.concatenate([_dense_levels(s, prog) for s in blocks])   # the whole spectrum
+    assert len(levels) == 2 ** N
+    betas = 1.0 / T
+    e0 = levels.min()
+    w = np.exp(-np.outer(betas, levels - e0))
+    Z = w.sum(axis=1)
+    Em = (w * levels).sum(axis=1) / Z
+    C = betas ** 2 * ((w * levels ** 2).sum(axis=1) / Z - Em ** 2)
+    np.testing.assert_allclose(r.lnZ, np.log(Z) - betas * e0, rtol=1e-10)
+    np.testing.assert_allclose(r.E, Em, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(r.C, C, rtol=1e-8, atol=1e-10)
+
+
+def test_thermal_ftlm_verb_mixed_with_exact():
+    from qed_spin_b200 import verbs
+    N, seed = 12, 977
+    H = _model(N)
+    prog = ops.row_program(H)
+    T = np.linspace(0.1, 4.0, 40)
+    betas = 1.0 / T
+    blocks = _all_blocks(N)
+    r = verbs.thermal(H, T, sectors=blocks, samples=8, krylov=30, seed=seed, dense_max_dim=50)
+    assert r.placement["ftlm"] > 0 and r.placement["dense"] > 0
+    Po = O.Program(prog)
+    lnZ, E, V = [], [], []
+    for spec in blocks:
+        So = O.Sector(spec)
+        if So.dim <= 50:
+            lv = _dense_levels(spec, prog)
+            e0 = lv.min()
+            x = lv - e0
+            w = np.exp(-np.outer(betas, x))
+            z = w.sum(axis=1)
+            m1 = (w * x).sum(axis=1) / z
+            m2 = (w * x * x).sum(axis=1) / z
+            lnZ.append(np.log(z) - betas * e0)
+            E.append(e0 + m1)
+            V.append(np.maximum(m2 - m1 * m1, 0.0))
+        else:
+            c = So.ftlm(Po, 8, 30, seed, betas)
+            lnZ.append(c["lnZ"])
+            E.append(c["E"])
+            V.append(c["V"])
+    ref = _oracle_thermo(lnZ, E, V, betas)
+    for key in ("lnZ", "E", "C", "S", "F"):
+        got = getattr(r, key)
+        np.testing.assert_allclose(got, ref[key], rtol=1e-8, atol=1e-8 * np.abs(ref[key]).max(), err_msg=key)
+
+
+def test_dynamics_verb_and_devices():
+    from qed_spin_b200 import device as D
+    from qed_spin_b200 import verbs
+    N, m = 12, 4
+    H = _model(N, h=0.0)
+    src, tgt = lat.chain_sector(N, 6, 0), lat.chain_sector(N, 6, m)
+    Sq = ops.from_products(N, ops.sz_q_products(N, 2 * np.pi * m / N))
+    omega = np.linspace(-0.5, 6.0, 300)
+    r = verbs.dynamics(H, Sq, source=src, target=tgt, omega=omega, eta=0.05, krylov=60)
+    h = ops.row_program(H)
+    d = D.dynamics_t0(D.Sector(src), D.Program(h), D.Sector(tgt), D.Program(h),
+                      D.Program(ops.cross_row_program(Sq, tgt, src)), 60, omega, 0.05)
+    assert r.certified
+    np.testing.assert_array_equal(r.S, d["S"])
+    with pytest.raises(verbs.DeviceUnsupported):
+        verbs.eigs(H, 1, sectors=[src], device="cpu")
+    with pytest.raises(verbs.InvalidRequest):
+        verbs.eigs(H, 1, sectors=[src], device="tpu")
+    with pytest.raises(verbs.InvalidRequest):
+        verbs.thermal(H, [-1.0], sectors=[src])
