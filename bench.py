@@ -384,6 +384,13 @@ def main():
             cpu = cpu_baseline_sample(n)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"unavailable": str(e)}
+    # config 2's two lowest levels (the k > 1 lane on the CSR lane, FP64) and config 1 (chain-20, four levels)
+    levels = None
+    if rank == 0 and world == 1:
+        try:
+            levels = levels_measure(S, P, args)
+        except Exception as e:
+            levels = {"unavailable": str(e)}
     # the served request stream, rank 0 at N = 1
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
@@ -437,6 +444,7 @@ def main():
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "levels": levels,
         "ftlm": ftlm,
         "serve": serve,
     }
@@ -536,6 +544,48 @@ def ftlm_measure(args, with_cpu=True):
             out["cpu_baseline"] = ftlm_reference_sample(os.cpu_count() or 1)
         except Exception as e:
             out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
+def levels_measure(S, P, args):
+    """The k > 1 lane: config 2's two lowest levels on the attached CSR (FP64), and config 1 (the Heisenberg chain
+    N = 20, Sz = 0, k = 0, lowest four) on the device against the reference engine's krylov_schur_kernel on the
+    host cores."""
+    import torch
+
+    from qed_spin_b200 import device as D
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    out = {}
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r2 = D.eigs(S, P, 2)
+    out["chain32_k2"] = {"s": time.perf_counter() - t, "values": list(map(float, r2["values"])),
+                         "converged": r2["converged"], "matvecs": r2["matvecs"], "lane": "Krylov-Schur on the CSR"}
+    spec = lat.chain_sector(20, 10, 0)
+    prods = ops.heisenberg_products(lat.chain_bonds(20))
+    prog = ops.row_program(ops.from_products(20, prods))
+    S20, P20 = D.Sector(spec), D.Program(prog)
+    D.eigs(S20, P20, 4)   # warm
+    t = time.perf_counter()
+    r4 = D.eigs(S20, P20, 4)
+    dev_s = time.perf_counter() - t
+    out["chain20_k4"] = {"device_s": dev_s, "values": list(map(float, r4["values"])), "converged": r4["converged"],
+                         "matvecs": r4["matvecs"], "dim": S20.dim}
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref as R
+            if R.available():
+                R.set_threads(os.cpu_count() or 1)
+                rs = R.Sector(20, 10, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+                rp = R.Operator(20, prods).row_program()
+                t = time.perf_counter()
+                ev, cv, ap = rs.ks_lowest(rp, 4, use_csr=True)
+                out["chain20_k4"]["reference_cpu_s"] = time.perf_counter() - t
+                out["chain20_k4"]["reference_values"] = list(map(float, ev))
+                out["chain20_k4"]["max_abs_diff"] = float(np.max(np.abs(np.array(ev) - r4["values"])))
+        except Exception as e:
+            out["chain20_k4"]["reference_unavailable"] = str(e)
     return out
 
 

@@ -76,6 +76,8 @@ def lib():
     L.qref_lanczos.argtypes = [vp, vp, _f64p, C.c_int, C.c_int, C.c_double, _f64p, _f64p, C.POINTER(C.c_int)]
     L.qref_scan_lowest.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.qref_ks_lowest.argtypes = [vp, vp, C.c_int, _f64p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.qref_ks_lowest_lane.argtypes = [vp, vp, C.c_int, C.c_int, _f64p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]
     L.qref_ftlm.argtypes = [vp, vp, C.c_int, C.c_int, C.c_uint64, _f64p, C.c_int, _f64p, _f64p, _f64p,
                             C.POINTER(C.c_double)]
     L.qref_cf.argtypes = [vp, vp, _f64p, C.c_int, _f64p, C.c_int, C.c_double, C.c_double, C.c_double, _f64p,
@@ -235,10 +237,13 @@ class Sector:
         _check(lib().qref_scan_lowest(self.h, prog.h, max_iter, C.byref(e), C.byref(it), C.byref(conv)))
         return e.value, it.value, bool(conv.value)
 
-    def ks_lowest(self, prog: Program, k):
+    def ks_lowest(self, prog: Program, k, use_csr=False):
+        """The reference's krylov_schur_kernel on the block, applying H through its walk or (use_csr) its
+        merged reduced CSR, the host default lane."""
         ev = np.zeros(k, np.float64)
         n, conv, ap = C.c_int(), C.c_int(), C.c_int()
-        _check(lib().qref_ks_lowest(self.h, prog.h, k, ev, C.byref(n), C.byref(conv), C.byref(ap)))
+        _check(lib().qref_ks_lowest_lane(self.h, prog.h, k, int(bool(use_csr)), ev, C.byref(n), C.byref(conv),
+                                         C.byref(ap)))
         return ev[: n.value].copy(), bool(conv.value), ap.value
 
     def ftlm(self, prog: Program, samples, depth, seed, betas):

@@ -508,17 +508,24 @@ int qref_scan_lowest(void* sec, void* prog, int max_iter, double* e0, int* iters
 
 // The k > 1 block lane (krylov_schur_lane, block_solve.cpp:433-510) without a memory cap: thick-restart
 // Krylov-Schur from staged_seed(0x51ED0B70), lock tolerance kLockRel * s_H.
-int qref_ks_lowest(void* sec, void* prog, int k, double* evals, int* n_found, int* converged, int* applies) {
+int qref_ks_lowest_lane(void* sec, void* prog, int k, int use_csr, double* evals, int* n_found, int* converged,
+                        int* applies) {
     return guarded([&] {
         auto* S = static_cast<RefSector*>(sec);
         const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
         const std::size_t nb = S->rd.dim();
         const std::size_t kk = static_cast<std::size_t>(k);
         Walk W{S, S, P, true, S->rd.make_policy(), S->rd.make_policy()};
+        // the host default lane applies through the merged reduced CSR (build_sector_csr); the walk otherwise
+        std::optional<ed::matvec::ReducedSymmetryCsr<Complex>> csr;
+        if (use_csr) csr = ed::matvec::build_sector_csr(P->view(), S->rd.make_policy(), S->rd.dim());
         std::uint64_t count = 0;
         auto H = [&](const Complex* in, Complex* out, std::size_t n) {
             ++count;
-            W(in, out, n);
+            if (csr)
+                csr->spmv(in, out);
+            else
+                W(in, out, n);
         };
         const std::uint64_t budget = std::max<std::uint64_t>(200u * kk, 2000u);
         const std::size_t per_cycle = std::min<std::size_t>(ed::krylov::krylov_subspace_dim(kk, 2 * kk + 60, nb, 0),
@@ -546,6 +553,10 @@ int qref_ks_lowest(void* sec, void* prog, int k, double* evals, int* n_found, in
         *converged = (r.converged || r.exhausted) ? 1 : 0;
         *applies = static_cast<int>(count);
     });
+}
+
+int qref_ks_lowest(void* sec, void* prog, int k, double* evals, int* n_found, int* converged, int* applies) {
+    return qref_ks_lowest_lane(sec, prog, k, 0, evals, n_found, converged, applies);
 }
 
 // FTLM on one block (ftlm_kernel<CpuBackend>, include/ed/thermal/ftlm.h:277-480) with the options the
