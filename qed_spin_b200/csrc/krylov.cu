@@ -97,6 +97,215 @@ __global__ void k_sample_start(std::uint64_t n, int k, const double2* G, std::ui
     }
 }
 
+// ---- the fused block recurrence on a block's reduced CSR (three passes a step) ----
+// Working precision: float for FP32 storage, double for FP64; products and sums with fused multiply-adds (the
+// FTLM curves are compared within a tolerance, not bit for bit).
+template <class T> struct Work;
+template <> struct Work<float2> {
+    using R = float;
+    __device__ static float2 ld(const float2* p, std::size_t i) { return __ldg(p + i); }
+    __device__ static void st(float2* p, std::size_t i, float x, float y) { p[i] = make_float2(x, y); }
+};
+template <> struct Work<double2> {
+    using R = double;
+    __device__ static double2 ld(const double2* p, std::size_t i) { return __ldg(p + i); }
+    __device__ static void st(double2* p, std::size_t i, double x, double y) { p[i] = make_double2(x, y); }
+};
+
+// Pass 1: w = A v_j - beta_j v_{j-1} on the CSR (8 lanes per row, lane l owns columns l, l + 8, ...), and
+// alpha_j = Re <v_j, w> per column: block partials in shared memory summed in row order, the block sums in
+// block order by the last block.
+template <class T, int CPL>
+__global__ void __launch_bounds__(256) fmv_alpha(std::uint64_t rows, int k, int j,
+                                                 const unsigned long long* __restrict__ row_ptr,
+                                                 const std::uint32_t* __restrict__ col,
+                                                 const unsigned char* __restrict__ ids, int id_bytes,
+                                                 const double2* __restrict__ vals, int n_dict, const T* __restrict__ vc,
+                                                 const T* __restrict__ vp, T* __restrict__ w, BScal S) {
+    using Rt = typename Work<T>::R;
+    __shared__ double2 dict[256];
+    __shared__ double red[kMaxCols][33];
+    if (id_bytes == 1)
+        for (int i = threadIdx.x; i < n_dict; i += blockDim.x) dict[i] = vals[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 7, rg = threadIdx.x >> 3;
+    Rt b[CPL];
+    double ap[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+        const int cc = lane + 8 * c;
+        b[c] = (j > 0 && cc < k) ? static_cast<Rt>(S.beta[static_cast<std::size_t>(j) * k + cc]) : Rt(0);
+        ap[c] = 0.0;
+    }
+    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * 32;
+    for (std::uint64_t r = static_cast<std::uint64_t>(blockIdx.x) * 32 + rg; r < rows; r += stride) {
+        Rt ar[CPL], ai[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) ar[c] = ai[c] = Rt(0);
+        const std::uint64_t e1 = row_ptr[r + 1];
+        for (std::uint64_t e = row_ptr[r]; e < e1; ++e) {
+            const double2 v2 = id_bytes == 1 ? dict[ids[e]]
+                                             : (id_bytes == 2 ? __ldg(vals + reinterpret_cast<const unsigned short*>(ids)[e])
+                                                              : __ldg(vals + e));
+            const Rt vr = static_cast<Rt>(v2.x), vi = static_cast<Rt>(v2.y);
+            const std::size_t base = static_cast<std::size_t>(__ldg(col + e)) * k;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int cc = lane + 8 * c;
+                if (cc < k) {
+                    const T x = Work<T>::ld(vc, base + cc);
+                    ar[c] = fma(vr, x.x, fma(-vi, x.y, ar[c]));
+                    ai[c] = fma(vr, x.y, fma(vi, x.x, ai[c]));
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) {
+            const int cc = lane + 8 * c;
+            if (cc >= k) continue;
+            const std::size_t i = static_cast<std::size_t>(r) * k + cc;
+            Rt yr = ar[c], yi = ai[c];
+            if (j > 0) {
+                const T p = Work<T>::ld(vp, i);
+                yr = fma(-b[c], p.x, yr);
+                yi = fma(-b[c], p.y, yi);
+            }
+            Work<T>::st(w, i, yr, yi);
+            const T z = Work<T>::ld(vc, i);
+            ap[c] += static_cast<double>(z.x) * yr + static_cast<double>(z.y) * yi;
+        }
+    }
+    // the block's partial per column: the 32 row groups in order
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+        const int cc = lane + 8 * c;
+        if (cc < k) red[cc][rg] = ap[c];
+    }
+    __syncthreads();
+    __shared__ bool is_last;
+    if (threadIdx.x < k) {
+        double s = 0.0;
+        for (int g = 0; g < 32; ++g) s += red[threadIdx.x][g];
+        S.partials[static_cast<std::size_t>(threadIdx.x) * kMaxRedBlocks + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(S.counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    for (int c = wp; c < k; c += blockDim.x >> 5) {   // one warp per column, a fixed xor-butterfly
+        const double* p = S.partials + static_cast<std::size_t>(c) * kMaxRedBlocks;
+        double s = 0.0;
+        for (unsigned g = ln; g < gridDim.x; g += 32) s += __ldcg(p + g);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (ln == 0) S.alpha[static_cast<std::size_t>(j) * k + c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *S.counter = 0;
+}
+
+// Pass 2: the norms and the local-reorthogonalisation overlaps of w - alpha_j v_j (not stored) -> beta_{j+1}.
+template <class T, int CPL>
+__global__ void fbeta(std::uint64_t n, int k, int j, const T* w, const T* vc, BScal S) {
+    extern __shared__ double bsm[];
+    __shared__ double tot[3][kMaxCols];
+    const int lane = threadIdx.x & 31;
+    double v[3][CPL];
+    double a[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+        v[0][c] = v[1][c] = v[2][c] = 0.0;
+        const int col = lane + 32 * c;
+        a[c] = col < k ? S.alpha[static_cast<std::size_t>(j) * k + col] : 0.0;
+    }
+    // four rows per warp iteration, all their loads issued before the sums
+    constexpr int kRows = 4;
+    const std::uint64_t warps = static_cast<std::uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (std::uint64_t r0 = (static_cast<std::uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRows;
+         r0 < n; r0 += warps * kRows) {
+        T y0[kRows][CPL], z0[kRows][CPL];
+#pragma unroll
+        for (int q = 0; q < kRows; ++q)
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int col = lane + 32 * c;
+                if (col < k && r0 + q < n) {
+                    const std::size_t i = (r0 + q) * k + col;
+                    y0[q][c] = w[i];
+                    z0[q][c] = vc[i];
+                }
+            }
+#pragma unroll
+        for (int q = 0; q < kRows; ++q)
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int col = lane + 32 * c;
+                if (col >= k || r0 + q >= n) continue;
+                const double zx = z0[q][c].x, zy = z0[q][c].y;
+                const double yx = y0[q][c].x - a[c] * zx, yy = y0[q][c].y - a[c] * zy;
+                v[0][c] += yx * yx + yy * yy;
+                v[1][c] += zx * yx + zy * yy;
+                v[2][c] += zx * yy - zy * yx;
+            }
+    }
+    if (block_cols_total<3, CPL>(v, k, S, bsm, tot) && threadIdx.x < k) {
+        const int c = threadIdx.x;
+        double nrm2 = tot[0][c];
+        const double ore = tot[1][c], oim = tot[2][c];
+        const bool proj = j > 0 && sqrt(ore * ore + oim * oim) > kLocalThreshold;
+        if (proj) nrm2 = fmax(nrm2 - (ore * ore + oim * oim), 0.0);
+        S.ovl[c] = proj ? -ore : 0.0;
+        S.ovl[kMaxCols + c] = proj ? -oim : 0.0;
+        S.beta[static_cast<std::size_t>(j + 1) * k + c] = sqrt(nrm2);
+    }
+}
+
+// Pass 3: v_{j+1} = (w - alpha_j v_j + o v_j) / beta_{j+1}; a column past its breakdown goes to zero.
+template <class T>
+__global__ void fnext(std::uint64_t n, int k, int j, double tol, const T* w, const T* vc, T* vn, BScal S) {
+    const std::uint64_t total = n * k;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % k);
+        const double b = S.beta[static_cast<std::size_t>(j + 1) * k + c];
+        const double inv = b >= tol && b > 0.0 ? 1.0 / b : 0.0;
+        const double a = S.alpha[static_cast<std::size_t>(j) * k + c];
+        const double ore = S.ovl[c], oim = S.ovl[kMaxCols + c];
+        const T y0 = w[i], z0 = vc[i];
+        const double zx = z0.x, zy = z0.y;
+        double yx = y0.x - a * zx, yy = y0.y - a * zy;
+        yx += ore * zx - oim * zy;
+        yy += ore * zy + oim * zx;
+        Work<T>::st(vn, i, static_cast<typename Work<T>::R>(yx * inv), static_cast<typename Work<T>::R>(yy * inv));
+    }
+}
+
+template <class T>
+void fused_step(const qb_csr* A, std::uint64_t n, int k, int j, double tol, const T* vc, const T* vp, T* w, T* vn,
+                BScal S, cudaStream_t st) {
+    const unsigned grid = static_cast<unsigned>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 31) / 32,
+                                                                                                    2 * kBlockRecGrid)));
+    const int cpl = (k + 7) / 8;
+#define QB_FMV(C) fmv_alpha<T, C><<<grid, 256, 0, st>>>(n, k, j, A->row_ptr.p, A->col_idx.p, A->ids.p, A->id_bytes, \
+                                                        A->vals.p, A->n_dict, vc, vp, w, S)
+    if (cpl <= 1) QB_FMV(1);
+    else if (cpl <= 2) QB_FMV(2);
+    else if (cpl <= 4) QB_FMV(4);
+    else if (cpl <= 5) QB_FMV(5);
+    else QB_FMV(8);
+#undef QB_FMV
+    const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kBlockRecGrid)));
+    const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
+    if (k <= 32)
+        fbeta<T, 1><<<rb, kThreads, bsm, st>>>(n, k, j, w, vc, S);
+    else
+        fbeta<T, 2><<<rb, kThreads, bsm, st>>>(n, k, j, w, vc, S);
+    fnext<T><<<red_blocks(n * k), kThreads, 0, st>>>(n, k, j, tol, w, vc, vn, S);
+    cuda_check(cudaGetLastError(), "fused ftlm step");
+}
+
 // The scratch of one stream's block recurrences, grown to the largest block it runs.
 struct BlockBufs {
     DevBuf<double2> w;
@@ -135,14 +344,22 @@ void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr
     cuda_check(cudaMemsetAsync(B.cnt.p, 0, 4, st), "zero");
     BScal S{B.alpha.p, B.beta.p, B.ovl.p, B.part.p, B.cnt.p};
     int cur = 1;
-    const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kMaxRedBlocks)));
+    const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kBlockRecGrid)));
     const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
     for (int j = 0; j < cap; ++j) {
         void* vc = B.vb[cur].p;
         void* vp = B.vb[cur ^ 1].p;
-        if (csr)
-            csr_spmv(csr, vc, B.w.p, k, dtype, QB_C128, st);
-        else if (k == 1)
+        if (csr) {   // the fused three passes, w in the storage type (it reuses the FP64 w buffer's memory)
+            if (dtype == QB_C64)
+                fused_step<float2>(csr, n, k, j, tol, (const float2*)vc, (const float2*)vp, (float2*)B.w.p,
+                                   (float2*)vp, S, st);
+            else
+                fused_step<double2>(csr, n, k, j, tol, (const double2*)vc, (const double2*)vp, B.w.p, (double2*)vp,
+                                    S, st);
+            cur ^= 1;
+            continue;
+        }
+        if (k == 1)
             launch_walk_mixed(sec, sec, prog, vc, B.w.p, dtype, QB_C128, st);   // one sample: the plain walk
         else
             launch_block_mixed(sec, sec, prog, vc, B.w.p, k, dtype, QB_C128, st);
@@ -324,9 +541,23 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         }
     } csrs{std::vector<qb_csr*>(n_blocks, nullptr)};
     t_phase = clock::now();
-    if (use_csr)
-        for (int b = 0; b < n_blocks; ++b)
-            if (qb_csr_build(secs[b], secs[b], progs[b], 0, &csrs.h[b]) != QB_OK) csrs.h[b] = nullptr;
+    if (use_csr) {
+        // the builds synchronise with the host a few times each: a few host threads, each on its own stream, keep
+        // the device busy across them
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "device");
+        std::atomic<int> next_b{0};
+        std::vector<std::thread> builders;
+        const int nt = std::max(1, std::min(8, n_blocks));
+        for (int t = 0; t < nt; ++t)
+            builders.emplace_back([&] {
+                cudaSetDevice(dev);
+                for (int b = next_b++; b < n_blocks; b = next_b++)
+                    if (qb_csr_build(secs[b], secs[b], progs[b], 0, &csrs.h[b]) != QB_OK) csrs.h[b] = nullptr;
+                cudaStreamSynchronize(cudaStreamPerThread);
+            });
+        for (auto& t : builders) t.join();
+    }
     st_csr = secs_since(t_phase);
     t_phase = clock::now();
     for (int i = 0; i < n_blocks; ++i) {

@@ -358,18 +358,24 @@ __device__ __forceinline__ bool block_cols_total(double (&v)[NQ][CPL], int k, BS
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
-    if (threadIdx.x < k) {
-        for (int q = 0; q < NQ; ++q) {
-            double s = 0.0;
-            const volatile double* p = S.partials + (static_cast<std::size_t>(q) * kMaxCols + threadIdx.x) * kMaxRedBlocks;
-            for (unsigned b = 0; b < gridDim.x; ++b) s += p[b];
-            total[q][threadIdx.x] = s;
-        }
+    // the block sums, one warp per (quantity, column) pair: lanes stride over the blocks' partials (read from
+    // L2, where the other blocks' fenced writes are), then a fixed xor-butterfly -- deterministic for a grid
+    for (int pr = warp; pr < NQ * k; pr += nw) {
+        const int q = pr / k, c = pr % k;
+        const double* p = S.partials + (static_cast<std::size_t>(q) * kMaxCols + c) * kMaxRedBlocks;
+        double s = 0.0;
+        for (unsigned b = lane; b < gridDim.x; b += 32) s += __ldcg(p + b);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) total[q][c] = s;
     }
     __syncthreads();
     if (threadIdx.x == 0) *S.counter = 0;
     return true;
 }
+
+// The grid of the block (multi-sample) recurrence passes: two blocks of 256 threads per SM of a B200 keep the
+// memory system busy, and the last block's sums then run over few partials.
+constexpr int kBlockRecGrid = 2 * 148;
 
 template <class T, int CPL>
 __global__ void brec_alpha(std::uint64_t n, int k, int j, double2* w, const T* vp, const T* vc, BScal S) {
