@@ -107,6 +107,22 @@ int qb_sector_info(const qb_sector* s, uint64_t* device_bytes, int* slc_L, int* 
  * include/ed/matvec/rep_symmetry_basis_policy.h:221-241), for n states at once (host arrays). */
 int qb_index_and_projection(const qb_sector* s, const uint64_t* states, uint64_t n, int64_t* index, double* proj);
 
+/* ---- sectors by content ----------------------------------------------------------------------
+ * qb_sector_acquire returns the one device sector of a descriptor (the device, group, characters,
+ * representative order and lookup), enumerating it on first use: repeated requests share it, as the
+ * reference shares its content-keyed sector mirrors (src/gpu/rep_matvec.cu:501-609). Release it with
+ * qb_sector_release (not qb_sector_destroy); released sectors stay cached up to a byte capacity (default
+ * 4 GiB, oldest evicted first; qb_registry_capacity changes it, 0 empties the cache). */
+int qb_sector_acquire(const qb_sector_desc* desc, qb_sector** out);
+int qb_sector_release(qb_sector* s);
+int qb_registry_capacity(uint64_t bytes);
+int qb_registry_stats(uint64_t* sectors, uint64_t* idle_sectors, uint64_t* idle_bytes);
+/* A sector's descriptor, representatives and 1/norms in a file (a checksummed little-endian format), and a
+ * sector made from such a file (the tables and lookup rebuilt, no enumeration): the cached sector-table
+ * format of repeated runs (the reference keeps its orbit tables in a registry, include/ed/basis/orbit_table.h). */
+int qb_sector_save(const qb_sector* s, const char* path);
+int qb_sector_load(const char* path, qb_sector** out);
+
 /* ---- programs ------------------------------------------------------------------------------ */
 int qb_program_create(const qb_program_desc* desc, qb_program** out);
 int qb_program_destroy(qb_program* p);

@@ -193,6 +193,11 @@ struct qb_sector {
     qb::u64 bucket_base = 0, bucket_count = 0;
     int bucket_shift = 0;
     std::vector<double> chars_host;   // 2G
+    // the descriptor the sector was made from (saved with it, and the key of the registry)
+    std::vector<std::int32_t> desc_perms;
+    std::vector<std::uint64_t> desc_flips;
+    int desc_slc_mode = 0, desc_lookup = 0;
+    bool registered = false;          // owned by the registry (qb_sector_acquire / qb_sector_release)
     qb::DSector view() const;
     std::uint64_t device_bytes() const;
 };

@@ -655,6 +655,20 @@ int qb_device_count(int* count) {
     });
 }
 
+}  // extern "C"
+
+namespace qb {
+void keep_desc(qb_sector& s, const qb_sector_desc& d) {
+    s.desc_perms.assign(d.perms, d.perms + static_cast<std::size_t>(d.group_size) * d.n_sites);
+    if (d.flips) s.desc_flips.assign(d.flips, d.flips + d.group_size);
+    s.chars_host.assign(d.chars, d.chars + 2 * static_cast<std::size_t>(d.group_size));
+    s.desc_slc_mode = d.sublattice_mode;
+    s.desc_lookup = d.lookup;
+}
+}  // namespace qb
+
+extern "C" {
+
 int qb_sector_create(const qb_sector_desc* d, qb_sector** out) {
     return qb::guarded([&] {
         using namespace qb;
@@ -664,6 +678,7 @@ int qb_sector_create(const qb_sector_desc* d, qb_sector** out) {
         s->n_up = d->n_up;
         s->G = d->group_size;
         s->bpw = (d->n_sites + 7) / 8;
+        keep_desc(*s, *d);
         upload_group(*s, *d);
         const auto Ch = pascal();
         const u64 total = Ch[s->N * 65 + s->n_up];
@@ -718,6 +733,7 @@ int qb_sector_create_from_reps(const qb_sector_desc* d, const uint64_t* reps, co
         s->n_up = d->n_up;
         s->G = d->group_size;
         s->bpw = (d->n_sites + 7) / 8;
+        keep_desc(*s, *d);
         upload_group(*s, *d);
         s->dim = dim;
         s->reps.upload(reinterpret_cast<const u64*>(reps), dim);
@@ -728,7 +744,10 @@ int qb_sector_create_from_reps(const qb_sector_desc* d, const uint64_t* reps, co
 }
 
 int qb_sector_destroy(qb_sector* s) {
-    return qb::guarded([&] { delete s; });
+    return qb::guarded([&] {
+        if (s && s->registered) throw qb::Error(QB_EINVAL, "a sector from qb_sector_acquire is released, not destroyed");
+        delete s;
+    });
 }
 
 uint64_t qb_sector_dim(const qb_sector* s) { return s ? s->dim : 0; }

@@ -194,7 +194,8 @@ struct qb_server {
 
 namespace {
 
-// Destroys the library objects of one solve.
+// Releases the library objects of one solve (sectors come from the registry: a block that recurs across
+// requests is enumerated once).
 struct Owned {
     std::vector<qb_sector*> secs;
     std::vector<qb_program*> progs;
@@ -202,7 +203,7 @@ struct Owned {
     ~Owned() {
         for (auto* c : csrs) qb_csr_destroy(c);
         for (auto* p : progs) qb_program_destroy(p);
-        for (auto* s : secs) qb_sector_destroy(s);
+        for (auto* s : secs) qb_sector_release(s);
     }
 };
 
@@ -220,7 +221,7 @@ void qb_server::run(qb::Job& j) {
     Owned o;
     auto sector = [&](const qb_sector_desc& d) -> qb_sector* {
         qb_sector* s = nullptr;
-        if (step(qb_sector_create(&d, &s), j) != QB_OK) return nullptr;
+        if (step(qb_sector_acquire(&d, &s), j) != QB_OK) return nullptr;
         o.secs.push_back(s);
         return s;
     };

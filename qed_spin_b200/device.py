@@ -33,8 +33,13 @@ class Sector:
     """A symmetry sector resident on the device (its representatives enumerated there)."""
 
     def __init__(self, spec: SectorSpec, sublattice_mode: int = -1, lookup: int = _lib.QB_LOOKUP_AUTO,
-                 reps=None, inv_norms=None):
+                 reps=None, inv_norms=None, shared: bool = False, _handle=None):
+        """shared: take the registry's sector for this descriptor (qb_sector_acquire) instead of a private one."""
         self.spec = spec
+        self._shared = bool(shared)
+        if _handle is not None:
+            self.h = _handle
+            return
         self._perms = np.ascontiguousarray(spec.perms, np.int32)
         chars = np.asarray(spec.chars, np.complex128)
         self._chars = np.ascontiguousarray(np.stack([chars.real, chars.imag], 1).reshape(-1))
@@ -43,7 +48,9 @@ class Sector:
                             None if self._flips is None else self._flips.ctypes.data, self._chars.ctypes.data,
                             sublattice_mode, lookup)
         h = C.c_void_p()
-        if reps is None:
+        if shared:
+            check(lib().qb_sector_acquire(C.byref(d), C.byref(h)))
+        elif reps is None:
             check(lib().qb_sector_create(C.byref(d), C.byref(h)))
         else:
             r = np.ascontiguousarray(reps, np.uint64)
@@ -54,12 +61,26 @@ class Sector:
     def close(self):
         if getattr(self, "h", None) and self.h.value:
             try:
-                lib().qb_sector_destroy(self.h)
+                if getattr(self, "_shared", False):
+                    lib().qb_sector_release(self.h)
+                else:
+                    lib().qb_sector_destroy(self.h)
             except Exception:   # interpreter shutdown: the library is already gone
                 pass
             self.h = None   # (no module globals here: this also runs at interpreter shutdown)
 
     __del__ = close
+
+    def save(self, path: str) -> None:
+        """Writes the descriptor, representatives and 1/norms (qb_sector_save)."""
+        check(lib().qb_sector_save(self.h, str(path).encode()))
+
+    @classmethod
+    def load(cls, path: str, spec: SectorSpec = None) -> "Sector":
+        """A sector from a file written by save (no enumeration)."""
+        h = C.c_void_p()
+        check(lib().qb_sector_load(str(path).encode(), C.byref(h)))
+        return cls(spec, _handle=h)
 
     @property
     def dim(self) -> int:
@@ -424,3 +445,14 @@ class Server:
             self.h = None
 
     __del__ = close
+
+
+def registry_capacity(nbytes: int) -> None:
+    """The byte capacity of the cache of released shared sectors (0 empties it)."""
+    check(lib().qb_registry_capacity(int(nbytes)))
+
+
+def registry_stats() -> dict:
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    check(lib().qb_registry_stats(C.byref(a), C.byref(b), C.byref(c)))
+    return {"sectors": a.value, "idle_sectors": b.value, "idle_bytes": c.value}
