@@ -226,6 +226,10 @@ int qb_dynamics_t0(const qb_sector* src, const qb_program* h_src, const qb_secto
  * The block is assembled on the device from the block matvec on identity columns; the host reduces it by
  * Householder reflections to a real tridiagonal and takes its eigenvalues by implicit QL. */
 int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values);
+/* The same for many blocks at once (largest first over host threads, each assembling on its own stream):
+ * block b's levels at values[sum of the earlier blocks' dims ...]. */
+int qb_dense_levels_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks,
+                           double* values);
 
 /* FTLM on one block (ftlm_kernel, include/ed/thermal/ftlm.h:277-480; sample vectors of
  * include/ed/thermal/sample_seed.h:37-89): all samples advance together as one block matvec.

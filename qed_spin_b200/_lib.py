@@ -27,6 +27,7 @@ EXPORTS = [
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
     "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0", "qb_dense_levels",
+    "qb_dense_levels_blocks",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
     "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_sector_save",
     "qb_sector_load",
@@ -128,6 +129,7 @@ def lib():
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
     L.qb_dense_levels.argtypes = [vp, vp, vp]
+    L.qb_dense_levels_blocks.argtypes = [vp, vp, i, vp]
     L.qb_sector_acquire.argtypes = [C.POINTER(SectorDesc), C.POINTER(vp)]
     L.qb_sector_release.argtypes = [vp]
     L.qb_registry_capacity.argtypes = [u64]

@@ -18,7 +18,10 @@
 #include <complex>
 #include <limits>
 #include <memory>
+#include <atomic>
 #include <random>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "qb_krylov.cuh"
@@ -560,25 +563,73 @@ std::vector<double> hermitian_levels(std::vector<std::complex<double>> A, int n)
 
 extern "C" {
 
+}  // extern "C"
+
+namespace qb {
+namespace {
+// One block's full spectrum: assembled on the calling thread's stream, reduced on the host.
+void dense_levels(const qb_sector* sec, const qb_program* prog, double* values) {
+    const std::uint64_t n = sec->dim;
+    if (n == 0) return;
+    if (n > 8192) throw Error(QB_EINVAL, "dense levels: a block of more than 8192 states");
+    const int kc = static_cast<int>(std::min<std::uint64_t>(n, 64));
+    DevBuf<double2> X(n * kc), Y(n * kc);
+    std::vector<std::complex<double>> A(static_cast<std::size_t>(n) * n), Yh(static_cast<std::size_t>(n) * kc);
+    for (std::uint64_t c0 = 0; c0 < n; c0 += kc) {
+        k_identity_cols<<<red_blocks(n * kc), kThreads>>>(n, kc, c0, X.p);
+        launch_block_mixed(sec, sec, prog, X.p, Y.p, kc, QB_C128, QB_C128, nullptr);
+        cuda_check(cudaMemcpy(Yh.data(), Y.p, n * kc * 16, cudaMemcpyDeviceToHost), "dense columns");
+        for (int c = 0; c < kc && c0 + c < n; ++c)
+            for (std::uint64_t r = 0; r < n; ++r) A[(c0 + c) * n + r] = Yh[r * kc + c];
+    }
+    const std::vector<double> lv = hermitian_levels(std::move(A), static_cast<int>(n));
+    std::copy(lv.begin(), lv.end(), values);
+}
+}  // namespace
+}  // namespace qb
+
+extern "C" {
+
 int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values) {
     return qb::guarded([&] {
+        if (!sec || !prog || !values) throw qb::Error(QB_EINVAL, "null argument");
+        qb::dense_levels(sec, prog, values);
+    });
+}
+
+int qb_dense_levels_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks,
+                           double* values) {
+    return qb::guarded([&] {
         using namespace qb;
-        if (!sec || !prog || !values) throw Error(QB_EINVAL, "null argument");
-        const std::uint64_t n = sec->dim;
-        if (n == 0) return;
-        if (n > 8192) throw Error(QB_EINVAL, "dense levels: a block of more than 8192 states");
-        const int kc = static_cast<int>(std::min<std::uint64_t>(n, 64));
-        DevBuf<double2> X(n * kc), Y(n * kc);
-        std::vector<std::complex<double>> A(static_cast<std::size_t>(n) * n), Yh(static_cast<std::size_t>(n) * kc);
-        for (std::uint64_t c0 = 0; c0 < n; c0 += kc) {
-            k_identity_cols<<<red_blocks(n * kc), kThreads>>>(n, kc, c0, X.p);
-            launch_block_mixed(sec, sec, prog, X.p, Y.p, kc, QB_C128, QB_C128, nullptr);
-            cuda_check(cudaMemcpy(Yh.data(), Y.p, n * kc * 16, cudaMemcpyDeviceToHost), "dense columns");
-            for (int c = 0; c < kc && c0 + c < n; ++c)
-                for (std::uint64_t r = 0; r < n; ++r) A[(c0 + c) * n + r] = Yh[r * kc + c];
+        if (!secs || !progs || !values || n_blocks < 0) throw Error(QB_EINVAL, "null argument");
+        std::vector<std::size_t> off(n_blocks + 1, 0);
+        for (int b = 0; b < n_blocks; ++b) {
+            if (!secs[b] || !progs[b]) throw Error(QB_EINVAL, "null block");
+            off[b + 1] = off[b] + secs[b]->dim;
         }
-        const std::vector<double> lv = hermitian_levels(std::move(A), static_cast<int>(n));
-        std::copy(lv.begin(), lv.end(), values);
+        // largest first over a pool of host threads, each assembling on its own stream
+        std::vector<int> order(n_blocks);
+        for (int b = 0; b < n_blocks; ++b) order[b] = b;
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return secs[a]->dim > secs[b]->dim; });
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "device");
+        const int nt = std::max(1, std::min<int>(n_blocks, static_cast<int>(std::max(1u, std::thread::hardware_concurrency()))));
+        std::atomic<int> next{0};
+        std::vector<std::string> errs(nt);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                cudaSetDevice(dev);
+                try {
+                    for (int i = next++; i < n_blocks; i = next++)
+                        dense_levels(secs[order[i]], progs[order[i]], values + off[order[i]]);
+                } catch (const std::exception& e) {
+                    errs[t] = e.what();
+                }
+            });
+        for (auto& t : pool) t.join();
+        for (const auto& e : errs)
+            if (!e.empty()) throw Error(QB_EINVAL, e);
     });
 }
 

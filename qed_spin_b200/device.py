@@ -291,6 +291,21 @@ def dense_levels(sec: Sector, prog: Program) -> np.ndarray:
     return vals
 
 
+def dense_levels_blocks(sectors, prog: Program) -> list:
+    """The full spectra of many small blocks at once (host threads), one array per block."""
+    nb = len(sectors)
+    dims = [s.dim for s in sectors]
+    vals = np.zeros(max(1, sum(dims)))
+    sh = (C.c_void_p * nb)(*[s.h.value for s in sectors])
+    ph = (C.c_void_p * nb)(*[prog.h.value] * nb)
+    check(lib().qb_dense_levels_blocks(sh, ph, nb, vals.ctypes.data))
+    out, o = [], 0
+    for d in dims:
+        out.append(vals[o:o + d].copy())
+        o += d
+    return out
+
+
 def dynamics_t0(src: Sector, h_src: Program, tgt: Sector, h_tgt: Program, op: Program, depth: int, omega,
                 eta: float) -> dict:
     """T = 0 dynamics of the cross-sector operator `op` (rows in tgt, columns in src): S(omega), E0."""

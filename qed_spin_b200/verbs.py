@@ -206,11 +206,15 @@ def thermal(H, T: Sequence[float], *, sectors: Sequence[SectorSpec], method: str
     lnZ, E, V = np.zeros((nb, len(T))), np.zeros((nb, len(T))), np.zeros((nb, len(T)))
     sampled = []
     P = D.Program(prog)
+    dense = []
     for j, (i, spec, S) in enumerate(blocks):
         if method == "exact" or S.dim <= dmax:
-            lnZ[j], E[j], V[j] = _exact_curves(D.dense_levels(S, P), betas)
+            dense.append(j)
         else:
             sampled.append(j)
+    if dense:
+        for j, lv in zip(dense, D.dense_levels_blocks([blocks[j][2] for j in dense], P)):
+            lnZ[j], E[j], V[j] = _exact_curves(lv, betas)
     if sampled:
         r = D.ftlm_blocks([blocks[j][2] for j in sampled], P, int(samples), depth, seed, betas, dtype=dtype)
         for q, j in enumerate(sampled):

@@ -54,6 +54,18 @@ def test_dense_levels_match_dense_solve():
         np.testing.assert_allclose(got, _dense_levels(spec, prog), rtol=0, atol=1e-12 * 20)
 
 
+def test_dense_levels_blocks_equal_one_by_one():
+    """The threaded batch returns each block's spectrum exactly as the single-block call does."""
+    from qed_spin_b200 import device as D
+    N = 12
+    prog = ops.row_program(_model(N))
+    secs = [D.Sector(s) for s in _all_blocks(N) if O.Sector(s).dim <= 400]
+    P = D.Program(prog)
+    many = D.dense_levels_blocks(secs, P)
+    for S, lv in zip(secs, many):
+        assert np.array_equal(lv.view(np.uint64), D.dense_levels(S, P).view(np.uint64))
+
+
 @pytest.mark.parametrize("dense_max_dim", [0, 64])
 def test_eigs_verb(dense_max_dim):
     from qed_spin_b200 import verbs
