@@ -43,9 +43,11 @@ enum { QB_C128 = 0, QB_C64 = 1 };
 enum { QB_REORTH_NONE = 0, QB_REORTH_FULL = 1, QB_REORTH_LOCAL = 2 };
 
 /* The state -> index structure: AUTO picks HASH; RANK a table over the combinadic ranks; BUCKETS offsets
- * into the ascending representatives; HASH an open-addressing table of 16-byte slots holding the state,
- * its index and its 1/norm class (one probe answers index and norm). */
-enum { QB_LOOKUP_AUTO = 0, QB_LOOKUP_RANK = 1, QB_LOOKUP_BUCKETS = 2, QB_LOOKUP_HASH = 3 };
+ * into the ascending representatives; HASH an open-addressing table whose slots hold the state, its index
+ * and its 1/norm class (one probe answers index and norm): 8-byte slots at load <= 2/3 when the state fits 32
+ * bits and index + class fit 31 (qb_sector_info reports kind 4), else 16-byte slots at load <= 1/2 (kind 3);
+ * HASH_WIDE forces the 16-byte slots. */
+enum { QB_LOOKUP_AUTO = 0, QB_LOOKUP_RANK = 1, QB_LOOKUP_BUCKETS = 2, QB_LOOKUP_HASH = 3, QB_LOOKUP_HASH_WIDE = 4 };
 
 typedef struct qb_sector qb_sector;
 typedef struct qb_program qb_program;

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libqed_b200.so")
 QB_OK, QB_EINVAL, QB_ENOMEM, QB_ECUDA, QB_EUNSUPPORTED, QB_ETIMEOUT, QB_ENODEV = range(7)
 QB_C128, QB_C64 = 0, 1
 QB_REORTH_NONE, QB_REORTH_FULL, QB_REORTH_LOCAL = 0, 1, 2
-QB_LOOKUP_AUTO, QB_LOOKUP_RANK, QB_LOOKUP_BUCKETS, QB_LOOKUP_HASH = 0, 1, 2, 3
+QB_LOOKUP_AUTO, QB_LOOKUP_RANK, QB_LOOKUP_BUCKETS, QB_LOOKUP_HASH, QB_LOOKUP_HASH_WIDE = 0, 1, 2, 3, 4
 QB_NOALLOC_MAX_ITER = 1024
 
 #: every symbol include/qed_b200.h declares

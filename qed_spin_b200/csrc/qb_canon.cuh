@@ -219,8 +219,29 @@ __device__ __forceinline__ long long hash_find(const DSector& S, u64 rb, int& cl
     }
 }
 
+// The compact table (N <= 32): an 8-byte slot holds the 32-bit state and index | class << idx_bits.
+__device__ __forceinline__ long long hash_find8(const DSector& S, u64 rb, int& cls) {
+    const u64 mask = (1ULL << S.hash_bits) - 1ULL;
+    u64 h = hash_slot(rb, S.hash_bits);
+    const u32 key = static_cast<u32>(rb);
+    for (;;) {
+        const u64 e = __ldg(S.slots8 + h);
+        if (e == ~0ULL) return -1;
+        if (static_cast<u32>(e) == key) {
+            const u32 pay = static_cast<u32>(e >> 32);
+            cls = static_cast<int>(pay >> S.idx_bits);
+            return static_cast<long long>(pay & ((1u << S.idx_bits) - 1u));
+        }
+        h = (h + 1) & mask;
+    }
+}
+
 // Index of representative rb in the sector, or -1 (index_of_rep, rep_symmetry_basis_policy.h:169-202).
 __device__ __forceinline__ long long index_of_rep(const DSector& S, u64 rb) {
+    if (S.lookup == 4) {
+        int cls;
+        return hash_find8(S, rb, cls);
+    }
     if (S.lookup == 3) {
         int cls;
         return hash_find(S, rb, cls);
@@ -253,9 +274,9 @@ __device__ __forceinline__ long long index_and_projection(const DSector& S, cons
     const u64 rb = static_cast<u64>(canonicalize<ST>(S, T, t, are, aim));
     long long j;
     double s;
-    if (S.lookup == 3) {
+    if (S.lookup >= 3) {
         int cls = 0;
-        j = hash_find(S, rb, cls);
+        j = S.lookup == 4 ? hash_find8(S, rb, cls) : hash_find(S, rb, cls);
         if (j < 0) return -1;
         s = S.n_class ? T.inv_class[cls] : __ldg(S.inv_norms + j);
     } else {

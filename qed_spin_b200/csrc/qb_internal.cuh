@@ -147,6 +147,8 @@ struct DSector {
     // lookup: kind 1 rank table, 2 state buckets, 3 hash slots
     int lookup = 0;
     const ulonglong2* slots = nullptr;   // [state, index | class << 32], 2^hash_bits slots; empty: state ~0
+    const u64* slots8 = nullptr;         // state (low 32 bits) | (index | class << idx_bits) << 32; empty: ~0
+    int idx_bits = 0;
     int hash_bits = 0;
     const double* inv_class = nullptr;   // the distinct 1/norm values, indexed by class (hash lookup)
     int n_class = 0;
@@ -186,6 +188,8 @@ struct qb_sector {
     qb::DevBuf<qb::u64> rank_lut;
     qb::DevBuf<qb::u32> bucket_off;
     qb::DevBuf<ulonglong2> slots;
+    qb::DevBuf<qb::u64> slots8;
+    int idx_bits = 0;
     qb::DevBuf<double> inv_class;
     int hash_bits = 0, n_class = 0;
     int slc_on = 0, slc_L = 0, slc_m = 0;

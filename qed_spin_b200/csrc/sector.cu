@@ -385,6 +385,34 @@ __global__ void hash_insert_kernel(const u64* reps, const double* inv, u64 dim, 
     }
 }
 
+// The compact table: every representative's 32-bit state and index | class << idx_bits in one 8-byte slot.
+__global__ void hash_insert8_kernel(const u64* reps, const double* inv, u64 dim, u64* slots, int bits, int idx_bits,
+                                    const u64* classes, int n_class) {
+    const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= dim) return;
+    const u64 s = reps[i];
+    u64 cls = 0;
+    if (n_class > 0) {
+        const u64 v = static_cast<u64>(__double_as_longlong(inv[i]));
+        int lo = 0, hi = n_class;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (classes[mid] < v)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        cls = static_cast<u64>(lo);
+    }
+    const u64 entry = (s & 0xFFFFFFFFULL) | ((i | (cls << idx_bits)) << 32);
+    const u64 mask = (1ULL << bits) - 1ULL;
+    u64 h = hash_slot(s, bits);
+    for (u64 probe = 0; probe <= mask; ++probe) {
+        if (atomicCAS(reinterpret_cast<unsigned long long*>(slots + h), ~0ULL, entry) == ~0ULL) return;
+        h = (h + 1) & mask;
+    }
+}
+
 __global__ void index_proj_kernel(DSector S, const u64* states, u64 n, long long* idx, double2* proj) {
     extern __shared__ __align__(16) unsigned char smem[];
     const Tables T = stage_tables(S, smem);
@@ -499,6 +527,7 @@ void validate(const qb_sector_desc* d) {
     if (d->n_up < 0 || d->n_up > d->n_sites) throw Error(QB_EINVAL, "n_up must be in [0, n_sites]");
     if (d->group_size < 1 || d->group_size > 65535) throw Error(QB_EINVAL, "group_size must be in [1, 65535]");
     if (!d->perms || !d->chars) throw Error(QB_EINVAL, "perms and chars are required");
+    if (d->lookup < QB_LOOKUP_AUTO || d->lookup > QB_LOOKUP_HASH_WIDE) throw Error(QB_EINVAL, "unknown lookup kind");
     for (int g = 0; g < d->group_size; ++g) {
         std::vector<int> seen(d->n_sites, 0);
         for (int i = 0; i < d->n_sites; ++i) {
@@ -531,16 +560,11 @@ void build_lookup(qb_sector& s, int want) {
     cuda_check(cudaMemcpy(&ends[0], s.reps.p, 8, cudaMemcpyDeviceToHost), "read reps");
     cuda_check(cudaMemcpy(&ends[1], s.reps.p + (s.dim - 1), 8, cudaMemcpyDeviceToHost), "read reps");
     int mode = want;
-    if (mode == QB_LOOKUP_AUTO) mode = QB_LOOKUP_HASH;
+    const bool wide = mode == QB_LOOKUP_HASH_WIDE;
+    if (mode == QB_LOOKUP_AUTO || mode == QB_LOOKUP_HASH_WIDE) mode = QB_LOOKUP_HASH;
     if (mode == QB_LOOKUP_HASH && (s.dim >= (1ULL << 32) || (s.N == 64 && s.n_up == 64))) mode = QB_LOOKUP_BUCKETS;
     (void)table_bytes;
     if (mode == QB_LOOKUP_HASH) {
-        // load factor <= 1/2
-        int bits = 4;
-        while ((1ULL << bits) < 2 * s.dim) ++bits;
-        s.hash_bits = bits;
-        s.slots.alloc(1ULL << bits);
-        cuda_check(cudaMemset(s.slots.p, 0xFF, (1ULL << bits) * sizeof(ulonglong2)), "hash clear");
         // the 1/norm classes
         DevBuf<u64> set(kClassSet);
         DevBuf<int> ovf(1);
@@ -566,9 +590,31 @@ void build_lookup(qb_sector& s, int want) {
             s.inv_class.upload(vals);
         }
         s.n_class = static_cast<int>(cls.size());
-        hash_insert_kernel<<<blocks, 256>>>(s.reps.p, s.inv_norms.p, s.dim, s.slots.p, bits, dcls.p, s.n_class);
+        // compact 8-byte slots (load <= 2/3) when the state fits 32 bits and index + class fit 31 bits (so a full
+        // slot is never all ones), else 16-byte slots (load <= 1/2)
+        int idx_bits = 1, cls_bits = 0;
+        while ((1ULL << idx_bits) < s.dim) ++idx_bits;
+        while ((1 << cls_bits) < s.n_class) ++cls_bits;
+        const bool compact = !wide && s.N <= 32 && !(s.N == 32 && s.n_up == 32) && idx_bits + cls_bits <= 31;
+        int bits = 4;
+        if (compact) {
+            while ((1ULL << bits) < s.dim + s.dim / 2) ++bits;
+            s.hash_bits = bits;
+            s.idx_bits = idx_bits;
+            s.slots8.alloc(1ULL << bits);
+            cuda_check(cudaMemset(s.slots8.p, 0xFF, (1ULL << bits) * 8), "hash clear");
+            hash_insert8_kernel<<<blocks, 256>>>(s.reps.p, s.inv_norms.p, s.dim, s.slots8.p, bits, idx_bits, dcls.p,
+                                                 s.n_class);
+            s.lookup = 4;
+        } else {
+            while ((1ULL << bits) < 2 * s.dim) ++bits;
+            s.hash_bits = bits;
+            s.slots.alloc(1ULL << bits);
+            cuda_check(cudaMemset(s.slots.p, 0xFF, (1ULL << bits) * sizeof(ulonglong2)), "hash clear");
+            hash_insert_kernel<<<blocks, 256>>>(s.reps.p, s.inv_norms.p, s.dim, s.slots.p, bits, dcls.p, s.n_class);
+            s.lookup = 3;
+        }
         cuda_check(cudaGetLastError(), "hash insert");
-        s.lookup = 3;
     } else if (mode == QB_LOOKUP_RANK) {
         if (s.dim >= (1ULL << 31)) throw Error(QB_EUNSUPPORTED, "rank table: more than 2^31 representatives");
         s.rank_table.alloc(static_cast<std::size_t>(ranks));
@@ -630,6 +676,8 @@ qb::DSector qb_sector::view() const {
     v.bucket_count = bucket_count;
     v.bucket_shift = bucket_shift;
     v.slots = slots.p;
+    v.slots8 = slots8.p;
+    v.idx_bits = idx_bits;
     v.hash_bits = hash_bits;
     v.inv_class = inv_class.p;
     v.n_class = n_class;
@@ -639,7 +687,7 @@ qb::DSector qb_sector::view() const {
 std::uint64_t qb_sector::device_bytes() const {
     return reps.bytes() + inv_norms.bytes() + lut.bytes() + flips.bytes() + chars.bytes() + to_key.bytes() +
            lead_pack.bytes() + cand.bytes() + edesc.bytes() + emask.bytes() + rank_table.bytes() + rank_lut.bytes() +
-           bucket_off.bytes() + slots.bytes() + inv_class.bytes();
+           bucket_off.bytes() + slots.bytes() + slots8.bytes() + inv_class.bytes();
 }
 
 extern "C" {

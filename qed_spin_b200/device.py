@@ -98,7 +98,7 @@ class Sector:
         b, L, m, k = C.c_uint64(), C.c_int(), C.c_int(), C.c_int()
         check(lib().qb_sector_info(self.h, C.byref(b), C.byref(L), C.byref(m), C.byref(k)))
         return dict(device_bytes=b.value, slc_L=L.value, slc_m=m.value,
-                    lookup={0: "none", 1: "rank", 2: "buckets", 3: "hash"}[k.value])
+                    lookup={0: "none", 1: "rank", 2: "buckets", 3: "hash", 4: "hash8"}[k.value])
 
     def index_and_projection(self, states):
         st = np.ascontiguousarray(states, np.uint64)

@@ -48,11 +48,12 @@ def _bits(a):
 
 
 @pytest.mark.parametrize("name", NAMES)
-@pytest.mark.parametrize("lookup", [1, 2])
+@pytest.mark.parametrize("lookup", [0, 1, 2, 4])   # auto (the compact hash), rank, buckets, wide hash
 def test_sector_and_matvec_bit_exact(fixtures, name, lookup):
     d = D()
     spec = CASE[name][1]
     S = d.Sector(spec, lookup=lookup)
+    assert S.info()["lookup"] == {0: "hash8", 1: "rank", 2: "buckets", 4: "hash"}[lookup]
     reps, inv = S.reps()
     assert np.array_equal(reps, fixtures[f"{name}/reps"])
     assert np.array_equal(_bits(inv), _bits(fixtures[f"{name}/inv_norms"]))
