@@ -30,6 +30,7 @@
 #include <complex>
 #include <cstring>
 #include <limits>
+#include <math_constants.h>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -310,15 +311,13 @@ void fused_step(const qb_csr* A, std::uint64_t n, int k, int j, double tol, cons
 struct BlockBufs {
     DevBuf<double2> w;
     DevBuf<unsigned char> vb[2];
-    DevBuf<double> alpha, beta, ovl, part, inv;
+    DevBuf<double> ovl, part, inv;
     DevBuf<unsigned> cnt;
-    void ensure(std::uint64_t n, int k, int cap, std::size_t es) {
+    void ensure(std::uint64_t n, int k, std::size_t es) {
         const std::size_t nk = static_cast<std::size_t>(n) * k;
         if (w.n < nk) w.alloc(nk);
         for (auto& b : vb)
             if (b.n < nk * es) b.alloc(nk * es);
-        if (alpha.n < static_cast<std::size_t>(cap) * k) alpha.alloc(static_cast<std::size_t>(cap) * k);
-        if (beta.n < static_cast<std::size_t>(cap + 1) * k) beta.alloc(static_cast<std::size_t>(cap + 1) * k);
         if (ovl.n == 0) ovl.alloc(2 * kMaxCols);
         if (part.n == 0) part.alloc(static_cast<std::size_t>(3) * kMaxCols * kMaxRedBlocks);
         if (inv.n == 0) inv.alloc(kMaxCols);
@@ -328,10 +327,10 @@ struct BlockBufs {
 
 // The lock-step recurrence of one block's k sample columns (ftlm_kernel's per-sample Lanczos with the
 // local reorthogonalisation, include/ed/thermal/ftlm.h:277-480), from the unit start columns in B.w
-// (FP64, interleaved by row), cap steps; queues alpha [cap][k] and beta [cap + 1][k] into host memory on st.
-// The matvec runs on the block's reduced CSR when one is given, else on the row walk.
+// (FP64, interleaved by row), cap steps; writes alpha [cap][k] and beta [cap + 1][k] to the device arrays d_alpha,
+// d_beta on st. The matvec runs on the block's reduced CSR when one is given, else on the row walk.
 void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr* csr, int k, int cap, double tol,
-                      int dtype, BlockBufs& B, cudaStream_t st, double* h_alpha, double* h_beta) {
+                      int dtype, BlockBufs& B, cudaStream_t st, double* d_alpha, double* d_beta) {
     const std::uint64_t n = sec->dim;
     const std::size_t nk = static_cast<std::size_t>(n) * k;
     const std::size_t es = dtype == QB_C64 ? 8 : 16;
@@ -340,9 +339,9 @@ void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr
         k_cast_from<float2><<<red_blocks(nk), kThreads, 0, st>>>(nk, B.w.p, reinterpret_cast<float2*>(B.vb[1].p));
     else
         cuda_check(cudaMemcpyAsync(B.vb[1].p, B.w.p, nk * 16, cudaMemcpyDeviceToDevice, st), "copy");
-    cuda_check(cudaMemsetAsync(B.beta.p, 0, static_cast<std::size_t>(cap + 1) * k * 8, st), "zero");
+    cuda_check(cudaMemsetAsync(d_beta, 0, static_cast<std::size_t>(cap + 1) * k * 8, st), "zero");
     cuda_check(cudaMemsetAsync(B.cnt.p, 0, 4, st), "zero");
-    BScal S{B.alpha.p, B.beta.p, B.ovl.p, B.part.p, B.cnt.p};
+    BScal S{d_alpha, d_beta, B.ovl.p, B.part.p, B.cnt.p};
     int cur = 1;
     const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kBlockRecGrid)));
     const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
@@ -385,100 +384,185 @@ void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr
         cuda_check(cudaGetLastError(), "ftlm step");
         cur ^= 1;
     }
-    cuda_check(cudaMemcpyAsync(h_alpha, B.alpha.p, static_cast<std::size_t>(cap) * k * 8, cudaMemcpyDeviceToHost, st),
-               "alpha");
-    cuda_check(cudaMemcpyAsync(h_beta, B.beta.p, static_cast<std::size_t>(cap + 1) * k * 8, cudaMemcpyDeviceToHost, st),
-               "beta");
 }
 
-// A block's curves from its samples' alpha / beta: each sample's run up to its breakdown, its Ritz values and
-// first-component weights, moments about its lowest level (sample_moments, ftlm.h:165-192), then the samples
-// combined (combine_samples, ftlm.h:199-235): lnZ = ln n + ln<Z> - beta e_ref, E, V.
-void block_curves(const double* ha, const double* hb, int k, int cap, double tol, std::uint64_t n,
-                  const double* betas, int n_beta, double* lnZ, double* E, double* V, double* e_min) {
-    struct Mom {
-        double e_min;
-        std::vector<double> Z, E1, E2;
-    };
-    std::vector<Mom> mom;
-    double gs = std::numeric_limits<double>::infinity();
-    for (int s = 0; s < k; ++s) {
-        std::vector<double> a, b;
-        b.push_back(0.0);
-        for (int j = 0; j < cap; ++j) {
-            a.push_back(ha[static_cast<std::size_t>(j) * k + s]);
-            b.push_back(hb[static_cast<std::size_t>(j + 1) * k + s]);
-            if (b.back() < tol) break;
-        }
-        std::vector<double> d(a), e(a.size() > 1 ? a.size() - 1 : 1, 0.0), vals, z0;
-        for (std::size_t i = 0; i + 1 < a.size(); ++i) e[i] = b[i + 1];
-        eig_first_row(d, e, vals, z0);
-        Mom mo;
-        mo.e_min = std::numeric_limits<double>::infinity();
-        std::vector<double> wts(vals.size());
-        for (std::size_t i = 0; i < vals.size(); ++i) {
-            wts[i] = z0[i] * z0[i];
-            if (wts[i] > 0.0) mo.e_min = std::min(mo.e_min, vals[i]);
-        }
-        if (!std::isfinite(mo.e_min)) mo.e_min = *std::min_element(vals.begin(), vals.end());
-        for (int t = 0; t < n_beta; ++t) {
-            double zz = 0.0, e1 = 0.0, e2 = 0.0;
-            for (std::size_t i = 0; i < vals.size(); ++i) {
-                const double x = vals[i] - mo.e_min;
-                const double bb = wts[i] * std::exp(-betas[t] * x);
-                zz += bb;
-                e1 += x * bb;
-                e2 += x * x * bb;
-            }
-            mo.Z.push_back(zz);
-            mo.E1.push_back(e1);
-            mo.E2.push_back(e2);
-        }
-        gs = std::min(gs, mo.e_min);
-        mom.push_back(std::move(mo));
-    }
-    double e_ref = mom.front().e_min;
-    for (const auto& m : mom) e_ref = std::min(e_ref, m.e_min);
-    const double ln_n = std::log(static_cast<double>(n));
-    for (int t = 0; t < n_beta; ++t) {
-        const double beta = betas[t];
-        double zz = 0.0, e1 = 0.0, e2 = 0.0;
-        for (const auto& m : mom) {
-            const double dd = m.e_min - e_ref, r = std::exp(-beta * dd);
-            zz += m.Z[t] * r;
-            e1 += (m.E1[t] + dd * m.Z[t]) * r;
-            e2 += (m.E2[t] + 2.0 * dd * m.E1[t] + dd * dd * m.Z[t]) * r;
-        }
-        zz /= k;
-        e1 /= k;
-        e2 /= k;
-        if (zz > 1e-300) {
-            const double m1 = e1 / zz, m2 = e2 / zz;
-            lnZ[t] = ln_n + std::log(zz) - beta * e_ref;
-            E[t] = e_ref + m1;
-            V[t] = std::max(m2 - m1 * m1, 0.0);
-        } else {
-            lnZ[t] = -beta * e_ref;
-            E[t] = e_ref;
-            V[t] = 0.0;
-        }
-    }
-    *e_min = gs;
-}
-
-// Pinned host memory owned by a host object.
-template <class T> struct PinnedBuf {
-    T* p = nullptr;
-    std::size_t n = 0;
-    explicit PinnedBuf(std::size_t count) : n(count) {
-        if (count) cuda_check(cudaMallocHost(reinterpret_cast<void**>(&p), count * sizeof(T)), "cudaMallocHost");
-    }
-    PinnedBuf(const PinnedBuf&) = delete;
-    PinnedBuf& operator=(const PinnedBuf&) = delete;
-    ~PinnedBuf() {
-        if (p) cudaFreeHost(p);
-    }
+// ---- the curves on the device ----
+// A block's place in the call's alpha [cap][k] / beta [cap + 1][k] arrays, its dimension and breakdown tolerance.
+struct CurveBlock {
+    unsigned long long a_off, b_off, dim;
+    double tol;
+    int cap;
 };
+
+// All eigenvalues and the first component of every unit eigenvector of the symmetric tridiagonal (d, e): implicit
+// QL with Wilkinson shifts, the rotations applied to the first row of the eigenvector matrix only (the reference's
+// tridiag_eig, include/ed/krylov/tridiag.h:42-80, returns the whole matrix; FTLM reads its first row). The arrays
+// are one thread's strided columns, element i at p[i * ld]. Returns false when an eigenvalue takes over 100 sweeps.
+__device__ bool ql_first_row(double* d, double* e, double* z, int m, std::size_t ld) {
+#define QB_D(i) d[static_cast<std::size_t>(i) * ld]
+#define QB_E(i) e[static_cast<std::size_t>(i) * ld]
+#define QB_Z(i) z[static_cast<std::size_t>(i) * ld]
+    const double eps = 2.220446049250313e-16;
+    for (int l = 0; l < m; ++l) {
+        for (int iter = 0;; ++iter) {
+            int mm = l;
+            for (; mm < m - 1; ++mm) {
+                const double dd = fabs(QB_D(mm)) + fabs(QB_D(mm + 1));
+                if (fabs(QB_E(mm)) <= eps * dd) break;
+            }
+            if (mm == l) break;
+            if (iter > 100) return false;
+            double g = (QB_D(l + 1) - QB_D(l)) / (2.0 * QB_E(l));
+            double r = hypot(g, 1.0);
+            g = QB_D(mm) - QB_D(l) + QB_E(l) / (g + (g >= 0 ? r : -r));
+            double s = 1.0, c = 1.0, p = 0.0;
+            int i = mm - 1;
+            for (; i >= l; --i) {
+                double f = s * QB_E(i);
+                const double b = c * QB_E(i);
+                r = hypot(f, g);
+                QB_E(i + 1) = r;
+                if (r == 0.0) {
+                    QB_D(i + 1) -= p;
+                    QB_E(mm) = 0.0;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = QB_D(i + 1) - p;
+                r = (QB_D(i) - g) * s + 2.0 * c * b;
+                p = s * r;
+                QB_D(i + 1) = g + p;
+                g = c * r - b;
+                f = QB_Z(i + 1);
+                QB_Z(i + 1) = s * QB_Z(i) + c * f;
+                QB_Z(i) = c * QB_Z(i) - s * f;
+            }
+            if (r == 0.0 && i >= l) continue;
+            QB_D(l) -= p;
+            QB_E(l) = g;
+            QB_E(mm) = 0.0;
+        }
+    }
+#undef QB_D
+#undef QB_E
+#undef QB_Z
+    return true;
+}
+
+// One thread per (block, sample) item: the sample's run up to its breakdown, its Ritz values and first-component
+// weights w_i = z_i^2, and its moments about its lowest weighted level e_min (sample_moments,
+// include/ed/thermal/ftlm.h:165-192): Z_t = sum_i w_i e^{-beta_t x_i}, E1_t = sum_i x_i w_i e^{-beta_t x_i},
+// E2_t = sum_i x_i^2 w_i e^{-beta_t x_i}, x_i = theta_i - e_min, summed in ascending theta (ties in QL order).
+// mom[q * n_items + item]: q = 0 e_min, then Z, E1, E2 of temperature t at q = 1 + 3t, 2 + 3t, 3 + 3t. scratch holds
+// 3 cap_max doubles and ord cap_max ints per item, strided by n_items so that a warp's loads coalesce.
+__global__ void k_sample_moments(const CurveBlock* blocks, int n_items, int k, const double* alpha, const double* beta,
+                                 const double* betas, int n_beta, int cap_max, double* scratch, int* ord, double* mom,
+                                 int* err) {
+    const int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= n_items) return;
+    const CurveBlock B = blocks[item / k];
+    const int s = item % k;
+    const std::size_t ld = static_cast<std::size_t>(n_items);
+    double* d = scratch + item;
+    double* e = scratch + static_cast<std::size_t>(cap_max) * ld + item;
+    double* z = scratch + 2 * static_cast<std::size_t>(cap_max) * ld + item;
+    int* o = ord + item;
+    const double* a = alpha + B.a_off;
+    const double* b = beta + B.b_off;
+    int m = 0;
+    for (int j = 0; j < B.cap; ++j) {
+        d[static_cast<std::size_t>(j) * ld] = a[static_cast<std::size_t>(j) * k + s];
+        const double bj = b[static_cast<std::size_t>(j + 1) * k + s];
+        e[static_cast<std::size_t>(j) * ld] = bj;
+        z[static_cast<std::size_t>(j) * ld] = j == 0 ? 1.0 : 0.0;
+        ++m;
+        if (bj < B.tol) break;
+    }
+    e[static_cast<std::size_t>(m - 1) * ld] = 0.0;
+    if (!ql_first_row(d, e, z, m, ld)) {
+        atomicExch(err, 1);
+        return;
+    }
+    // ascending order, stable: each value's rank among the values
+    for (int i = 0; i < m; ++i) {
+        const double vi = d[static_cast<std::size_t>(i) * ld];
+        int r = 0;
+        for (int q = 0; q < m; ++q) {
+            const double vq = d[static_cast<std::size_t>(q) * ld];
+            r += (vq < vi || (vq == vi && q < i)) ? 1 : 0;
+        }
+        o[static_cast<std::size_t>(r) * ld] = i;
+    }
+    double e_min = CUDART_INF, lo = CUDART_INF;
+    for (int r = 0; r < m; ++r) {
+        const int i = o[static_cast<std::size_t>(r) * ld];
+        const double v = d[static_cast<std::size_t>(i) * ld], zz = z[static_cast<std::size_t>(i) * ld];
+        lo = fmin(lo, v);
+        if (zz * zz > 0.0) e_min = fmin(e_min, v);
+    }
+    if (!isfinite(e_min)) e_min = lo;
+    mom[item] = e_min;
+    for (int t = 0; t < n_beta; ++t) {
+        const double bt = betas[t];
+        double zs = 0.0, e1 = 0.0, e2 = 0.0;
+        for (int r = 0; r < m; ++r) {
+            const int i = o[static_cast<std::size_t>(r) * ld];
+            const double x = d[static_cast<std::size_t>(i) * ld] - e_min;
+            const double zz = z[static_cast<std::size_t>(i) * ld];
+            const double bb = (zz * zz) * exp(-bt * x);
+            zs += bb;
+            e1 += x * bb;
+            e2 += x * x * bb;
+        }
+        mom[(1 + 3 * static_cast<std::size_t>(t)) * ld + item] = zs;
+        mom[(2 + 3 * static_cast<std::size_t>(t)) * ld + item] = e1;
+        mom[(3 + 3 * static_cast<std::size_t>(t)) * ld + item] = e2;
+    }
+}
+
+// One thread per (block, temperature): the block's samples combined in sample order about the least sample minimum
+// e_ref (combine_samples, include/ed/thermal/ftlm.h:199-235), a log-sum-exp over the samples' shifted partition
+// functions: lnZ = ln n + ln <Z> - beta e_ref, E = e_ref + <E1>/<Z>, V = <E2>/<Z> - (<E1>/<Z>)^2.
+__global__ void k_block_combine(const CurveBlock* blocks, int n_blocks, int k, const double* mom, int n_items,
+                                const double* betas, int n_beta, double* lnZ, double* E, double* V, double* e_min) {
+    const int nt = n_beta > 0 ? n_beta : 1;   // no temperatures: e_min alone
+    const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<long long>(n_blocks) * nt) return;
+    const int b = static_cast<int>(idx / nt), t = static_cast<int>(idx % nt);
+    const std::size_t ld = static_cast<std::size_t>(n_items);
+    const int i0 = b * k;
+    double e_ref = mom[i0];
+    for (int s = 1; s < k; ++s) e_ref = fmin(e_ref, mom[i0 + s]);
+    if (t == 0) e_min[b] = e_ref;
+    if (n_beta == 0) return;
+    const double bt = betas[t];
+    double zz = 0.0, e1 = 0.0, e2 = 0.0;
+    for (int s = 0; s < k; ++s) {
+        const int it = i0 + s;
+        const double dd = mom[it] - e_ref, r = exp(-bt * dd);
+        const double Z = mom[(1 + 3 * static_cast<std::size_t>(t)) * ld + it];
+        const double E1 = mom[(2 + 3 * static_cast<std::size_t>(t)) * ld + it];
+        const double E2 = mom[(3 + 3 * static_cast<std::size_t>(t)) * ld + it];
+        zz += Z * r;
+        e1 += (E1 + dd * Z) * r;
+        e2 += (E2 + 2.0 * dd * E1 + dd * dd * Z) * r;
+    }
+    zz /= k;
+    e1 /= k;
+    e2 /= k;
+    const std::size_t o = static_cast<std::size_t>(b) * n_beta + t;
+    if (zz > 1e-300) {
+        const double m1 = e1 / zz, m2 = e2 / zz;
+        lnZ[o] = log(static_cast<double>(blocks[b].dim)) + log(zz) - bt * e_ref;
+        E[o] = e_ref + m1;
+        V[o] = fmax(m2 - m1 * m1, 0.0);
+    } else {
+        lnZ[o] = -bt * e_ref;
+        E[o] = e_ref;
+        V[o] = 0.0;
+    }
+}
 
 // FTLM over many blocks (qb_ftlm_blocks; one block: qb_ftlm).
 void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int k, int depth,
@@ -529,7 +613,7 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         a_tot += static_cast<std::size_t>(caps[b]) * k;
         b_tot += static_cast<std::size_t>(caps[b] + 1) * k;
     }
-    PinnedBuf<double> ha(a_tot), hb(b_tot);
+    DevBuf<double> d_alpha(a_tot), d_beta(b_tot);
     std::vector<double> tol(n_blocks);
     // every block's reduced CSR, built before the recurrences (a build synchronises the device); a block
     // whose CSR does not fit runs on the walk
@@ -569,36 +653,53 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         tol[b] = 64.0 * std::numeric_limits<double>::epsilon() * norm_bound(progs[b]);
         // the buffers grow on the host's side of the stream: wait for the stream's previous block first
         BlockBufs& B = bufs[si];
-        const bool grow = B.w.n < static_cast<std::size_t>(n) * k || B.alpha.n < static_cast<std::size_t>(caps[b]) * k;
+        const bool grow = B.w.n < static_cast<std::size_t>(n) * k;
         if (grow) cuda_check(cudaStreamSynchronize(st), "stream");
-        B.ensure(n, k, caps[b], es);
+        B.ensure(n, k, es);
         k_sample_norms<<<k, kThreads, 0, st>>>(n, dG.p, len, B.inv.p);
         k_sample_start<<<red_blocks(static_cast<std::uint64_t>(n) * k), kThreads, 0, st>>>(n, k, dG.p, len, B.inv.p,
                                                                                             B.w.p);
-        block_recurrence(sec, progs[b], csrs.h[b], k, caps[b], tol[b], dtype, B, st, ha.p + a_off[b], hb.p + b_off[b]);
+        block_recurrence(sec, progs[b], csrs.h[b], k, caps[b], tol[b], dtype, B, st, d_alpha.p + a_off[b],
+                         d_beta.p + b_off[b]);
     }
     for (auto st : streams) cuda_check(cudaStreamSynchronize(st), "ftlm blocks");
     st_rec = secs_since(t_phase);
     t_phase = clock::now();
-    // the curves, on host threads
-    std::atomic<int> next{0};
-    std::vector<std::thread> pool;
-    const int nt = std::max(1, std::min<int>(n_blocks, static_cast<int>(std::thread::hardware_concurrency())));
-    std::vector<std::string> errs(nt);
-    for (int t = 0; t < nt; ++t)
-        pool.emplace_back([&, t] {
-            try {
-                for (int b = next++; b < n_blocks; b = next++)
-                    block_curves(ha.p + a_off[b], hb.p + b_off[b], k, caps[b], tol[b], secs[b]->dim, betas, n_beta,
-                                 lnZ + static_cast<std::size_t>(b) * n_beta, E + static_cast<std::size_t>(b) * n_beta,
-                                 V + static_cast<std::size_t>(b) * n_beta, e_min + b);
-            } catch (const std::exception& e) {
-                errs[t] = e.what();
-            }
-        });
-    for (auto& t : pool) t.join();
-    for (const auto& e : errs)
-        if (!e.empty()) throw Error(QB_EINVAL, e);
+    // the curves on the device: one thread per (block, sample), then one per (block, temperature)
+    const int n_items = n_blocks * k;
+    int cap_max = 1;
+    std::vector<CurveBlock> cb(n_blocks);
+    for (int b = 0; b < n_blocks; ++b) {
+        cb[b] = CurveBlock{a_off[b], b_off[b], secs[b]->dim, tol[b], caps[b]};
+        cap_max = std::max(cap_max, caps[b]);
+    }
+    DevBuf<CurveBlock> d_cb(n_blocks);
+    DevBuf<double> d_betas(std::max(1, n_beta)), scratch(3 * static_cast<std::size_t>(cap_max) * n_items);
+    DevBuf<double> mom((1 + 3 * static_cast<std::size_t>(n_beta)) * n_items);
+    DevBuf<int> ord(static_cast<std::size_t>(cap_max) * n_items), err(1);
+    const std::size_t nbt = static_cast<std::size_t>(n_blocks) * n_beta;
+    DevBuf<double> out(3 * nbt + n_blocks);
+    cudaStream_t st0 = cudaStreamPerThread;
+    cuda_check(cudaMemcpyAsync(d_cb.p, cb.data(), n_blocks * sizeof(CurveBlock), cudaMemcpyHostToDevice, st0), "upload");
+    if (n_beta > 0)
+        cuda_check(cudaMemcpyAsync(d_betas.p, betas, n_beta * 8, cudaMemcpyHostToDevice, st0), "upload");
+    cuda_check(cudaMemsetAsync(err.p, 0, 4, st0), "zero");
+    k_sample_moments<<<(n_items + 127) / 128, 128, 0, st0>>>(d_cb.p, n_items, k, d_alpha.p, d_beta.p, d_betas.p, n_beta,
+                                                           cap_max, scratch.p, ord.p, mom.p, err.p);
+    const std::size_t n_comb = static_cast<std::size_t>(n_blocks) * std::max(1, n_beta);
+    k_block_combine<<<static_cast<unsigned>((n_comb + 127) / 128), 128, 0, st0>>>(
+        d_cb.p, n_blocks, k, mom.p, n_items, d_betas.p, n_beta, out.p, out.p + nbt, out.p + 2 * nbt, out.p + 3 * nbt);
+    cuda_check(cudaGetLastError(), "ftlm curves");
+    std::vector<double> host(3 * nbt + n_blocks);
+    int h_err = 0;
+    cuda_check(cudaMemcpyAsync(host.data(), out.p, host.size() * 8, cudaMemcpyDeviceToHost, st0), "curves");
+    cuda_check(cudaMemcpyAsync(&h_err, err.p, 4, cudaMemcpyDeviceToHost, st0), "curves");
+    cuda_check(cudaStreamSynchronize(st0), "ftlm curves");
+    if (h_err) throw Error(QB_ECUDA, "tridiagonal QL did not converge");
+    std::copy(host.begin(), host.begin() + nbt, lnZ);
+    std::copy(host.begin() + nbt, host.begin() + 2 * nbt, E);
+    std::copy(host.begin() + 2 * nbt, host.begin() + 3 * nbt, V);
+    std::copy(host.begin() + 3 * nbt, host.end(), e_min);
     st_curves = secs_since(t_phase);
     if (stats) {
         stats[0] = st_draw;
