@@ -42,6 +42,7 @@
 #include "qb_internal.cuh"
 
 #include "qb_krylov.cuh"
+#include "qb_walk.cuh"
 
 namespace qb {
 namespace {
@@ -386,6 +387,327 @@ void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr
     }
 }
 
+// ---- the small blocks, packed: one CTA runs a whole block ----
+// A block's recurrence is launch-bound when the block is small: three launches a step do little work each. The
+// packed kernel hands whole blocks to persistent CTAs instead (largest first, from an atomic counter): the CTA
+// walks its block once into merged rows (each row's entries sorted by column, equal columns summed in emission
+// order, exact zeros dropped: the rows of the block's reduced CSR, bit for bit), forms the start columns from the
+// sample table, and runs every step of the block's recurrence with block-wide fixed-order reductions. It writes
+// alpha and beta where the per-block path would; only the order of the inner-product sums differs from it.
+struct PackItem {
+    DSector sec;
+    DProgram prog;
+    unsigned long long a_off, b_off;
+    double tol;
+    int cap, in_smem;
+};
+
+// A CTA's scratch: each row's merged entries (at most max_entries) and the three working columns of the block.
+struct PackSlot {
+    std::size_t col_off, val_off, cnt_off, vec_off, vec_bytes, bytes;
+};
+
+__host__ __device__ inline PackSlot pack_slot(std::uint64_t n_max, int max_entries, int k, std::size_t es) {
+    auto al = [](std::size_t x) { return (x + 255) & ~std::size_t(255); };
+    PackSlot p;
+    const std::size_t ne = static_cast<std::size_t>(n_max) * max_entries;
+    p.col_off = 0;
+    p.val_off = al(ne * 4);
+    p.cnt_off = p.val_off + al(ne * 16);
+    p.vec_off = p.cnt_off + al(static_cast<std::size_t>(n_max) * 4);
+    p.vec_bytes = al(static_cast<std::size_t>(n_max) * k * es);
+    p.bytes = p.vec_off + 3 * p.vec_bytes;
+    return p;
+}
+
+// The column sums of a block-wide quantity: red[c][rg] holds row group rg's partial of column c; thread c < k
+// sums the 32 row groups in order.
+__device__ __forceinline__ double pack_col_sum(double (*red)[33], int c) {
+    double s = 0.0;
+    for (int g = 0; g < 32; ++g) s += red[c][g];
+    return s;
+}
+
+template <class T, class ST, int CPL>
+__global__ void __launch_bounds__(256) ftlm_pack(const PackItem* items, int n_items, unsigned* next_item, int k,
+                                                 int max_entries, const double2* G, std::uint64_t ld, double* alpha,
+                                                 double* beta, unsigned char* scratch, PackSlot slot) {
+    using Rt = typename Work<T>::R;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[kMaxCols][33];
+    __shared__ double sm[32];
+    __shared__ double s_a[kMaxCols], s_b[kMaxCols], s_o[2][kMaxCols], s_inv[kMaxCols];
+    __shared__ unsigned s_item;
+    unsigned char* base = scratch + static_cast<std::size_t>(blockIdx.x) * slot.bytes;
+    u32* ecol = reinterpret_cast<u32*>(base + slot.col_off);
+    double2* eval = reinterpret_cast<double2*>(base + slot.val_off);
+    int* ecnt = reinterpret_cast<int*>(base + slot.cnt_off);
+    T* vbuf[3] = {reinterpret_cast<T*>(base + slot.vec_off), reinterpret_cast<T*>(base + slot.vec_off + slot.vec_bytes),
+                  reinterpret_cast<T*>(base + slot.vec_off + 2 * slot.vec_bytes)};
+    const int lane = threadIdx.x & 7, rg = threadIdx.x >> 3;
+    for (;;) {
+        __syncthreads();   // the previous block's last reads of the shared tables are done
+        if (threadIdx.x == 0) s_item = atomicAdd(next_item, 1u);
+        __syncthreads();
+        const unsigned it = s_item;
+        if (it >= static_cast<unsigned>(n_items)) return;
+        const PackItem& I = items[it];
+        const std::uint64_t n = I.sec.dim;
+        const int cap = I.cap;
+        // ---- the block's merged rows ----
+        const SmemProgram sp = stage(I.prog, I.sec, smem, I.in_smem != 0);
+        for (std::uint64_t r = threadIdx.x; r < n; r += blockDim.x) {
+            const ST s = static_cast<ST>(__ldg(I.sec.reps + r));
+            const double wr = __ldg(I.sec.inv_norms + r);
+            u32* rc = ecol + r * max_entries;
+            double2* rv = eval + r * max_entries;
+            int m = 0;
+            for (u32 g = 0; g < sp.P.n_groups; ++g) {
+                const int vi = acting_subgroup<ST>(sp.P, s, g);
+                if (vi < 0) continue;
+                const cplx h = subgroup_value<ST>(sp.P, s, vi);
+                const ST t = s ^ static_cast<ST>(sp.P.group_flip[g]);
+                long long j;
+                cplx c;
+                if (!entry<true, ST>(I.sec, sp.T, s, static_cast<long long>(r), wr, t, h, j, c)) continue;
+                // insertion by column; an equal column goes after the earlier emissions
+                int p = m++;
+                while (p > 0 && rc[p - 1] > static_cast<u32>(j)) {
+                    rc[p] = rc[p - 1];
+                    rv[p] = rv[p - 1];
+                    --p;
+                }
+                rc[p] = static_cast<u32>(j);
+                rv[p] = make_double2(c.re, c.im);
+            }
+            int mo = 0;
+            for (int p = 0; p < m;) {
+                const u32 cj = rc[p];
+                cplx sum{rv[p].x, rv[p].y};
+                int q = p + 1;
+                for (; q < m && rc[q] == cj; ++q) sum = cadd(sum, {rv[q].x, rv[q].y});
+                if (sum.re != 0.0 || sum.im != 0.0) {
+                    rc[mo] = cj;
+                    rv[mo] = make_double2(sum.re, sum.im);
+                    ++mo;
+                }
+                p = q;
+            }
+            ecnt[r] = mo;
+        }
+        // ---- the start columns: sample s normalised over the block's prefix (the fixed tree of k_sample_norms) ----
+        for (int s = 0; s < k; ++s) {
+            const double2* g = G + static_cast<std::size_t>(s) * ld;
+            double v[1] = {0.0};
+            for (std::uint64_t i = threadIdx.x; i < n; i += blockDim.x) v[0] += g[i].x * g[i].x + g[i].y * g[i].y;
+            block_reduce<1>(v, sm);
+            if (threadIdx.x == 0) s_inv[s] = v[0] > 0.0 ? 1.0 / sqrt(v[0]) : 0.0;
+            __syncthreads();
+        }
+        T* vp = vbuf[0];
+        T* vc = vbuf[1];
+        T* w = vbuf[2];
+        for (std::uint64_t i = threadIdx.x; i < n * k; i += blockDim.x) {
+            const int s = static_cast<int>(i % k);
+            const double2 g = G[static_cast<std::size_t>(s) * ld + i / k];
+            Work<T>::st(vc, i, static_cast<Rt>(g.x * s_inv[s]), static_cast<Rt>(g.y * s_inv[s]));
+            Work<T>::st(vp, i, Rt(0), Rt(0));
+        }
+        double* al = alpha + I.a_off;
+        double* be = beta + I.b_off;
+        if (threadIdx.x < k) {
+            s_b[threadIdx.x] = 0.0;
+            be[threadIdx.x] = 0.0;   // beta_0
+        }
+        __syncthreads();
+        for (int j = 0; j < cap; ++j) {
+            // pass 1: w = A v_j - beta_j v_{j-1}, and alpha_j = Re <v_j, w>
+            Rt b[CPL];
+            double ap[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int cc = lane + 8 * c;
+                b[c] = (j > 0 && cc < k) ? static_cast<Rt>(s_b[cc]) : Rt(0);
+                ap[c] = 0.0;
+            }
+            for (std::uint64_t r = rg; r < n; r += 32) {
+                Rt ar[CPL], ai[CPL];
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) ar[c] = ai[c] = Rt(0);
+                const int m = ecnt[r];
+                for (int e = 0; e < m; ++e) {
+                    const double2 v2 = eval[r * max_entries + e];
+                    const Rt vr = static_cast<Rt>(v2.x), vi = static_cast<Rt>(v2.y);
+                    const std::size_t xb = static_cast<std::size_t>(ecol[r * max_entries + e]) * k;
+#pragma unroll
+                    for (int c = 0; c < CPL; ++c) {
+                        const int cc = lane + 8 * c;
+                        if (cc < k) {
+                            const T x = vc[xb + cc];
+                            ar[c] = fma(vr, x.x, fma(-vi, x.y, ar[c]));
+                            ai[c] = fma(vr, x.y, fma(vi, x.x, ai[c]));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                    const int cc = lane + 8 * c;
+                    if (cc >= k) continue;
+                    const std::size_t i = static_cast<std::size_t>(r) * k + cc;
+                    Rt yr = ar[c], yi = ai[c];
+                    if (j > 0) {
+                        const T p = vp[i];
+                        yr = fma(-b[c], p.x, yr);
+                        yi = fma(-b[c], p.y, yi);
+                    }
+                    Work<T>::st(w, i, yr, yi);
+                    const T z = vc[i];
+                    ap[c] += static_cast<double>(z.x) * yr + static_cast<double>(z.y) * yi;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int cc = lane + 8 * c;
+                if (cc < k) red[cc][rg] = ap[c];
+            }
+            __syncthreads();
+            if (threadIdx.x < k) {
+                const double a = pack_col_sum(red, threadIdx.x);
+                s_a[threadIdx.x] = a;
+                al[static_cast<std::size_t>(j) * k + threadIdx.x] = a;
+            }
+            __syncthreads();
+            // pass 2: the norms and local overlaps of w - alpha_j v_j -> beta_{j+1}
+            double q3[3][CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) q3[0][c] = q3[1][c] = q3[2][c] = 0.0;
+            for (std::uint64_t r = rg; r < n; r += 32) {
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                    const int cc = lane + 8 * c;
+                    if (cc >= k) continue;
+                    const std::size_t i = static_cast<std::size_t>(r) * k + cc;
+                    const T y0 = w[i], z0 = vc[i];
+                    const double zx = z0.x, zy = z0.y, a = s_a[cc];
+                    const double yx = y0.x - a * zx, yy = y0.y - a * zy;
+                    q3[0][c] += yx * yx + yy * yy;
+                    q3[1][c] += zx * yx + zy * yy;
+                    q3[2][c] += zx * yy - zy * yx;
+                }
+            }
+            double tot[3] = {0.0, 0.0, 0.0};
+            for (int q = 0; q < 3; ++q) {
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                    const int cc = lane + 8 * c;
+                    if (cc < k) red[cc][rg] = q3[q][c];
+                }
+                __syncthreads();
+                if (threadIdx.x < k) tot[q] = pack_col_sum(red, threadIdx.x);
+                __syncthreads();
+            }
+            if (threadIdx.x < k) {
+                const int c = threadIdx.x;
+                double nrm2 = tot[0];
+                const double ore = tot[1], oim = tot[2];
+                const bool proj = j > 0 && sqrt(ore * ore + oim * oim) > kLocalThreshold;
+                if (proj) nrm2 = fmax(nrm2 - (ore * ore + oim * oim), 0.0);
+                s_o[0][c] = proj ? -ore : 0.0;
+                s_o[1][c] = proj ? -oim : 0.0;
+                s_b[c] = sqrt(nrm2);
+                be[static_cast<std::size_t>(j + 1) * k + c] = s_b[c];
+            }
+            __syncthreads();
+            // pass 3: v_{j+1} = (w - alpha_j v_j + o v_j) / beta_{j+1}, into v_{j-1}'s columns
+            for (std::uint64_t i = threadIdx.x; i < n * k; i += blockDim.x) {
+                const int c = static_cast<int>(i % k);
+                const double bb = s_b[c];
+                const double inv = bb >= I.tol && bb > 0.0 ? 1.0 / bb : 0.0;
+                const double a = s_a[c], ore = s_o[0][c], oim = s_o[1][c];
+                const T y0 = w[i], z0 = vc[i];
+                const double zx = z0.x, zy = z0.y;
+                double yx = y0.x - a * zx, yy = y0.y - a * zy;
+                yx += ore * zx - oim * zy;
+                yy += ore * zy + oim * zx;
+                Work<T>::st(vp, i, static_cast<Rt>(yx * inv), static_cast<Rt>(yy * inv));
+            }
+            __syncthreads();
+            T* t = vp;
+            vp = vc;
+            vc = t;
+        }
+    }
+}
+
+// The largest block the packed kernel takes whole (QB_FTLM_PACK_DIM, default 4096 states; 0 turns it off).
+std::uint64_t pack_max_dim() {
+    const char* e = std::getenv("QB_FTLM_PACK_DIM");
+    if (!e || !*e) return 4096;
+    return std::strtoull(e, nullptr, 10);
+}
+
+// Shared memory of a packed block's staged tables and program, and the most the packed kernel accepts.
+constexpr std::size_t kPackSmemMax = 160 * 1024;
+constexpr int kPackMaxEntries = 256;
+
+// Launches ftlm_pack over the blocks `set` (largest first) on st; the scratch and item buffers are the caller's
+// and must outlive the kernel.
+template <class ST>
+void launch_pack(const std::vector<int>& set, const qb_sector* const* secs, const qb_program* const* progs, int k,
+                 int dtype, const std::vector<std::size_t>& a_off, const std::vector<std::size_t>& b_off,
+                 const std::vector<int>& caps, const std::vector<double>& tol, const double2* G, std::uint64_t ld,
+                 double* alpha, double* beta, DevBuf<PackItem>& d_items, DevBuf<unsigned>& counter,
+                 DevBuf<unsigned char>& scratch, cudaStream_t st) {
+    if (set.empty()) return;
+    std::vector<PackItem> items(set.size());
+    std::uint64_t n_max = 1;
+    int max_entries = 1;
+    std::size_t smem = 0;
+    for (std::size_t i = 0; i < set.size(); ++i) {
+        const int b = set[i];
+        bool in_smem = false;
+        smem = std::max(smem, smem_for(progs[b], secs[b], in_smem));
+        items[i] = PackItem{secs[b]->view(), progs[b]->view, a_off[b], b_off[b], tol[b], caps[b], in_smem ? 1 : 0};
+        n_max = std::max(n_max, secs[b]->dim);
+        max_entries = std::max(max_entries, static_cast<int>(progs[b]->view.n_groups));
+    }
+    const std::size_t es = dtype == QB_C64 ? 8 : 16;
+    const PackSlot slot = pack_slot(n_max, max_entries, k, es);
+    const int cpl = (k + 7) / 8;
+    auto go = [&](auto kernel) {
+        set_smem(kernel, smem);
+        int dev = 0, sms = 148, per_sm = 1;
+        cuda_check(cudaGetDevice(&dev), "device");
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem), "occupancy");
+        const int grid = static_cast<int>(std::min<std::size_t>(set.size(), static_cast<std::size_t>(sms) *
+                                                                               std::max(1, std::min(per_sm, 2))));
+        d_items.alloc(items.size());
+        counter.alloc(1);
+        scratch.alloc(slot.bytes * grid);
+        cuda_check(cudaMemcpyAsync(d_items.p, items.data(), items.size() * sizeof(PackItem), cudaMemcpyHostToDevice,
+                                   st), "pack items");
+        cuda_check(cudaMemsetAsync(counter.p, 0, 4, st), "zero");
+        kernel<<<grid, 256, smem, st>>>(d_items.p, static_cast<int>(items.size()), counter.p, k, max_entries, G, ld,
+                                        alpha, beta, scratch.p, slot);
+        cuda_check(cudaGetLastError(), "ftlm_pack launch");
+    };
+#define QB_PACK(T, C) go(ftlm_pack<T, ST, C>)
+#define QB_PACK_T(T)                  \
+    if (cpl <= 1) QB_PACK(T, 1);      \
+    else if (cpl <= 2) QB_PACK(T, 2); \
+    else if (cpl <= 4) QB_PACK(T, 4); \
+    else if (cpl <= 5) QB_PACK(T, 5); \
+    else QB_PACK(T, 8);
+    if (dtype == QB_C64) {
+        QB_PACK_T(float2)
+    } else {
+        QB_PACK_T(double2)
+    }
+#undef QB_PACK_T
+#undef QB_PACK
+}
+
 // ---- the curves on the device ----
 // A block's place in the call's alpha [cap][k] / beta [cap + 1][k] arrays, its dimension and breakdown tolerance.
 struct CurveBlock {
@@ -615,6 +937,39 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
     }
     DevBuf<double> d_alpha(a_tot), d_beta(b_tot);
     std::vector<double> tol(n_blocks);
+    for (int b = 0; b < n_blocks; ++b) tol[b] = 64.0 * std::numeric_limits<double>::epsilon() * norm_bound(progs[b]);
+    // the small blocks, run whole by the packed kernel on a stream of their own while the others build their CSRs
+    std::vector<char> packed(n_blocks, 0);
+    std::vector<int> pack_set[2];   // 32-bit and 64-bit states
+    if (use_csr) {
+        const std::uint64_t pmax = pack_max_dim();
+        for (int i = 0; i < n_blocks; ++i) {
+            const int b = order[i];
+            bool in_smem = false;
+            if (secs[b]->dim > pmax || smem_for(progs[b], secs[b], in_smem) > kPackSmemMax ||
+                progs[b]->view.n_groups > static_cast<u32>(kPackMaxEntries))
+                continue;
+            packed[b] = 1;
+            pack_set[secs[b]->N <= 32 ? 0 : 1].push_back(b);
+        }
+    }
+    cudaStream_t pst = nullptr;
+    cuda_check(cudaStreamCreateWithFlags(&pst, cudaStreamNonBlocking), "stream");
+    struct PackStream {
+        cudaStream_t s;
+        ~PackStream() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    };
+    DevBuf<PackItem> pack_items[2];
+    DevBuf<unsigned> pack_counter[2];
+    DevBuf<unsigned char> pack_scratch[2];
+    PackStream pack_guard{pst};
+    launch_pack<u32>(pack_set[0], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, len, d_alpha.p, d_beta.p,
+                     pack_items[0], pack_counter[0], pack_scratch[0], pst);
+    launch_pack<u64>(pack_set[1], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, len, d_alpha.p, d_beta.p,
+                     pack_items[1], pack_counter[1], pack_scratch[1], pst);
     // every block's reduced CSR, built before the recurrences (a build synchronises the device); a block
     // whose CSR does not fit runs on the walk
     struct Csrs {
@@ -637,20 +992,21 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
             builders.emplace_back([&] {
                 cudaSetDevice(dev);
                 for (int b = next_b++; b < n_blocks; b = next_b++)
-                    if (qb_csr_build(secs[b], secs[b], progs[b], 0, &csrs.h[b]) != QB_OK) csrs.h[b] = nullptr;
+                    if (!packed[b] && qb_csr_build(secs[b], secs[b], progs[b], 0, &csrs.h[b]) != QB_OK)
+                        csrs.h[b] = nullptr;
                 cudaStreamSynchronize(cudaStreamPerThread);
             });
         for (auto& t : builders) t.join();
     }
     st_csr = secs_since(t_phase);
     t_phase = clock::now();
-    for (int i = 0; i < n_blocks; ++i) {
+    for (int i = 0, q = 0; i < n_blocks; ++i) {
         const int b = order[i];
-        const int si = i % ns;
+        if (packed[b]) continue;
+        const int si = q++ % ns;
         cudaStream_t st = streams[si];
         const qb_sector* sec = secs[b];
         const std::uint64_t n = sec->dim;
-        tol[b] = 64.0 * std::numeric_limits<double>::epsilon() * norm_bound(progs[b]);
         // the buffers grow on the host's side of the stream: wait for the stream's previous block first
         BlockBufs& B = bufs[si];
         const bool grow = B.w.n < static_cast<std::size_t>(n) * k;
@@ -663,6 +1019,7 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
                          d_beta.p + b_off[b]);
     }
     for (auto st : streams) cuda_check(cudaStreamSynchronize(st), "ftlm blocks");
+    cuda_check(cudaStreamSynchronize(pst), "ftlm packed blocks");
     st_rec = secs_since(t_phase);
     t_phase = clock::now();
     // the curves on the device: one thread per (block, sample), then one per (block, temperature)

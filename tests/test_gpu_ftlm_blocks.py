@@ -48,9 +48,13 @@ def oracle_curves():
     return specs, prog, curves
 
 
-@pytest.mark.parametrize("dtype,use_csr", [("c128", True), ("c128", False), ("c64", True)])
-def test_blocks_match_oracle(oracle_curves, dtype, use_csr):
+# pack: the largest block the packed kernel runs whole (QB_FTLM_PACK_DIM; "0" sends every block down the
+# per-block path, "40" splits the N = 12 blocks between the two)
+@pytest.mark.parametrize("dtype,use_csr,pack", [("c128", True, "4096"), ("c128", True, "40"), ("c128", True, "0"),
+                                                ("c128", False, "4096"), ("c64", True, "4096"), ("c64", True, "0")])
+def test_blocks_match_oracle(oracle_curves, monkeypatch, dtype, use_csr, pack):
     from qed_spin_b200 import device as D
+    monkeypatch.setenv("QB_FTLM_PACK_DIM", pack)
     specs, prog, curves = oracle_curves
     secs = [D.Sector(s) for s in specs]
     P = D.Program(prog)
@@ -95,3 +99,22 @@ def test_one_block_call_equals_batch(oracle_curves):
         one = D.ftlm(s, P, 8, 30, SEED, BETAS)
         for key in ("lnZ", "E", "V"):
             np.testing.assert_array_equal(one[key], r[key][j])
+
+
+@pytest.mark.parametrize("dtype,tol", [("c128", 1e-10), ("c64", 1e-5)])
+def test_packed_blocks_equal_per_block_path(monkeypatch, dtype, tol):
+    """Blocks of a few hundred states run whole by one CTA each give the curves of the per-block path (the two
+    differ only in the order of their inner-product sums): 1e-10 relative in FP64 storage, 1e-5 in FP32."""
+    from qed_spin_b200 import device as D
+    n = 16
+    prods = ops.xxz_products(lat.chain_bonds(n), 1.0, 0.5) + ops.zeeman_z_products(n, 0.1)
+    P = D.Program(ops.row_program(ops.from_products(n, prods)))
+    secs = [D.Sector(lat.chain_sector(n, n_up, k)) for n_up, k in [(8, 0), (8, 3), (7, 5), (5, 1), (2, 2), (1, 0)]]
+    assert max(s.dim for s in secs) > 700
+    out = {}
+    for pack in ("4096", "0"):
+        monkeypatch.setenv("QB_FTLM_PACK_DIM", pack)
+        out[pack] = D.ftlm_blocks(secs, P, 12, 40, SEED, BETAS, dtype=dtype)
+    for key in ("lnZ", "E", "V"):
+        a, b = out["4096"][key], out["0"][key]
+        np.testing.assert_allclose(a, b, rtol=tol, atol=tol * np.abs(b).max(), err_msg=key)
