@@ -114,6 +114,51 @@ template <> struct Work<double2> {
     __device__ static void st(double2* p, std::size_t i, double x, double y) { p[i] = make_double2(x, y); }
 };
 
+// Deterministic grid-wide sums of NQ per-column quantities, in two levels: every block writes its partials; the
+// last block to finish in each group of 32 blocks sums the group's partials in block order; the last group to
+// finish sums the group totals in group order into tot (shared memory) and returns true, in that one block only.
+// Thread t < NQ k holds its block's partial of quantity t / k, column t % k in `mine`; every thread calls.
+template <int NQ>
+__device__ __forceinline__ bool grid_sum2(double mine, int k, const BScal& S, double (*tot)[kMaxCols]) {
+    __shared__ bool last;
+    const int t = threadIdx.x, nqk = NQ * k;
+    const unsigned b = blockIdx.x, g = b >> 5, ng = (gridDim.x + 31) >> 5;
+    const unsigned gsize = min(32u, gridDim.x - (g << 5));
+    if (t < nqk) S.partials[static_cast<std::size_t>(t) * kMaxRedBlocks + b] = mine;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(S.group_counter + g, 1u) == gsize - 1;
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    if (t < nqk) {
+        const double* p = S.partials + static_cast<std::size_t>(t) * kMaxRedBlocks + (g << 5);
+        double s = 0.0;
+        for (unsigned i = 0; i < gsize; ++i) s += __ldcg(p + i);
+        S.partials2[static_cast<std::size_t>(t) * kMaxGroups + g] = s;
+    }
+    if (t == 0) S.group_counter[g] = 0;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(S.counter, 1u) == ng - 1;
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    if (t < nqk) {
+        const double* p = S.partials2 + static_cast<std::size_t>(t) * kMaxGroups;
+        double s = 0.0;
+        for (unsigned i = 0; i < ng; ++i) s += __ldcg(p + i);
+        tot[t / k][t % k] = s;
+    }
+    if (t == 0) *S.counter = 0;
+    __syncthreads();
+    return true;
+}
+
+// The row-tile shape of the streaming passes: a block of R k threads, thread t on column t % k and row t / k of
+// each R-row tile, so a block reads whole rows contiguously and every thread keeps one column.
+__host__ __device__ inline int tile_rows(int k) { return k >= 256 ? 1 : 256 / k; }
+
 // Pass 1: w = A v_j - beta_j v_{j-1} on the CSR (8 lanes per row, lane l owns columns l, l + 8, ...), and
 // alpha_j = Re <v_j, w> per column: block partials in shared memory summed in row order, the block sums in
 // block order by the last block.
@@ -209,72 +254,75 @@ __global__ void __launch_bounds__(256) fmv_alpha(std::uint64_t rows, int k, int 
 }
 
 // Pass 2: the norms and the local-reorthogonalisation overlaps of w - alpha_j v_j (not stored) -> beta_{j+1}.
-template <class T, int CPL>
-__global__ void fbeta(std::uint64_t n, int k, int j, const T* w, const T* vc, BScal S) {
-    extern __shared__ double bsm[];
+template <class T>
+__global__ void __launch_bounds__(256) fbeta(std::uint64_t n, int k, int j, const T* __restrict__ w,
+                                             const T* __restrict__ vc, BScal S) {
+    __shared__ double sm[3][256];
     __shared__ double tot[3][kMaxCols];
-    const int lane = threadIdx.x & 31;
-    double v[3][CPL];
-    double a[CPL];
+    const int R = tile_rows(k);
+    const int c = threadIdx.x % k, rr = threadIdx.x / k;
+    const double a = S.alpha[static_cast<std::size_t>(j) * k + c];
+    double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+    const std::uint64_t step = static_cast<std::uint64_t>(gridDim.x) * R;
+    constexpr int U = 4;   // rows in flight per thread
+    std::uint64_t r = static_cast<std::uint64_t>(blockIdx.x) * R + rr;
+    auto add = [&](const T y0, const T z0) {
+        const double zx = z0.x, zy = z0.y;
+        const double yx = y0.x - a * zx, yy = y0.y - a * zy;
+        q0 += yx * yx + yy * yy;
+        q1 += zx * yx + zy * yy;
+        q2 += zx * yy - zy * yx;
+    };
+    for (; r + (U - 1) * step < n; r += U * step) {
+        T y[U], z[U];
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) {
-        v[0][c] = v[1][c] = v[2][c] = 0.0;
-        const int col = lane + 32 * c;
-        a[c] = col < k ? S.alpha[static_cast<std::size_t>(j) * k + col] : 0.0;
+        for (int u = 0; u < U; ++u) {
+            const std::size_t i = (r + u * step) * k + c;
+            y[u] = w[i];
+            z[u] = vc[i];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) add(y[u], z[u]);
     }
-    // four rows per warp iteration, all their loads issued before the sums
-    constexpr int kRows = 4;
-    const std::uint64_t warps = static_cast<std::uint64_t>(gridDim.x) * (blockDim.x >> 5);
-    for (std::uint64_t r0 = (static_cast<std::uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRows;
-         r0 < n; r0 += warps * kRows) {
-        T y0[kRows][CPL], z0[kRows][CPL];
-#pragma unroll
-        for (int q = 0; q < kRows; ++q)
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) {
-                const int col = lane + 32 * c;
-                if (col < k && r0 + q < n) {
-                    const std::size_t i = (r0 + q) * k + col;
-                    y0[q][c] = w[i];
-                    z0[q][c] = vc[i];
-                }
-            }
-#pragma unroll
-        for (int q = 0; q < kRows; ++q)
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) {
-                const int col = lane + 32 * c;
-                if (col >= k || r0 + q >= n) continue;
-                const double zx = z0[q][c].x, zy = z0[q][c].y;
-                const double yx = y0[q][c].x - a[c] * zx, yy = y0[q][c].y - a[c] * zy;
-                v[0][c] += yx * yx + yy * yy;
-                v[1][c] += zx * yx + zy * yy;
-                v[2][c] += zx * yy - zy * yx;
-            }
+    for (; r < n; r += step) {
+        const std::size_t i = r * k + c;
+        add(w[i], vc[i]);
     }
-    if (block_cols_total<3, CPL>(v, k, S, bsm, tot) && threadIdx.x < k) {
-        const int c = threadIdx.x;
-        double nrm2 = tot[0][c];
-        const double ore = tot[1][c], oim = tot[2][c];
+    sm[0][threadIdx.x] = q0;
+    sm[1][threadIdx.x] = q1;
+    sm[2][threadIdx.x] = q2;
+    __syncthreads();
+    // the block's partial of (quantity q, column cc): its R row slots in order
+    double mine = 0.0;
+    if (threadIdx.x < 3 * k) {
+        const int q = threadIdx.x / k, cc = threadIdx.x % k;
+        for (int s = 0; s < R; ++s) mine += sm[q][s * k + cc];
+    }
+    if (grid_sum2<3>(mine, k, S, tot) && threadIdx.x < k) {
+        const int cc = threadIdx.x;
+        double nrm2 = tot[0][cc];
+        const double ore = tot[1][cc], oim = tot[2][cc];
         const bool proj = j > 0 && sqrt(ore * ore + oim * oim) > kLocalThreshold;
         if (proj) nrm2 = fmax(nrm2 - (ore * ore + oim * oim), 0.0);
-        S.ovl[c] = proj ? -ore : 0.0;
-        S.ovl[kMaxCols + c] = proj ? -oim : 0.0;
-        S.beta[static_cast<std::size_t>(j + 1) * k + c] = sqrt(nrm2);
+        S.ovl[cc] = proj ? -ore : 0.0;
+        S.ovl[kMaxCols + cc] = proj ? -oim : 0.0;
+        S.beta[static_cast<std::size_t>(j + 1) * k + cc] = sqrt(nrm2);
     }
 }
 
 // Pass 3: v_{j+1} = (w - alpha_j v_j + o v_j) / beta_{j+1}; a column past its breakdown goes to zero.
 template <class T>
-__global__ void fnext(std::uint64_t n, int k, int j, double tol, const T* w, const T* vc, T* vn, BScal S) {
-    const std::uint64_t total = n * k;
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % k);
-        const double b = S.beta[static_cast<std::size_t>(j + 1) * k + c];
-        const double inv = b >= tol && b > 0.0 ? 1.0 / b : 0.0;
-        const double a = S.alpha[static_cast<std::size_t>(j) * k + c];
-        const double ore = S.ovl[c], oim = S.ovl[kMaxCols + c];
+__global__ void __launch_bounds__(256) fnext(std::uint64_t n, int k, int j, double tol, const T* __restrict__ w,
+                                             const T* __restrict__ vc, T* __restrict__ vn, BScal S) {
+    const int R = tile_rows(k);
+    const int c = threadIdx.x % k, rr = threadIdx.x / k;
+    const double b = S.beta[static_cast<std::size_t>(j + 1) * k + c];
+    const double inv = b >= tol && b > 0.0 ? 1.0 / b : 0.0;
+    const double a = S.alpha[static_cast<std::size_t>(j) * k + c];
+    const double ore = S.ovl[c], oim = S.ovl[kMaxCols + c];
+    const std::uint64_t step = static_cast<std::uint64_t>(gridDim.x) * R;
+    for (std::uint64_t r = static_cast<std::uint64_t>(blockIdx.x) * R + rr; r < n; r += step) {
+        const std::size_t i = r * k + c;
         const T y0 = w[i], z0 = vc[i];
         const double zx = z0.x, zy = z0.y;
         double yx = y0.x - a * zx, yy = y0.y - a * zy;
@@ -298,13 +346,11 @@ void fused_step(const qb_csr* A, std::uint64_t n, int k, int j, double tol, cons
     else if (cpl <= 5) QB_FMV(5);
     else QB_FMV(8);
 #undef QB_FMV
-    const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kBlockRecGrid)));
-    const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);
-    if (k <= 32)
-        fbeta<T, 1><<<rb, kThreads, bsm, st>>>(n, k, j, w, vc, S);
-    else
-        fbeta<T, 2><<<rb, kThreads, bsm, st>>>(n, k, j, w, vc, S);
-    fnext<T><<<red_blocks(n * k), kThreads, 0, st>>>(n, k, j, tol, w, vc, vn, S);
+    const int R = tile_rows(k);
+    const std::uint64_t tiles = (n + R - 1) / R;
+    const unsigned rb = static_cast<unsigned>(std::min<std::uint64_t>(tiles, kMaxRedBlocks));
+    fbeta<T><<<rb, R * k, 0, st>>>(n, k, j, w, vc, S);
+    fnext<T><<<rb, R * k, 0, st>>>(n, k, j, tol, w, vc, vn, S);
     cuda_check(cudaGetLastError(), "fused ftlm step");
 }
 
@@ -312,7 +358,7 @@ void fused_step(const qb_csr* A, std::uint64_t n, int k, int j, double tol, cons
 struct BlockBufs {
     DevBuf<double2> w;
     DevBuf<unsigned char> vb[2];
-    DevBuf<double> ovl, part, inv;
+    DevBuf<double> ovl, part, part2, inv;
     DevBuf<unsigned> cnt;
     void ensure(std::uint64_t n, int k, std::size_t es) {
         const std::size_t nk = static_cast<std::size_t>(n) * k;
@@ -321,8 +367,9 @@ struct BlockBufs {
             if (b.n < nk * es) b.alloc(nk * es);
         if (ovl.n == 0) ovl.alloc(2 * kMaxCols);
         if (part.n == 0) part.alloc(static_cast<std::size_t>(3) * kMaxCols * kMaxRedBlocks);
+        if (part2.n == 0) part2.alloc(static_cast<std::size_t>(3) * kMaxCols * kMaxGroups);
         if (inv.n == 0) inv.alloc(kMaxCols);
-        if (cnt.n == 0) cnt.alloc(1);
+        if (cnt.n == 0) cnt.alloc(1 + kMaxGroups);
     }
 };
 
@@ -341,8 +388,8 @@ void block_recurrence(const qb_sector* sec, const qb_program* prog, const qb_csr
     else
         cuda_check(cudaMemcpyAsync(B.vb[1].p, B.w.p, nk * 16, cudaMemcpyDeviceToDevice, st), "copy");
     cuda_check(cudaMemsetAsync(d_beta, 0, static_cast<std::size_t>(cap + 1) * k * 8, st), "zero");
-    cuda_check(cudaMemsetAsync(B.cnt.p, 0, 4, st), "zero");
-    BScal S{d_alpha, d_beta, B.ovl.p, B.part.p, B.cnt.p};
+    cuda_check(cudaMemsetAsync(B.cnt.p, 0, (1 + kMaxGroups) * 4, st), "zero");
+    BScal S{d_alpha, d_beta, B.ovl.p, B.part.p, B.cnt.p, B.part2.p, B.cnt.p + 1};
     int cur = 1;
     const int rb = static_cast<int>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 7) / 8, kBlockRecGrid)));
     const std::size_t bsm = static_cast<std::size_t>(3) * kMaxCols * 8 * sizeof(double);

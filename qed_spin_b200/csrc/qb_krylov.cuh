@@ -330,7 +330,10 @@ struct BScal {
     double* ovl;       // [2][k]
     double* partials;  // [3][k][kMaxRedBlocks]
     unsigned* counter;
+    double* partials2 = nullptr;          // [3][k][kMaxGroups]: the two-level sums' group totals
+    unsigned* group_counter = nullptr;    // [kMaxGroups]
 };
+constexpr int kMaxGroups = (kMaxRedBlocks + 31) / 32;
 
 template <int NQ, int CPL>
 __device__ __forceinline__ bool block_cols_total(double (&v)[NQ][CPL], int k, BScal S, double* sm /*[NQ][kMaxCols][8]*/,
