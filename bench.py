@@ -258,10 +258,12 @@ def main():
     ap.add_argument("--e0-6x6", action="store_true",
                     help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
                          "(FP64, and FP32 storage + FP64 refinement), one JSON line")
-    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36"], default=None,
-                    help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing")
-    ap.add_argument("--profile-lane", choices=["walk", "csr"], default="walk",
-                    help="the lane of the profiling run: the on-the-fly walk or the device reduced CSR")
+    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36", "ftlm4"], default=None,
+                    help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing; "
+                         "ftlm4: batched FTLM (40 samples, depth 100) on the four largest N = 24 XXZ blocks")
+    ap.add_argument("--profile-lane", choices=["walk", "csr", "c64", "c128"], default="walk",
+                    help="the lane of the profiling run: the on-the-fly walk or the device reduced CSR; for ftlm4 "
+                         "the storage type")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
@@ -768,6 +770,20 @@ def profile_case(args):
     from qed_spin_b200 import lattice as lat
     from qed_spin_b200 import operators as ops
     build.build()
+    if args.profile_case == "ftlm4":
+        N = FTLM_N
+        prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.5) + ops.zeeman_z_products(N, 0.1)
+        P = D.Program(ops.row_program(ops.from_products(N, prods)))
+        secs = [D.Sector(lat.chain_sector(N, n, k)) for n, k in [(12, 0), (11, 1), (13, 2), (12, 5)]]
+        betas = 1.0 / np.linspace(0.1, 4.0, 40)
+        dt = args.profile_lane if args.profile_lane in ("c64", "c128") else "c64"
+        D.ftlm_blocks(secs, P, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas, dtype=dt)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = D.ftlm_blocks(secs, P, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas, dtype=dt)
+        print(json.dumps({"profile_case": "ftlm4", "dtype": dt, "dims": [s.dim for s in secs],
+                          "s": time.perf_counter() - t, "phases": r["stats"]}))
+        return
     if args.profile_case == "chain32":
         spec, prog, _ = workload()
     else:
