@@ -809,7 +809,7 @@ def profile_case(args):
     torch.cuda.synchronize()
     print(json.dumps({"profile_case": args.profile_case, "lane": args.profile_lane, "dim": S.dim,
                       "ms_per_matvec": (time.perf_counter() - t) / args.steps * 1e3, "sector": S.info(),
-                      "csr": A.info() if A is not None else None}))
+                      "csr": A.info() if A is not None else None, "tuned_shapes": D.tune_entries()}))
 
 
 def emitted_per_row(reps: np.ndarray, prog) -> float:

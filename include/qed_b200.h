@@ -284,6 +284,31 @@ int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void*
                        int reorth, double breakdown_tol, int dtype, double* alpha, double* beta, int* iters,
                        void* stream);
 
+/* ---- launch-shape tuning ----------------------------------------------------------------------
+ * Kernel families with several launch shapes that give the same result bit for bit:
+ *   "walk"       the row walk (qb_matvec and the Krylov lanes on the walk): 0 one thread per state,
+ *                1 a warp's states compacted (every lane canonicalises a target while any row has one);
+ *   "walk_team"  the block walk of k interleaved vectors (qb_matvec_block, FTLM on the walk): 0, 1, 2, 3 =
+ *                8, 16, 32, 4 lanes per state (4 only when k <= 32).
+ * The first launch for a size class (the sector's group and lookup, the program's groups, the row count by
+ * powers of two, the vectors' number and types, the device) times every shape on the caller's stream (one
+ * warm-up and three timed runs each; this synchronises that stream once) and keeps the fastest. A stream
+ * that is capturing a graph is never timed. No reference counterpart: the reference fixes its launch shapes
+ * (src/gpu/rep_matvec.cu).
+ * mode: 1 measure on first use (the default; QB_TUNE overrides it at start), 2 only choices already known
+ * (this process, or a loaded file), else shape 0; 0 always shape 0; -1 only reads *previous.
+ * QB_TUNE_CACHE=path: choices are read from path at first use and each new one is appended to it. */
+int qb_tune_mode(int mode, int* previous);
+/* Forces candidate `choice` for every launch of a family (choice < 0 removes the force). */
+int qb_tune_force(const char* family, int choice);
+/* Forgets every known choice and every force. */
+int qb_tune_clear(void);
+/* Writes the known choices ("key<TAB>choice<TAB>ms per candidate" lines) to path; reads such a file. */
+int qb_tune_save(const char* path);
+int qb_tune_load(const char* path);
+/* The known choices as that text, NUL-terminated, in buf (len bytes); *needed: the bytes it takes. */
+int qb_tune_entries(char* buf, uint64_t len, uint64_t* needed);
+
 /* ---- the request server ---------------------------------------------------------------------
  * Eigs and T = 0 dynamics solves of sectors of different sizes served on one GPU with continuous
  * batching: requests queue in arrival order; a worker admits the head when one of max_active slots is

@@ -31,6 +31,7 @@ EXPORTS = [
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
     "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_sector_save",
     "qb_sector_load",
+    "qb_tune_mode", "qb_tune_force", "qb_tune_clear", "qb_tune_save", "qb_tune_load", "qb_tune_entries",
 ]
 
 
@@ -145,6 +146,12 @@ def lib():
     L.qb_thermal_combine.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]
     L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]
     L.qb_lanczos_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i), vp]
+    L.qb_tune_mode.argtypes = [i, C.POINTER(i)]
+    L.qb_tune_force.argtypes = [C.c_char_p, i]
+    L.qb_tune_clear.argtypes = []
+    L.qb_tune_save.argtypes = [C.c_char_p]
+    L.qb_tune_load.argtypes = [C.c_char_p]
+    L.qb_tune_entries.argtypes = [C.c_char_p, u64, C.POINTER(u64)]
     for name in EXPORTS:
         if name not in ("qb_last_error", "qb_sector_dim"):
             getattr(L, name).restype = i

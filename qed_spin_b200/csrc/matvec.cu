@@ -25,6 +25,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <string>
 
 #include "qb_walk.cuh"
 
@@ -81,11 +82,109 @@ __global__ void __launch_bounds__(256, 4) walk_rows(DSector row, DSector col, DP
     for (int v = 0; v < NV; ++v) So::store(static_cast<typename So::T*>(io.out[v]), r, acc[v]);
 }
 
-// Team kernel: kTeam lanes per row, kCpl columns per lane (k <= kTeam kCpl vectors).
-template <int kCpl, bool kF32, bool kOutF32, bool kSame>
+// Warp-compacted walk (the same y as walk_rows, bit for bit): a warp owns 32 consecutive rows. For each window
+// of 32 groups every lane builds its row's acting-group mask; a warp prefix sum lays the (row, group) pairs out
+// row-major, and the warp canonicalises them 32 at a time, one pair per lane, so no lane idles while another row
+// still has targets. Each pair's products c x_v[j] go to shared memory; the row's lane then adds its slots in
+// order -- the row's entries in group order, with walk_rows's operations.
+struct WarpSlots {
+    u64 state[32];
+    double w[32];
+    u32 mask[32], pre[32], incl[32];
+    int ok[32];
+};
+
+template <int NV, class ST, bool kInF32, bool kOutF32, bool kSame>
+__global__ void __launch_bounds__(256, 4) walk_warp(DSector row, DSector col, DProgram P, bool prog_in_smem,
+                                                    std::size_t stage_bytes, VecPtrs<NV> io) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using St = Store<kInF32>;
+    using So = Store<kOutF32>;
+    const SmemProgram sp = stage(P, col, smem, prog_in_smem);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpSlots& W = reinterpret_cast<WarpSlots*>(smem + stage_bytes)[wid];
+    double2* prod = reinterpret_cast<double2*>(smem + stage_bytes + (blockDim.x >> 5) * sizeof(WarpSlots)) +
+                    static_cast<std::size_t>(wid) * 32 * NV;
+    const std::uint64_t r0 = (static_cast<std::uint64_t>(blockIdx.x) * blockDim.x) + (threadIdx.x & ~31u);
+    const std::uint64_t r = r0 + lane;
+    const bool live = r < row.dim;
+    const ST s = live ? static_cast<ST>(__ldg(row.reps + r)) : static_cast<ST>(0);
+    const double w = live ? __ldg(row.inv_norms + r) : 0.0;
+    W.state[lane] = static_cast<u64>(s);
+    W.w[lane] = w;
+    cplx acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = {0.0, 0.0};
+    const u32 ng = sp.P.n_groups;
+    for (u32 g0 = 0; g0 < ng; g0 += 32) {
+        const u32 gend = ng < g0 + 32 ? ng : g0 + 32;
+        u32 mask = 0;
+        if (live)
+            for (u32 g = g0; g < gend; ++g)
+                if (acting_subgroup<ST>(sp.P, s, g) >= 0) mask |= 1u << (g - g0);
+        const u32 cnt = static_cast<u32>(__popc(mask));
+        u32 incl = cnt;   // inclusive prefix over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const u32 pre = incl - cnt;
+        const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+        W.mask[lane] = mask;
+        W.pre[lane] = pre;
+        W.incl[lane] = incl;
+        __syncwarp();
+        for (u32 b = 0; b < total; b += 32) {
+            const u32 q = b + lane;
+            int ok = 0;
+            if (q < total) {
+                // the owner: the number of rows whose pairs all come before q
+                int o = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (W.incl[o + step - 1] <= q) o += step;
+                const ST so = static_cast<ST>(W.state[o]);
+                const u32 g = g0 + __fns(W.mask[o], 0, static_cast<int>(q - W.pre[o]) + 1);
+                const int vi = acting_subgroup<ST>(sp.P, so, g);
+                const cplx h = subgroup_value<ST>(sp.P, so, vi);
+                const ST t = so ^ static_cast<ST>(sp.P.group_flip[g]);
+                long long j;
+                cplx c;
+                if (entry<kSame, ST>(col, sp.T, so, static_cast<long long>(r0 + o), W.w[o], t, h, j, c)) {
+                    ok = 1;
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) {
+                        const cplx p = cmul(c, St::load(static_cast<const typename St::T*>(io.in[v]),
+                                                        static_cast<std::size_t>(j)));
+                        prod[lane * NV + v] = make_double2(p.re, p.im);
+                    }
+                }
+            }
+            W.ok[lane] = ok;
+            __syncwarp();
+            const u32 lo = pre > b ? pre : b, hi = incl < b + 32 ? incl : b + 32;
+            for (u32 p = lo; p < hi; ++p) {
+                if (!W.ok[p - b]) continue;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const double2 d = prod[(p - b) * NV + v];
+                    acc[v] = cadd(acc[v], {d.x, d.y});
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) So::store(static_cast<typename So::T*>(io.out[v]), r, acc[v]);
+}
+
+// Team kernel: kTeam lanes per row (4, 8, 16 or 32), kCpl columns per lane (k <= kTeam kCpl vectors). Every column
+// adds its row's entries in group order whatever kTeam is, so the team size changes only the time.
+template <int kTeam, int kCpl, bool kF32, bool kOutF32, bool kSame>
 __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProgram P, bool prog_in_smem,
                                                  const void* in_v, void* out_v, int k) {
-    constexpr int kTeam = 8;
     extern __shared__ __align__(16) unsigned char smem[];
     using St = Store<kF32>;
     using So = Store<kOutF32>;
@@ -95,7 +194,7 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
     const SmemProgram sp = stage(P, col, smem, prog_in_smem);
     const int lane = threadIdx.x & 31;
     const int team = lane / kTeam, tl = lane % kTeam;
-    const unsigned team_mask = 0xFFu << (team * kTeam);
+    const unsigned team_mask = kTeam == 32 ? 0xffffffffu : ((1u << kTeam) - 1u) << (team * kTeam);
     const std::uint64_t warp = (static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const std::uint64_t r = warp * (32 / kTeam) + team;
     const bool live = r < row.dim;
@@ -132,22 +231,52 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
         if (c0 + c < k) So::store(out, static_cast<std::size_t>(r) * k + c0 + c, acc[c]);
 }
 
+// The size classes a launch shape is tuned for: the sector's group and lookup, the program's groups, the row
+// count (by powers of two) and the vectors' number and types.
+std::string walk_key(const qb_sector* row, const qb_sector* col, const qb_program* P, int nv, int st_bits, int in32,
+                     int out32) {
+    const DSector c = col->view();
+    int lg = 0;
+    while ((1ULL << lg) < row->dim) ++lg;
+    return "N" + std::to_string(c.N) + ".G" + std::to_string(c.G) + ".gk" + std::to_string(c.gkind) + ".slc" +
+           std::to_string(c.slc.on ? 1 : 0) + ".lk" + std::to_string(c.lookup) + ".ng" +
+           std::to_string(P->view.n_groups) + ".d" + std::to_string(lg) + ".nv" + std::to_string(nv) + ".st" +
+           std::to_string(st_bits) + "." + std::to_string(in32) + std::to_string(out32) +
+           (row == col ? ".same" : ".cross");
+}
+
+template <int NV, class ST, bool kF32, bool kOutF32, bool kSame>
+void launch_rows_shape(int shape, const qb_sector* row, const qb_sector* col, const qb_program* P,
+                       const VecPtrs<NV>& io, cudaStream_t st) {
+    bool in_smem = false;
+    const std::size_t stage = (smem_for(P, col, in_smem) + 15) & ~std::size_t(15);
+    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
+    if (shape == 0) {
+        auto k = walk_rows<NV, ST, kF32, kOutF32, kSame>;
+        set_smem(k, stage);
+        k<<<blocks, 256, stage, st>>>(row->view(), col->view(), P->view, in_smem, io);
+    } else {
+        auto k = walk_warp<NV, ST, kF32, kOutF32, kSame>;
+        const std::size_t smem = stage + 8 * (sizeof(WarpSlots) + 32 * NV * sizeof(double2));
+        set_smem(k, smem);
+        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, stage, io);
+    }
+    cuda_check(cudaGetLastError(), "walk launch");
+}
+
+// The row walk over NV vectors: one thread per state (walk_rows) or a warp's states compacted (walk_warp), as
+// the tuner picks; the two give the same y bit for bit.
 template <int NV, class ST, bool kF32, bool kOutF32>
 void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
                     cudaStream_t st) {
-    bool in_smem = false;
-    const std::size_t smem = smem_for(P, col, in_smem);
-    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
-    if (row == col) {
-        auto k = walk_rows<NV, ST, kF32, kOutF32, true>;
-        set_smem(k, smem);
-        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
-    } else {
-        auto k = walk_rows<NV, ST, kF32, kOutF32, false>;
-        set_smem(k, smem);
-        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, io);
-    }
-    cuda_check(cudaGetLastError(), "walk_rows launch");
+    auto run = [&](int shape) {
+        if (row == col)
+            launch_rows_shape<NV, ST, kF32, kOutF32, true>(shape, row, col, P, io, st);
+        else
+            launch_rows_shape<NV, ST, kF32, kOutF32, false>(shape, row, col, P, io, st);
+    };
+    const int shape = tune_choose("walk", walk_key(row, col, P, NV, sizeof(ST) * 8, kF32, kOutF32), 2, 0, st, run);
+    run(shape);
 }
 
 template <int NV, bool kF32, bool kOutF32 = kF32>
@@ -165,41 +294,63 @@ void launch_rows_nv(const qb_sector* row, const qb_sector* col, const qb_program
         launch_rows_st<NV, u64, kF32, kOutF32>(row, col, P, io, st);
 }
 
-template <int kCpl, bool kF32, bool kOutF32>
+template <int kTeam, int kCpl, bool kF32, bool kOutF32>
 void launch_team_c(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* in, void* out, int k,
                    cudaStream_t st) {
     bool in_smem = false;
     const std::size_t smem = smem_for(P, col, in_smem);
-    const std::uint64_t warps = (row->dim + 3) / 4;
+    constexpr int kRowsPerWarp = 32 / kTeam;
+    const std::uint64_t warps = (row->dim + kRowsPerWarp - 1) / kRowsPerWarp;
     const unsigned blocks = static_cast<unsigned>((warps * 32 + 255) / 256);
     if (row == col) {
-        auto kk = walk_team<kCpl, kF32, kOutF32, true>;
+        auto kk = walk_team<kTeam, kCpl, kF32, kOutF32, true>;
         set_smem(kk, smem);
         kk<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, in, out, k);
     } else {
-        auto kk = walk_team<kCpl, kF32, kOutF32, false>;
+        auto kk = walk_team<kTeam, kCpl, kF32, kOutF32, false>;
         set_smem(kk, smem);
         kk<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, in, out, k);
     }
     cuda_check(cudaGetLastError(), "walk_team launch");
 }
 
+template <int kTeam, bool kF32, bool kOutF32>
+void launch_team_t(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* in, void* out, int k,
+                   cudaStream_t st) {
+    const int cpl = (k + kTeam - 1) / kTeam;
+    if (cpl <= 1)
+        launch_team_c<kTeam, 1, kF32, kOutF32>(row, col, P, in, out, k, st);
+    else if (cpl <= 2)
+        launch_team_c<kTeam, 2, kF32, kOutF32>(row, col, P, in, out, k, st);
+    else if (cpl <= 4)
+        launch_team_c<kTeam, 4, kF32, kOutF32>(row, col, P, in, out, k, st);
+    else if (cpl <= 5)
+        launch_team_c<kTeam, 5, kF32, kOutF32>(row, col, P, in, out, k, st);
+    else if (cpl <= 8)
+        launch_team_c<kTeam, 8, kF32, kOutF32>(row, col, P, in, out, k, st);
+    else
+        throw Error(QB_EUNSUPPORTED, "block matvec: at most 64 vectors");
+}
+
+// The block walk of k interleaved vectors with 8, 16, 32 or (k <= 32) 4 lanes per state, as the tuner picks (the
+// same y bit for bit).
 template <bool kF32, bool kOutF32>
 void launch_team(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* in, void* out, int k,
                  cudaStream_t st) {
-    const int cpl = (k + 7) / 8;
-    if (cpl <= 1)
-        launch_team_c<1, kF32, kOutF32>(row, col, P, in, out, k, st);
-    else if (cpl <= 2)
-        launch_team_c<2, kF32, kOutF32>(row, col, P, in, out, k, st);
-    else if (cpl <= 4)
-        launch_team_c<4, kF32, kOutF32>(row, col, P, in, out, k, st);
-    else if (cpl <= 5)
-        launch_team_c<5, kF32, kOutF32>(row, col, P, in, out, k, st);
-    else if (cpl <= 8)
-        launch_team_c<8, kF32, kOutF32>(row, col, P, in, out, k, st);
-    else
-        throw Error(QB_EUNSUPPORTED, "block matvec: at most 64 vectors");
+    if (k > 64) throw Error(QB_EUNSUPPORTED, "block matvec: at most 64 vectors");
+    auto run = [&](int shape) {
+        if (shape == 0)
+            launch_team_t<8, kF32, kOutF32>(row, col, P, in, out, k, st);
+        else if (shape == 1)
+            launch_team_t<16, kF32, kOutF32>(row, col, P, in, out, k, st);
+        else if (shape == 2)
+            launch_team_t<32, kF32, kOutF32>(row, col, P, in, out, k, st);
+        else
+            launch_team_t<4, kF32, kOutF32>(row, col, P, in, out, k, st);
+    };
+    const int shapes = k <= 32 ? 4 : 3;
+    const int shape = tune_choose("walk_team", walk_key(row, col, P, k, 64, kF32, kOutF32), shapes, 0, st, run);
+    run(shape);
 }
 
 void check_pair(const qb_sector* row, const qb_sector* col, const qb_program* P) {

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -47,6 +48,12 @@ void set_last_error(const std::string& m);
 // the footprint it admitted the request with; 0: none).
 std::size_t available_bytes();
 void set_thread_allowance(std::size_t bytes);
+
+// The launch shape of a kernel family for a size-class key (tune.cu): a forced or known choice, or -- when
+// measuring and st is not capturing -- the fastest of n candidates, each run by run(c) on st; else fallback.
+// The candidates must give the same result bit for bit.
+int tune_choose(const char* family, const std::string& key, int n, int fallback, cudaStream_t st,
+                const std::function<void(int)>& run);
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;

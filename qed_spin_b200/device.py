@@ -471,3 +471,44 @@ def registry_stats() -> dict:
     a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
     check(lib().qb_registry_stats(C.byref(a), C.byref(b), C.byref(c)))
     return {"sectors": a.value, "idle_sectors": b.value, "idle_bytes": c.value}
+
+
+# ---- launch-shape tuning ----
+
+def tune_mode(mode: int = -1) -> int:
+    """Sets the tuner's mode (1 measure on first use, 2 known choices only, 0 defaults; -1 leaves it) and
+    returns the previous one."""
+    prev = C.c_int(0)
+    check(lib().qb_tune_mode(int(mode), C.byref(prev)))
+    return prev.value
+
+
+def tune_force(family: str, choice: int) -> None:
+    """Forces launch shape `choice` for a kernel family ("walk", "walk_team"); a negative choice removes it."""
+    check(lib().qb_tune_force(family.encode(), int(choice)))
+
+
+def tune_clear() -> None:
+    check(lib().qb_tune_clear())
+
+
+def tune_save(path: str) -> None:
+    check(lib().qb_tune_save(str(path).encode()))
+
+
+def tune_load(path: str) -> None:
+    check(lib().qb_tune_load(str(path).encode()))
+
+
+def tune_entries() -> dict:
+    """The known choices: key -> (choice, [ms per candidate])."""
+    need = C.c_uint64(0)
+    check(lib().qb_tune_entries(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(int(need.value) + 1)
+    check(lib().qb_tune_entries(buf, len(buf), C.byref(need)))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        parts = line.split("\t")
+        if len(parts) >= 2:
+            out[parts[0]] = (int(parts[1]), [float(x) for x in parts[2:]])
+    return out
