@@ -588,6 +588,41 @@ def levels_measure(S, P, args):
                 out["chain20_k4"]["max_abs_diff"] = float(np.max(np.abs(np.array(ev) - r4["values"])))
         except Exception as e:
             out["chain20_k4"]["reference_unavailable"] = str(e)
+    out["graphs_chain20"] = graphs_measure(S20, P20)
+    return out
+
+
+def graphs_measure(S, P):
+    """The lanes that batch their steps into captured CUDA graphs on a small sector (chain-20, 9,252 states),
+    with graphs and launched step by step (QB_GRAPHS=0): the k = 1 lane, the certified ground-state vector and a
+    200-step continued fraction. Median seconds of 5 calls each after a warm-up call."""
+    from qed_spin_b200 import device as D
+    rng = np.random.default_rng(1)
+    phi = rng.standard_normal(S.dim) + 1j * rng.standard_normal(S.dim)
+    omega = np.linspace(-0.5, 6.0, 400)
+    calls = {"k1_lane": lambda: D.eigs_lowest(S, P),
+             "ground_state_vector": lambda: D.ground_state(S, P),
+             "continued_fraction_200": lambda: D.cf(S, P, phi, 200, omega, 0.05)}
+    out = {}
+    saved = os.environ.get("QB_GRAPHS")
+    try:
+        for flag, key in (("1", "graphs_s"), ("0", "step_by_step_s")):
+            os.environ["QB_GRAPHS"] = flag
+            for name, fn in calls.items():
+                fn()
+                ts = []
+                for _ in range(5):
+                    t = time.perf_counter()
+                    fn()
+                    ts.append(time.perf_counter() - t)
+                out.setdefault(name, {})[key] = float(np.median(ts))
+    finally:
+        if saved is None:
+            os.environ.pop("QB_GRAPHS", None)
+        else:
+            os.environ["QB_GRAPHS"] = saved
+    for v in out.values():
+        v["speedup"] = v["step_by_step_s"] / v["graphs_s"]
     return out
 
 

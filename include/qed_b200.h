@@ -288,6 +288,7 @@ int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void*
  * Kernel families with several launch shapes that give the same result bit for bit:
  *   "walk"       the row walk (qb_matvec and the Krylov lanes on the walk): 0 one thread per state,
  *                1 a warp's states compacted (every lane canonicalises a target while any row has one);
+ *                for one vector also 2, 3, 4, 5 = a team of 8, 16, 32, 4 lanes per state;
  *   "walk_team"  the block walk of k interleaved vectors (qb_matvec_block, FTLM on the walk): 0, 1, 2, 3 =
  *                8, 16, 32, 4 lanes per state (4 only when k <= 32).
  * The first launch for a size class (the sector's group and lookup, the program's groups, the row count by

@@ -209,25 +209,48 @@ GsOut gs_vector(const qb_sector* sec, const qb_program* prog, double2* u, int ma
             R.start_from_device(seed.p);
             if (keep) R.keep_current();
             double sc = 0.0;   // largest |alpha| or beta so far
-            while (m < cap) {
-                if (keep && m > 0) R.keep_current();
-                R.step(m, QB_REORTH_NONE);
-                double a, b;
-                R.read_scalars(m, a, b);
+            // one step's test: false once the run is done
+            auto more = [&](double a, double b) {
                 alpha.push_back(a);
                 beta.push_back(b);
                 ++m;
                 sc = std::max(sc, std::abs(a));
-                if (!(b > 1e-12 * sc)) break;   // an invariant subspace: its tridiagonal is exact
+                if (!(b > 1e-12 * sc)) return false;   // an invariant subspace: its tridiagonal is exact
                 sc = std::max(sc, b);
                 if (m >= 3) {
                     const Ends t = tridiag_ends(alpha, beta, m, 1);
                     const double ts = std::max({std::abs(t.values[0]), std::abs(t.top), 1e-300});
-                    if (beta[m] * std::abs(t.zlast[0]) < 1e-9 * ts) break;
+                    if (beta[m] * std::abs(t.zlast[0]) < 1e-9 * ts) return false;
+                }
+                return true;
+            };
+            int launched = 0;
+            const int batch = graph_batch(n, true);
+            if (batch > 0) {
+                // graphs of `batch` steps; the tests run on each batch's scalars (up to batch - 1 steps past the end)
+                std::vector<double> ab(batch), bb(batch);
+                bool go = true;
+                while (go && m < cap) {
+                    const int cnt = std::min(batch, cap - m);
+                    const int j0 = m;
+                    R.advance(cnt, keep, QB_REORTH_NONE, batch);
+                    launched += cnt;
+                    R.read_range(j0, cnt, ab.data(), bb.data());
+                    for (int i = 0; i < cnt && go; ++i) go = more(ab[i], bb[i]);
+                }
+                if (keep && static_cast<int>(R.basis.size()) > m) R.basis.resize(m);
+            } else {
+                while (m < cap) {
+                    if (keep && m > 0) R.keep_current();
+                    R.step(m, QB_REORTH_NONE);
+                    ++launched;
+                    double a, b;
+                    R.read_scalars(m, a, b);
+                    if (!more(a, b)) break;
                 }
             }
-            out.matvecs += m;
-            left -= m;
+            out.matvecs += launched;
+            left -= launched;
             std::vector<double> e(std::max(1, m - 1));
             for (int i = 0; i + 1 < m; ++i) e[i] = beta[i + 1];
             double lo, hi;

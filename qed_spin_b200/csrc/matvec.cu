@@ -231,69 +231,6 @@ __global__ void __launch_bounds__(256) walk_team(DSector row, DSector col, DProg
         if (c0 + c < k) So::store(out, static_cast<std::size_t>(r) * k + c0 + c, acc[c]);
 }
 
-// The size classes a launch shape is tuned for: the sector's group and lookup, the program's groups, the row
-// count (by powers of two) and the vectors' number and types.
-std::string walk_key(const qb_sector* row, const qb_sector* col, const qb_program* P, int nv, int st_bits, int in32,
-                     int out32) {
-    const DSector c = col->view();
-    int lg = 0;
-    while ((1ULL << lg) < row->dim) ++lg;
-    return "N" + std::to_string(c.N) + ".G" + std::to_string(c.G) + ".gk" + std::to_string(c.gkind) + ".slc" +
-           std::to_string(c.slc.on ? 1 : 0) + ".lk" + std::to_string(c.lookup) + ".ng" +
-           std::to_string(P->view.n_groups) + ".d" + std::to_string(lg) + ".nv" + std::to_string(nv) + ".st" +
-           std::to_string(st_bits) + "." + std::to_string(in32) + std::to_string(out32) +
-           (row == col ? ".same" : ".cross");
-}
-
-template <int NV, class ST, bool kF32, bool kOutF32, bool kSame>
-void launch_rows_shape(int shape, const qb_sector* row, const qb_sector* col, const qb_program* P,
-                       const VecPtrs<NV>& io, cudaStream_t st) {
-    bool in_smem = false;
-    const std::size_t stage = (smem_for(P, col, in_smem) + 15) & ~std::size_t(15);
-    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
-    if (shape == 0) {
-        auto k = walk_rows<NV, ST, kF32, kOutF32, kSame>;
-        set_smem(k, stage);
-        k<<<blocks, 256, stage, st>>>(row->view(), col->view(), P->view, in_smem, io);
-    } else {
-        auto k = walk_warp<NV, ST, kF32, kOutF32, kSame>;
-        const std::size_t smem = stage + 8 * (sizeof(WarpSlots) + 32 * NV * sizeof(double2));
-        set_smem(k, smem);
-        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, stage, io);
-    }
-    cuda_check(cudaGetLastError(), "walk launch");
-}
-
-// The row walk over NV vectors: one thread per state (walk_rows) or a warp's states compacted (walk_warp), as
-// the tuner picks; the two give the same y bit for bit.
-template <int NV, class ST, bool kF32, bool kOutF32>
-void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
-                    cudaStream_t st) {
-    auto run = [&](int shape) {
-        if (row == col)
-            launch_rows_shape<NV, ST, kF32, kOutF32, true>(shape, row, col, P, io, st);
-        else
-            launch_rows_shape<NV, ST, kF32, kOutF32, false>(shape, row, col, P, io, st);
-    };
-    const int shape = tune_choose("walk", walk_key(row, col, P, NV, sizeof(ST) * 8, kF32, kOutF32), 2, 0, st, run);
-    run(shape);
-}
-
-template <int NV, bool kF32, bool kOutF32 = kF32>
-void launch_rows_nv(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* const* ins,
-                    void* const* outs, cudaStream_t st) {
-    VecPtrs<NV> io;
-    for (int v = 0; v < NV; ++v) {
-        io.in[v] = ins[v];
-        io.out[v] = outs[v];
-    }
-    // 32-bit states when every state fits
-    if (row->N <= 32 && col->N <= 32)
-        launch_rows_st<NV, u32, kF32, kOutF32>(row, col, P, io, st);
-    else
-        launch_rows_st<NV, u64, kF32, kOutF32>(row, col, P, io, st);
-}
-
 template <int kTeam, int kCpl, bool kF32, bool kOutF32>
 void launch_team_c(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* in, void* out, int k,
                    cudaStream_t st) {
@@ -330,6 +267,84 @@ void launch_team_t(const qb_sector* row, const qb_sector* col, const qb_program*
         launch_team_c<kTeam, 8, kF32, kOutF32>(row, col, P, in, out, k, st);
     else
         throw Error(QB_EUNSUPPORTED, "block matvec: at most 64 vectors");
+}
+
+// The size classes a launch shape is tuned for: the sector's group and lookup, the program's groups, the row
+// count (by powers of two) and the vectors' number and types.
+std::string walk_key(const qb_sector* row, const qb_sector* col, const qb_program* P, int nv, int st_bits, int in32,
+                     int out32) {
+    const DSector c = col->view();
+    int lg = 0;
+    while ((1ULL << lg) < row->dim) ++lg;
+    return "N" + std::to_string(c.N) + ".G" + std::to_string(c.G) + ".gk" + std::to_string(c.gkind) + ".slc" +
+           std::to_string(c.slc.on ? 1 : 0) + ".lk" + std::to_string(c.lookup) + ".ng" +
+           std::to_string(P->view.n_groups) + ".d" + std::to_string(lg) + ".nv" + std::to_string(nv) + ".st" +
+           std::to_string(st_bits) + "." + std::to_string(in32) + std::to_string(out32) +
+           (row == col ? ".same" : ".cross");
+}
+
+template <int NV, class ST, bool kF32, bool kOutF32, bool kSame>
+void launch_rows_shape(int shape, const qb_sector* row, const qb_sector* col, const qb_program* P,
+                       const VecPtrs<NV>& io, cudaStream_t st) {
+    bool in_smem = false;
+    const std::size_t stage = (smem_for(P, col, in_smem) + 15) & ~std::size_t(15);
+    const unsigned blocks = static_cast<unsigned>((row->dim + 255) / 256);
+    if (shape == 0) {
+        auto k = walk_rows<NV, ST, kF32, kOutF32, kSame>;
+        set_smem(k, stage);
+        k<<<blocks, 256, stage, st>>>(row->view(), col->view(), P->view, in_smem, io);
+    } else {
+        auto k = walk_warp<NV, ST, kF32, kOutF32, kSame>;
+        const std::size_t smem = stage + 8 * (sizeof(WarpSlots) + 32 * NV * sizeof(double2));
+        set_smem(k, smem);
+        k<<<blocks, 256, smem, st>>>(row->view(), col->view(), P->view, in_smem, stage, io);
+    }
+    cuda_check(cudaGetLastError(), "walk launch");
+}
+
+// The row walk over NV vectors, as the tuner picks: one thread per state (walk_rows), a warp's states compacted
+// (walk_warp), or -- one vector -- a team of 8, 16, 32 or 4 lanes per state (walk_team at k = 1). All give the
+// same y bit for bit: each row adds c x_j in group order with the same operations.
+template <int NV, class ST, bool kF32, bool kOutF32>
+void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program* P, const VecPtrs<NV>& io,
+                    cudaStream_t st) {
+    auto run = [&](int shape) {
+        if (shape >= 2) {
+            const void* in = io.in[0];
+            void* out = io.out[0];
+            if (shape == 2)
+                launch_team_t<8, kF32, kOutF32>(row, col, P, in, out, 1, st);
+            else if (shape == 3)
+                launch_team_t<16, kF32, kOutF32>(row, col, P, in, out, 1, st);
+            else if (shape == 4)
+                launch_team_t<32, kF32, kOutF32>(row, col, P, in, out, 1, st);
+            else
+                launch_team_t<4, kF32, kOutF32>(row, col, P, in, out, 1, st);
+        } else if (row == col) {
+            launch_rows_shape<NV, ST, kF32, kOutF32, true>(shape, row, col, P, io, st);
+        } else {
+            launch_rows_shape<NV, ST, kF32, kOutF32, false>(shape, row, col, P, io, st);
+        }
+    };
+    const int shapes = NV == 1 ? 6 : 2;
+    const int shape =
+        tune_choose("walk", walk_key(row, col, P, NV, sizeof(ST) * 8, kF32, kOutF32), shapes, 0, st, run);
+    run(shape);
+}
+
+template <int NV, bool kF32, bool kOutF32 = kF32>
+void launch_rows_nv(const qb_sector* row, const qb_sector* col, const qb_program* P, const void* const* ins,
+                    void* const* outs, cudaStream_t st) {
+    VecPtrs<NV> io;
+    for (int v = 0; v < NV; ++v) {
+        io.in[v] = ins[v];
+        io.out[v] = outs[v];
+    }
+    // 32-bit states when every state fits
+    if (row->N <= 32 && col->N <= 32)
+        launch_rows_st<NV, u32, kF32, kOutF32>(row, col, P, io, st);
+    else
+        launch_rows_st<NV, u64, kF32, kOutF32>(row, col, P, io, st);
 }
 
 // The block walk of k interleaved vectors with 8, 16, 32 or (k <= 32) 4 lanes per state, as the tuner picks (the

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <complex>
 #include <cstring>
 #include <limits>
@@ -137,7 +138,7 @@ template <class T> __global__ void k_scale_into(std::uint64_t n, const double2* 
 
 // alpha_j = Re <v_j, w - beta_j v_{j-1}>, w updated in place (axpy_dot, cpu_backend.h:174-191).
 template <class T>
-__global__ void rec_alpha(std::uint64_t n, int j, double2* w, const T* vp, const T* vc, Scal S) {
+__device__ __forceinline__ void rec_alpha_body(std::uint64_t n, int j, double2* w, const T* vp, const T* vc, Scal S) {
     __shared__ double sm[4 * 32];
     const double b = j > 0 ? S.beta[j] : 0.0;
     double v[1] = {0.0};
@@ -157,10 +158,14 @@ __global__ void rec_alpha(std::uint64_t n, int j, double2* w, const T* vp, const
     double tot[1];
     if (last_block_total<1>(v, S.partials, S.counter, sm, tot)) S.alpha[j] = tot[0];
 }
+template <class T>
+__global__ void rec_alpha(std::uint64_t n, int j, double2* w, const T* vp, const T* vc, Scal S) {
+    rec_alpha_body<T>(n, j, w, vp, vc, S);
+}
 
 // w -= alpha_j v_j; ||w||^2 and <v_j, w> -> beta_{j+1} and the deferred local projection.
 template <class T>
-__global__ void rec_beta(std::uint64_t n, int j, int local, double2* w, const T* vc, Scal S) {
+__device__ __forceinline__ void rec_beta_body(std::uint64_t n, int j, int local, double2* w, const T* vc, Scal S) {
     __shared__ double sm[4 * 32];
     const double a = S.alpha[j];
     double v[3] = {0.0, 0.0, 0.0};
@@ -187,9 +192,14 @@ __global__ void rec_beta(std::uint64_t n, int j, int local, double2* w, const T*
         S.beta[j + 1] = sqrt(nrm2);
     }
 }
+template <class T>
+__global__ void rec_beta(std::uint64_t n, int j, int local, double2* w, const T* vc, Scal S) {
+    rec_beta_body<T>(n, j, local, w, vc, S);
+}
 
 // v_{j+1} = (w + o v_j) / beta_{j+1}, written over v_{j-1}'s buffer.
-template <class T> __global__ void rec_next(std::uint64_t n, int j, const double2* w, const T* vc, T* vn, Scal S) {
+template <class T>
+__device__ __forceinline__ void rec_next_body(std::uint64_t n, int j, const double2* w, const T* vc, T* vn, Scal S) {
     const double b = S.beta[j + 1];
     const double inv = b > 0.0 ? 1.0 / b : 0.0;
     const double ore = S.ovl[0], oim = S.ovl[1];
@@ -203,6 +213,40 @@ template <class T> __global__ void rec_next(std::uint64_t n, int j, const double
         }
         V<T>::st(vn, i, y.x * inv, y.y * inv);
     }
+}
+template <class T> __global__ void rec_next(std::uint64_t n, int j, const double2* w, const T* vc, T* vn, Scal S) {
+    rec_next_body<T>(n, j, w, vc, vn, S);
+}
+
+// The same three passes with the step index in device memory (*dj), so that a captured graph of steps replays
+// unchanged: rec_next_dev advances *dj once every block has read it. k_keep_dev copies v_j into basis slot j.
+template <class T>
+__global__ void rec_alpha_dev(std::uint64_t n, const int* dj, double2* w, const T* vp, const T* vc, Scal S) {
+    rec_alpha_body<T>(n, *dj, w, vp, vc, S);
+}
+template <class T>
+__global__ void rec_beta_dev(std::uint64_t n, const int* dj, int local, double2* w, const T* vc, Scal S) {
+    rec_beta_body<T>(n, *dj, local, w, vc, S);
+}
+template <class T> __global__ void rec_next_dev(std::uint64_t n, int* dj, const double2* w, const T* vc, T* vn, Scal S) {
+    const int j = *dj;
+    rec_next_body<T>(n, j, w, vc, vn, S);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(S.counter, 1u) == gridDim.x - 1) {
+            *dj = j + 1;
+            *S.counter = 0;
+        }
+    }
+}
+__global__ void k_keep_dev(std::uint64_t bytes, const int* dj, const unsigned char* v, unsigned char* basis) {
+    const std::uint64_t words = bytes / 8;   // a vector is n elements of 8 or 16 bytes
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(v);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(basis + static_cast<std::uint64_t>(*dj) * bytes);
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < words;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x)
+        dst[i] = src[i];
 }
 
 // ---- full reorthogonalisation (CGS2 with the DGKS gate, lanczos.h:428-451) against the kept basis ----
@@ -756,8 +800,16 @@ struct Recurrence {
     DevBuf<double2> d_coeff, d_part;
     DevBuf<double> d_norms;                     // [0] before, [1] after
     DevBuf<int> d_flag;
+    DevBuf<int> d_j;                            // the step index of the graph-ready steps
     cudaEvent_t ev = nullptr;
     int cur = 1;   // vbuf[cur] = v_j, vbuf[cur ^ 1] = v_{j-1}
+    int host_j = 0;   // steps taken by advance()
+    // captured batches of steps, by (steps, keep, reorth)
+    struct Batch {
+        int steps, keep, reorth;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Batch> graphs;
 
     std::size_t esize() const { return dtype == QB_C64 ? 8 : 16; }
     Scal scal() { return Scal{d_alpha.p, d_beta.p, d_ovl.p, d_partials.p, d_counter.p}; }
@@ -774,10 +826,13 @@ struct Recurrence {
         d_partials.alloc(4 * kMaxRedBlocks);
         d_counter.alloc(1);
         cuda_check(cudaMemset(d_counter.p, 0, 4), "zero");
+        d_j.alloc(1);
+        cuda_check(cudaMemset(d_j.p, 0, 4), "zero");
         cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
     }
     ~Recurrence() {
         if (ev) cudaEventDestroy(ev);
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     }
 
     // v_0 = x / ||x|| from a device FP64 vector (x is overwritten scratch when x == w).
@@ -869,6 +924,100 @@ struct Recurrence {
         cuda_check(cudaEventRecord(ev, st), "event");
     }
 
+    // ---- graph-ready steps: the step index lives in d_j ----
+    // One step j = host_j (reorth NONE or LOCAL): keep v_j in basis slot j when asked, then the walk and the three
+    // passes reading j from d_j.
+    void step_dev(bool keep, int reorth) {
+        const int nb = red_blocks(n);
+        void* vc = vbuf[cur].p;
+        void* vp = vbuf[cur ^ 1].p;
+        const int local = reorth == QB_REORTH_LOCAL;
+        if (keep)
+            k_keep_dev<<<nb, kThreads, 0, st>>>(n * esize(), d_j.p, static_cast<const unsigned char*>(vc),
+                                                basis_block.p);
+        launch_walk_mixed(sec, sec, prog, vc, w.p, dtype, QB_C128, st);
+        if (dtype == QB_C64) {
+            rec_alpha_dev<float2><<<nb, kThreads, 0, st>>>(n, d_j.p, w.p, static_cast<float2*>(vp), static_cast<float2*>(vc), scal());
+            rec_beta_dev<float2><<<nb, kThreads, 0, st>>>(n, d_j.p, local, w.p, static_cast<float2*>(vc), scal());
+            rec_next_dev<float2><<<nb, kThreads, 0, st>>>(n, d_j.p, w.p, static_cast<float2*>(vc), static_cast<float2*>(vp), scal());
+        } else {
+            rec_alpha_dev<double2><<<nb, kThreads, 0, st>>>(n, d_j.p, w.p, static_cast<double2*>(vp), static_cast<double2*>(vc), scal());
+            rec_beta_dev<double2><<<nb, kThreads, 0, st>>>(n, d_j.p, local, w.p, static_cast<double2*>(vc), scal());
+            rec_next_dev<double2><<<nb, kThreads, 0, st>>>(n, d_j.p, w.p, static_cast<double2*>(vc), static_cast<double2*>(vp), scal());
+        }
+        cuda_check(cudaGetLastError(), "recurrence");
+        cur ^= 1;
+    }
+
+    // `count` more steps from host_j, in captured batches of `batch` steps (an even number, so the two working
+    // vectors are back in place after each) while whole batches fit, the rest one launch sequence at a time.
+    // keep: v_j goes to basis slot j (slot 0 must be kept before the first step). The same kernels in the same
+    // order as step(), so the same scalars and vectors bit for bit.
+    void advance(int count, bool keep, int reorth, int batch) {
+        if (keep && basis_block.n == 0) basis_block.alloc(static_cast<std::size_t>(max_iter + 1) * n * esize());
+        int done = 0;
+        while (done < count) {
+            if (batch >= 2 && batch % 2 == 0 && count - done >= batch) {
+                launch_batch(batch, keep, reorth);
+                done += batch;
+            } else {
+                step_dev(keep, reorth);
+                ++done;
+            }
+        }
+        if (keep)
+            for (int j = host_j; j < host_j + count; ++j)
+                if (j > 0) basis.push_back(basis_block.p + static_cast<std::size_t>(j) * n * esize());
+        host_j += count;
+    }
+
+    void launch_batch(int steps, bool keep, int reorth) {
+        cudaGraphExec_t exec = nullptr;
+        for (const auto& g : graphs)
+            if (g.steps == steps && g.keep == keep && g.reorth == reorth) exec = g.exec;
+        if (!exec) {
+            // one matvec into the scratch w first (the captured steps overwrite it), so that the walk's launch
+            // shape is tuned before the capture records it
+            launch_walk_mixed(sec, sec, prog, vbuf[cur].p, w.p, dtype, QB_C128, st);
+            // captured on a private stream (nothing runs there), launched on st
+            cudaStream_t cs = nullptr, saved = st;
+            cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+            cudaGraph_t graph = nullptr;
+            const int cur0 = cur;
+            st = cs;
+            cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                try {
+                    for (int i = 0; i < steps; ++i) step_dev(keep, reorth);
+                } catch (...) {
+                    cudaStreamEndCapture(cs, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    st = saved;
+                    cur = cur0;
+                    cudaStreamDestroy(cs);
+                    throw;
+                }
+                e = cudaStreamEndCapture(cs, &graph);
+            }
+            st = saved;
+            cur = cur0;
+            cudaStreamDestroy(cs);
+            cuda_check(e, "step graph capture");
+            e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            cuda_check(e, "step graph instantiate");
+            graphs.push_back(Batch{steps, keep ? 1 : 0, reorth, exec});
+        }
+        cuda_check(cudaGraphLaunch(exec, st), "step graph launch");
+    }
+
+    // alpha_j0 .. alpha_{j0+cnt-1} and beta_{j0+1} .. beta_{j0+cnt} in one read.
+    void read_range(int j0, int cnt, double* a, double* b) {
+        cuda_check(cudaMemcpyAsync(a, d_alpha.p + j0, cnt * 8, cudaMemcpyDeviceToHost, st), "alpha read");
+        cuda_check(cudaMemcpyAsync(b, d_beta.p + j0 + 1, cnt * 8, cudaMemcpyDeviceToHost, st), "beta read");
+        cuda_check(cudaStreamSynchronize(st), "scalars");
+    }
+
     void read_scalars(int j, double& a, double& b) {
         double ab[2];
         cuda_check(cudaMemcpyAsync(&ab[0], d_alpha.p + j, 8, cudaMemcpyDeviceToHost, st), "alpha read");
@@ -898,12 +1047,59 @@ struct ScanOut {
     int matvecs = 0;
 };
 
+// Steps per captured graph for a sector of n states (0: launch step by step). Up to 2^20 states a step is a
+// few short launches and the host's read of its scalars, so graphs of steps pay; a gated scan (one that tests
+// convergence between steps) reads its scalars once per 8 steps and may run up to 7 steps past its stopping
+// point, a cost that grows with the step time. QB_GRAPHS=0 turns graphs off.
+constexpr std::uint64_t kGraphMaxDim = 1ULL << 20;
+inline int graph_batch(std::uint64_t n, bool gated) {
+    const char* e = std::getenv("QB_GRAPHS");
+    if ((e && *e == '0') || n > kGraphMaxDim) return 0;
+    return gated ? 8 : 16;
+}
+
 ScanOut run_scan(Recurrence& R, int max_iter, int reorth, bool gate, double breakdown_tol, bool keep) {
     ScanOut o;
     o.beta.push_back(0.0);
     const int cap = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(max_iter), R.n));
     if (reorth == QB_REORTH_FULL) keep = true;
     if (keep) R.keep_current();
+    const int batch = reorth == QB_REORTH_FULL ? 0 : graph_batch(R.n, gate);
+    if (batch > 0) {
+        // graphs of `batch` steps; the scalars read once per batch (ungated: once)
+        auto check = [&](int j) -> bool {
+            const int m_all = j + 1;
+            if (!gate) return false;
+            const int m = leading_block(o.alpha, o.beta, m_all);
+            if (m == m_all && m_all < 3) return false;
+            return lowest_level(o.alpha, o.beta, m, nullptr);
+        };
+        std::vector<double> a, b;
+        bool stop = false;
+        int j = 0;
+        while (j < cap && !stop) {
+            const int cnt = gate ? std::min(batch, cap - j) : cap;
+            R.advance(cnt, keep, reorth, batch);
+            o.matvecs += cnt;
+            a.resize(cnt);
+            b.resize(cnt);
+            R.read_range(j, cnt, a.data(), b.data());
+            for (int i = 0; i < cnt && !stop; ++i) {
+                o.alpha.push_back(a[i]);
+                o.beta.push_back(b[i]);
+                if (b[i] < breakdown_tol || check(j + i)) stop = true;
+            }
+            j += cnt;
+        }
+        if (keep && R.basis.size() > o.alpha.size()) R.basis.resize(o.alpha.size());
+        if (gate && !o.alpha.empty()) {
+            std::vector<double> vals;
+            const int m = leading_block(o.alpha, o.beta, static_cast<int>(o.alpha.size()));
+            o.converged = lowest_level(o.alpha, o.beta, m, &vals);
+            if (!vals.empty()) o.e0 = vals.front();
+        }
+        return o;
+    }
     // pipelined: step j runs while the host tests step j - 1's prefix
     int launched = 0;
     auto check = [&](int j) -> bool {   // after alpha_j, beta_{j+1} are known
