@@ -269,6 +269,29 @@ void launch_team_t(const qb_sector* row, const qb_sector* col, const qb_program*
         throw Error(QB_EUNSUPPORTED, "block matvec: at most 64 vectors");
 }
 
+// The calling thread's last shape choices by launch identity (the sectors, the program, a tag of the vectors),
+// so that a step does not rebuild its size-class key. An entry made under another tuner generation is ignored;
+// one left by a destroyed object whose address came back can only cost time, as every shape gives the same y.
+struct ShapeMemo {
+    struct Entry {
+        const void *row = nullptr, *col = nullptr, *prog = nullptr;
+        int tag = -1, shape = 0;
+        unsigned gen = 0;
+    };
+    Entry e[8];
+    int next = 0;
+    int find(const void* r, const void* c, const void* p, int tag, unsigned gen) const {
+        for (const auto& x : e)
+            if (x.row == r && x.col == c && x.prog == p && x.tag == tag && x.gen == gen) return x.shape;
+        return -1;
+    }
+    void put(const void* r, const void* c, const void* p, int tag, unsigned gen, int shape) {
+        e[next] = Entry{r, c, p, tag, shape, gen};
+        next = (next + 1) % 8;
+    }
+};
+thread_local ShapeMemo t_memo;
+
 // The size classes a launch shape is tuned for: the sector's group and lookup, the program's groups, the row
 // count (by powers of two) and the vectors' number and types.
 std::string walk_key(const qb_sector* row, const qb_sector* col, const qb_program* P, int nv, int st_bits, int in32,
@@ -327,8 +350,15 @@ void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program
         }
     };
     const int shapes = NV == 1 ? 6 : 2;
-    const int shape =
-        tune_choose("walk", walk_key(row, col, P, NV, sizeof(ST) * 8, kF32, kOutF32), shapes, 0, st, run);
+    const int tag = (NV << 4) | (static_cast<int>(sizeof(ST)) << 1) | (kF32 ? 1 : 0) | (kOutF32 ? 256 : 0);
+    const unsigned gen = tune_generation();
+    int shape = t_memo.find(row, col, P, tag, gen);
+    if (shape < 0) {
+        shape = tune_choose("walk", walk_key(row, col, P, NV, sizeof(ST) * 8, kF32, kOutF32), shapes, 0, st, run);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st, &cap);
+        if (cap == cudaStreamCaptureStatusNone) t_memo.put(row, col, P, tag, gen, shape);
+    }
     run(shape);
 }
 
@@ -364,7 +394,15 @@ void launch_team(const qb_sector* row, const qb_sector* col, const qb_program* P
             launch_team_t<4, kF32, kOutF32>(row, col, P, in, out, k, st);
     };
     const int shapes = k <= 32 ? 4 : 3;
-    const int shape = tune_choose("walk_team", walk_key(row, col, P, k, 64, kF32, kOutF32), shapes, 0, st, run);
+    const int tag = 512 | (k << 10) | (kF32 ? 1 : 0) | (kOutF32 ? 2 : 0);
+    const unsigned gen = tune_generation();
+    int shape = t_memo.find(row, col, P, tag, gen);
+    if (shape < 0) {
+        shape = tune_choose("walk_team", walk_key(row, col, P, k, 64, kF32, kOutF32), shapes, 0, st, run);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st, &cap);
+        if (cap == cudaStreamCaptureStatusNone) t_memo.put(row, col, P, tag, gen, shape);
+    }
     run(shape);
 }
 

@@ -54,6 +54,8 @@ void set_thread_allowance(std::size_t bytes);
 // The candidates must give the same result bit for bit.
 int tune_choose(const char* family, const std::string& key, int n, int fallback, cudaStream_t st,
                 const std::function<void(int)>& run);
+// Changes whenever the tuner's modes, forces or known choices change (memos of choices compare it).
+unsigned tune_generation();
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;

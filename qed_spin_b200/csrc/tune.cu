@@ -2,8 +2,8 @@
 // tune.cu -- the launch-shape tuner.
 //
 // A kernel family with several launch shapes that give the same result bit for bit (the row walk: one thread
-// per state, or a warp's states compacted; the block walk: 8, 16 or 32 lanes per state; the CSR matvec: rows
-// per block) asks tune_choose for a shape. The first call for a shape key (the kernel family, the sector's and
+// per state, a warp's states compacted, or for one vector a team of 4 to 32 lanes per state; the block walk:
+// 4, 8, 16 or 32 lanes per state) asks tune_choose for a shape. The first call for a shape key (the kernel family, the sector's and
 // program's size classes, the vector count and types, the device) times every candidate on the caller's stream
 // with CUDA events -- each candidate runs once to warm up, then three times timed -- and keeps the fastest;
 // later calls reuse it. Because the candidates agree bit for bit, a choice changes only the time.
@@ -14,6 +14,7 @@
 // every new choice is appended: "key<TAB>choice<TAB>ms of each candidate".
 // No reference counterpart: the reference fixes its launch shapes (src/gpu/rep_matvec.cu).
 // =============================================================================
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -80,16 +81,27 @@ Tuner& tuner() {
     return *t;
 }
 
-std::string device_tag() {
-    int dev = 0, sms = 0, major = 0, minor = 0;
+std::atomic<unsigned> g_generation{1};
+
+// The device's architecture and SM count, resolved once per device.
+const std::string& device_tag() {
+    static std::mutex mu;
+    static std::map<int, std::string> tags;
+    int dev = 0;
     cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = tags.find(dev);
+    if (it != tags.end()) return it->second;
+    int sms = 0, major = 0, minor = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-    return "sm" + std::to_string(major) + std::to_string(minor) + "x" + std::to_string(sms);
+    return tags[dev] = "sm" + std::to_string(major) + std::to_string(minor) + "x" + std::to_string(sms);
 }
 
 }  // namespace
+
+unsigned tune_generation() { return g_generation.load(std::memory_order_relaxed); }
 
 int tune_choose(const char* family, const std::string& key, int n, int fallback, cudaStream_t st,
                 const std::function<void(int)>& run) {
@@ -164,6 +176,7 @@ int qb_tune_mode(int mode, int* previous) {
         T.init_locked();
         if (previous) *previous = T.mode;
         if (mode >= 0) T.mode = mode;
+        ++g_generation;
     });
 }
 
@@ -177,6 +190,7 @@ int qb_tune_force(const char* family, int choice) {
             T.forced.erase(family);
         else
             T.forced[family] = choice;
+        ++g_generation;
     });
 }
 
@@ -186,6 +200,7 @@ int qb_tune_clear(void) {
         std::lock_guard<std::mutex> lk(T.mu);
         T.known.clear();
         T.forced.clear();
+        ++qb::g_generation;
     });
 }
 
@@ -214,6 +229,7 @@ int qb_tune_load(const char* path) {
         std::lock_guard<std::mutex> lk(T.mu);
         T.init_locked();
         if (!T.load_locked(path)) throw Error(QB_EINVAL, std::string("cannot read ") + path);
+        ++g_generation;
     });
 }
 

@@ -1,7 +1,8 @@
 """Lanczos steps replayed from captured CUDA graphs give the scalars and vectors of steps launched one by one,
 bit for bit (QB_GRAPHS=0 launches every step; sectors of up to 2^20 states otherwise run batches of captured
-steps): the ungated recurrence (none and local reorthogonalisation, FP64 and FP32 storage), the k = 1 lane
-with its FP64 refinement from a kept basis, the certified ground-state vector, and the continued fraction."""
+steps): the ungated recurrence (none and local reorthogonalisation, FP64 and FP32 storage), the certified
+ground-state vector (its kept basis filled on the device), and the continued fraction; and the k = 1 lane, which
+launches step by step either way, is unchanged by the switch."""
 import numpy as np
 import pytest
 
