@@ -594,8 +594,9 @@ def levels_measure(S, P, args):
 
 def graphs_measure(S, P):
     """The lanes that batch their steps into captured CUDA graphs on a small sector (chain-20, 9,252 states),
-    with graphs and launched step by step (QB_GRAPHS=0): the k = 1 lane, the certified ground-state vector and a
-    200-step continued fraction. Median seconds of 5 calls each after a warm-up call."""
+    with graphs and launched step by step (QB_GRAPHS=0): the certified ground-state vector and a 200-step
+    continued fraction; and, as a control, the k = 1 lane, which runs step by step either way. Median seconds of
+    5 calls each after a warm-up call."""
     from qed_spin_b200 import device as D
     rng = np.random.default_rng(1)
     phi = rng.standard_normal(S.dim) + 1j * rng.standard_normal(S.dim)
