@@ -796,8 +796,9 @@ __device__ bool ql_first_row(double* d, double* e, double* z, int m, std::size_t
                     QB_E(mm) = 0.0;
                     break;
                 }
-                s = f / r;
-                c = g / r;
+                const double ir = 1.0 / r;
+                s = f * ir;
+                c = g * ir;
                 g = QB_D(i + 1) - p;
                 r = (QB_D(i) - g) * s + 2.0 * c * b;
                 p = s * r;
@@ -823,20 +824,26 @@ __device__ bool ql_first_row(double* d, double* e, double* z, int m, std::size_t
 // weights w_i = z_i^2, and its moments about its lowest weighted level e_min (sample_moments,
 // include/ed/thermal/ftlm.h:165-192): Z_t = sum_i w_i e^{-beta_t x_i}, E1_t = sum_i x_i w_i e^{-beta_t x_i},
 // E2_t = sum_i x_i^2 w_i e^{-beta_t x_i}, x_i = theta_i - e_min, summed in ascending theta (ties in QL order).
-// mom[q * n_items + item]: q = 0 e_min, then Z, E1, E2 of temperature t at q = 1 + 3t, 2 + 3t, 3 + 3t. scratch holds
-// 3 cap_max doubles and ord cap_max ints per item, strided by n_items so that a warp's loads coalesce.
+// mom[q * n_items + item]: q = 0 e_min, then Z, E1, E2 of temperature t at q = 1 + 3t, 2 + 3t, 3 + 3t. The
+// tridiagonal and its order sit in shared memory when `in_smem` (cap_max 28-byte rows per thread, strided by the
+// block's threads), else in `scratch` / `ord` (3 cap_max doubles and cap_max ints per item, strided by n_items).
 __global__ void k_sample_moments(const CurveBlock* blocks, int n_items, int k, const double* alpha, const double* beta,
-                                 const double* betas, int n_beta, int cap_max, double* scratch, int* ord, double* mom,
-                                 int* err) {
+                                 const double* betas, int n_beta, int cap_max, bool in_smem, double* scratch, int* ord,
+                                 double* mom, int* err) {
+    extern __shared__ __align__(16) unsigned char csm[];
     const int item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= n_items) return;
     const CurveBlock B = blocks[item / k];
     const int s = item % k;
-    const std::size_t ld = static_cast<std::size_t>(n_items);
-    double* d = scratch + item;
-    double* e = scratch + static_cast<std::size_t>(cap_max) * ld + item;
-    double* z = scratch + 2 * static_cast<std::size_t>(cap_max) * ld + item;
-    int* o = ord + item;
+    const std::size_t ld = in_smem ? blockDim.x : static_cast<std::size_t>(n_items);   // the tridiagonal's stride
+    const std::size_t mld = static_cast<std::size_t>(n_items);                         // the output's stride
+    double* base = in_smem ? reinterpret_cast<double*>(csm) + threadIdx.x : scratch + item;
+    double* d = base;
+    double* e = base + static_cast<std::size_t>(cap_max) * ld;
+    double* z = base + 2 * static_cast<std::size_t>(cap_max) * ld;
+    int* o = in_smem ? reinterpret_cast<int*>(reinterpret_cast<double*>(csm) + 3 * static_cast<std::size_t>(cap_max) *
+                                                                                 blockDim.x) + threadIdx.x
+                     : ord + item;
     const double* a = alpha + B.a_off;
     const double* b = beta + B.b_off;
     int m = 0;
@@ -884,9 +891,9 @@ __global__ void k_sample_moments(const CurveBlock* blocks, int n_items, int k, c
             e1 += x * bb;
             e2 += x * x * bb;
         }
-        mom[(1 + 3 * static_cast<std::size_t>(t)) * ld + item] = zs;
-        mom[(2 + 3 * static_cast<std::size_t>(t)) * ld + item] = e1;
-        mom[(3 + 3 * static_cast<std::size_t>(t)) * ld + item] = e2;
+        mom[(1 + 3 * static_cast<std::size_t>(t)) * mld + item] = zs;
+        mom[(2 + 3 * static_cast<std::size_t>(t)) * mld + item] = e1;
+        mom[(3 + 3 * static_cast<std::size_t>(t)) * mld + item] = e2;
     }
 }
 
@@ -1078,9 +1085,13 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         cap_max = std::max(cap_max, caps[b]);
     }
     DevBuf<CurveBlock> d_cb(n_blocks);
-    DevBuf<double> d_betas(std::max(1, n_beta)), scratch(3 * static_cast<std::size_t>(cap_max) * n_items);
+    // a thread's tridiagonal in shared memory (32 threads a block) while it fits, else in global scratch
+    const std::size_t row_bytes = static_cast<std::size_t>(cap_max) * (3 * 8 + 4);
+    const bool in_smem = row_bytes * 32 <= 200 * 1024;
+    const std::size_t n_scr = in_smem ? 1 : static_cast<std::size_t>(cap_max) * n_items;
+    DevBuf<double> d_betas(std::max(1, n_beta)), scratch(3 * n_scr);
     DevBuf<double> mom((1 + 3 * static_cast<std::size_t>(n_beta)) * n_items);
-    DevBuf<int> ord(static_cast<std::size_t>(cap_max) * n_items), err(1);
+    DevBuf<int> ord(n_scr), err(1);
     const std::size_t nbt = static_cast<std::size_t>(n_blocks) * n_beta;
     DevBuf<double> out(3 * nbt + n_blocks);
     cudaStream_t st0 = cudaStreamPerThread;
@@ -1088,8 +1099,13 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
     if (n_beta > 0)
         cuda_check(cudaMemcpyAsync(d_betas.p, betas, n_beta * 8, cudaMemcpyHostToDevice, st0), "upload");
     cuda_check(cudaMemsetAsync(err.p, 0, 4, st0), "zero");
-    k_sample_moments<<<(n_items + 127) / 128, 128, 0, st0>>>(d_cb.p, n_items, k, d_alpha.p, d_beta.p, d_betas.p, n_beta,
-                                                           cap_max, scratch.p, ord.p, mom.p, err.p);
+    const int cthreads = in_smem ? 32 : 128;
+    const std::size_t csmem = in_smem ? row_bytes * 32 : 0;
+    if (csmem > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(k_sample_moments, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(csmem)), "smem attribute");
+    k_sample_moments<<<(n_items + cthreads - 1) / cthreads, cthreads, csmem, st0>>>(
+        d_cb.p, n_items, k, d_alpha.p, d_beta.p, d_betas.p, n_beta, cap_max, in_smem, scratch.p, ord.p, mom.p, err.p);
     const std::size_t n_comb = static_cast<std::size_t>(n_blocks) * std::max(1, n_beta);
     k_block_combine<<<static_cast<unsigned>((n_comb + 127) / 128), 128, 0, st0>>>(
         d_cb.p, n_blocks, k, mom.p, n_items, d_betas.p, n_beta, out.p, out.p + nbt, out.p + 2 * nbt, out.p + 3 * nbt);
