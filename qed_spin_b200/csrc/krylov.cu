@@ -37,12 +37,17 @@
 #include <random>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "qb_internal.cuh"
 
 #include "qb_krylov.cuh"
 #include "qb_walk.cuh"
+
+#ifndef QB_FMV_BLOCKS
+#define QB_FMV_BLOCKS 5
+#endif
 
 namespace qb {
 namespace {
@@ -162,8 +167,17 @@ __host__ __device__ inline int tile_rows(int k) { return k >= 256 ? 1 : 256 / k;
 // Pass 1: w = A v_j - beta_j v_{j-1} on the CSR (8 lanes per row, lane l owns columns l, l + 8, ...), and
 // alpha_j = Re <v_j, w> per column: block partials in shared memory summed in row order, the block sums in
 // block order by the last block.
+// Blocks per SM the pass is compiled for: FP32 storage fits 48 registers without spills at five (the batched
+// FTLM's recurrences: 1.70 -> 1.62 s; six spill and take 1.75 s); FP64 holds three (80 registers, as unbounded).
+template <class T> struct FmvBlocks {
+    static constexpr int value = 3;
+};
+template <> struct FmvBlocks<float2> {
+    static constexpr int value = QB_FMV_BLOCKS;
+};
+
 template <class T, int CPL>
-__global__ void __launch_bounds__(256) fmv_alpha(std::uint64_t rows, int k, int j,
+__global__ void __launch_bounds__(256, FmvBlocks<T>::value) fmv_alpha(std::uint64_t rows, int k, int j,
                                                  const unsigned long long* __restrict__ row_ptr,
                                                  const std::uint32_t* __restrict__ col,
                                                  const unsigned char* __restrict__ ids, int id_bytes,
@@ -332,14 +346,25 @@ __global__ void __launch_bounds__(256) fnext(std::uint64_t n, int k, int j, doub
     }
 }
 
+// One wave of fmv_alpha blocks: as many as fit on the SMs at once (at least 2 kBlockRecGrid, at most
+// kMaxRedBlocks), and none past the rows.
+template <class T, int C> unsigned fmv_grid(std::uint64_t n) {
+    static const unsigned wave = [] {
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fmv_alpha<T, C>, 256, 0);
+        return static_cast<unsigned>(std::min(kMaxRedBlocks, std::max(2 * kBlockRecGrid, per_sm * sms)));
+    }();
+    return static_cast<unsigned>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 31) / 32, wave)));
+}
+
 template <class T>
 void fused_step(const qb_csr* A, std::uint64_t n, int k, int j, double tol, const T* vc, const T* vp, T* w, T* vn,
                 BScal S, cudaStream_t st) {
-    const unsigned grid = static_cast<unsigned>(std::max<std::uint64_t>(1, std::min<std::uint64_t>((n + 31) / 32,
-                                                                                                    2 * kBlockRecGrid)));
     const int cpl = (k + 7) / 8;
-#define QB_FMV(C) fmv_alpha<T, C><<<grid, 256, 0, st>>>(n, k, j, A->row_ptr.p, A->col_idx.p, A->ids.p, A->id_bytes, \
-                                                        A->vals.p, A->n_dict, vc, vp, w, S)
+#define QB_FMV(C) fmv_alpha<T, C><<<fmv_grid<T, C>(n), 256, 0, st>>>(n, k, j, A->row_ptr.p, A->col_idx.p, A->ids.p, \
+                                                                   A->id_bytes, A->vals.p, A->n_dict, vc, vp, w, S)
     if (cpl <= 1) QB_FMV(1);
     else if (cpl <= 2) QB_FMV(2);
     else if (cpl <= 4) QB_FMV(4);
