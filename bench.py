@@ -831,8 +831,13 @@ def profile_case(args):
     S = D.Sector(spec)
     P = D.Program(prog)
     A = None
+    build_s = None
     if args.profile_lane == "csr":
+        torch.cuda.synchronize()
+        t = time.perf_counter()
         A = D.Csr(S, S, P)
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t
         A.attach(P)
     x = torch.randn(S.dim, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
@@ -845,7 +850,8 @@ def profile_case(args):
     torch.cuda.synchronize()
     print(json.dumps({"profile_case": args.profile_case, "lane": args.profile_lane, "dim": S.dim,
                       "ms_per_matvec": (time.perf_counter() - t) / args.steps * 1e3, "sector": S.info(),
-                      "csr": A.info() if A is not None else None, "tuned_shapes": D.tune_entries()}))
+                      "csr": A.info() if A is not None else None, "csr_build_s": build_s,
+                      "tuned_shapes": D.tune_entries()}))
 
 
 def emitted_per_row(reps: np.ndarray, prog) -> float:

@@ -184,13 +184,43 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
     for (u64 r = static_cast<u64>(blockIdx.x) * kBuildWarps + wid; r < row.dim; r += nwarps) {
         const ST s = static_cast<ST>(__ldg(row.reps + r));
         const double w = __ldg(row.inv_norms + r);
+        // Up to 256 groups: the acting groups first (cheap tests, 32 groups a round), then the canonicalisations
+        // of the acting ones only, 32 at a time in group order (lane a of a round takes the a-th acting group).
+        // More groups: 32 groups a round, each lane canonicalising its own when it acts. Either way the entries
+        // come in group order.
+        constexpr int kWords = kMaxRowEntries / 32;
+        u32 amask[kWords];
+        const int n_words = static_cast<int>((sp.P.n_groups + 31) / 32);
+        const bool compact = n_words <= kWords;
+        int n_items = n_words * 32;
+        if (compact) {
+            n_items = 0;
+            for (int wi = 0; wi < n_words; ++wi) {
+                const u32 g = static_cast<u32>(wi) * 32 + lane;
+                const bool act = g < sp.P.n_groups && acting_subgroup<ST>(sp.P, s, g) >= 0;
+                amask[wi] = __ballot_sync(0xffffffffu, act);
+                n_items += __popc(amask[wi]);
+            }
+        }
         int m = 0;
-        for (u32 g0 = 0; g0 < sp.P.n_groups; g0 += 32) {
-            const u32 g = g0 + lane;
+        for (int a0 = 0; a0 < n_items; a0 += 32) {
+            const int a = a0 + lane;
             bool ok = false;
             long long j = 0;
             cplx c{0.0, 0.0};
-            if (g < sp.P.n_groups) {
+            u32 g = static_cast<u32>(a);
+            bool go = false;
+            if (compact) {
+                if (a < n_items) {
+                    int rem = a, wi = 0;
+                    while (rem >= __popc(amask[wi])) rem -= __popc(amask[wi++]);
+                    g = static_cast<u32>(wi) * 32 + __fns(amask[wi], 0, rem + 1);
+                    go = true;
+                }
+            } else {
+                go = g < sp.P.n_groups;
+            }
+            if (go) {
                 const int vi = acting_subgroup<ST>(sp.P, s, g);
                 if (vi >= 0) {
                     const cplx h = subgroup_value<ST>(sp.P, s, vi);
