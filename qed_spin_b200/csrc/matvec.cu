@@ -8,16 +8,19 @@
 // complex arithmetic (no fused multiply-adds), so y equals the reference's sector_gather bit for bit
 // in FP64 storage.
 //
-// Two kernels:
+// Three kernels, whose launch shapes the tuner (tune.cu) picks per size class; every shape gives the same y
+// bit for bit:
 //   walk_rows   one thread per row, up to 8 separate vectors (the reference's multi-apply contract:
 //               every output equals the single apply bit for bit). The row program and the key
 //               table are staged in shared memory; a warp's lanes advance in step over their own
-//               acting groups so the expensive canonicalisation runs with every lane busy.
-//   walk_team   the block matvec of the sampled methods: k vectors interleaved by row. A team of
-//               8 lanes owns a row: the lanes test 8 groups at once, canonicalise the acting targets
-//               in parallel, then every lane accumulates its slice of the k columns from each target
-//               in group order -- one canonicalisation per entry for all k vectors, and each x row
-//               read as one contiguous segment.
+//               acting groups.
+//   walk_warp   the same with a warp's 32 rows compacted: the acting (row, group) pairs are laid out
+//               row-major and canonicalised 32 at a time; each row adds its products in order.
+//   walk_team   a team of 4, 8, 16 or 32 lanes owns a row: the lanes test that many groups at once,
+//               canonicalise the acting targets in parallel, then every lane accumulates its slice of
+//               the k columns from each target in group order -- the block matvec of the sampled methods
+//               (k vectors interleaved by row), and for one vector on a small sector, where one thread
+//               per row leaves most of the GPU idle.
 // =============================================================================
 #include <algorithm>
 #include <cmath>
