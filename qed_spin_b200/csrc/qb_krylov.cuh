@@ -832,6 +832,7 @@ struct Recurrence {
     }
     ~Recurrence() {
         if (ev) cudaEventDestroy(ev);
+        if (!graphs.empty()) cudaStreamSynchronize(st);   // no batch of ours may still be running
         for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     }
 
