@@ -752,8 +752,11 @@ void launch_pack(const std::vector<int>& set, const qb_sector* const* secs, cons
         cuda_check(cudaGetDevice(&dev), "device");
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem), "occupancy");
-        const int grid = static_cast<int>(std::min<std::size_t>(set.size(), static_cast<std::size_t>(sms) *
-                                                                               std::max(1, std::min(per_sm, 2))));
+        // at most two blocks per SM, and at most 2 GB of scratch in all (each block's results are its own,
+        // whatever the grid)
+        const std::size_t by_bytes = std::max<std::size_t>(1, (std::size_t(2) << 30) / slot.bytes);
+        const int grid = static_cast<int>(std::min({set.size(), static_cast<std::size_t>(sms) *
+                                                                    std::max(1, std::min(per_sm, 2)), by_bytes}));
         d_items.alloc(items.size());
         counter.alloc(1);
         scratch.alloc(slot.bytes * grid);
