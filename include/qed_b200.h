@@ -292,9 +292,8 @@ int qb_lanczos_noalloc(const qb_sector* sec, const qb_program* prog, const void*
  *   "walk_team"  the block walk of k interleaved vectors (qb_matvec_block, FTLM on the walk): 0, 1, 2, 3 =
  *                8, 16, 32, 4 lanes per state (4 only when k <= 32).
  * The first launch for a size class (the sector's group and lookup, the program's groups, the row count by
- * powers of two, the vectors' number and types, the device) times every shape on the caller's stream (a timed
- * warm-up, then three timed runs unless the warm-up took 1.5x the best average so far; this synchronises that
- * stream) and keeps the fastest. A stream
+ * powers of two, the vectors' number and types, the device) times every shape on the caller's stream (one
+ * warm-up and three timed runs each; this synchronises that stream once) and keeps the fastest. A stream
  * that is capturing a graph is never timed. No reference counterpart: the reference fixes its launch shapes
  * (src/gpu/rep_matvec.cu).
  * mode: 1 measure on first use (the default; QB_TUNE overrides it at start), 2 only choices already known

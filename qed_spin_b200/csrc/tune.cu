@@ -5,8 +5,8 @@
 // per state, a warp's states compacted, or for one vector a team of 4 to 32 lanes per state; the block walk:
 // 4, 8, 16 or 32 lanes per state) asks tune_choose for a shape. The first call for a shape key (the kernel family, the sector's and
 // program's size classes, the vector count and types, the device) times every candidate on the caller's stream
-// with CUDA events -- each candidate runs once to warm up, then, unless that run already took 1.5x the best
-// average so far, three times timed -- and keeps the fastest; later calls reuse it. Because the candidates agree bit for bit, a choice changes only the time.
+// with CUDA events -- each candidate runs once to warm up, then three times timed -- and keeps the fastest;
+// later calls reuse it. Because the candidates agree bit for bit, a choice changes only the time.
 //
 // Modes (QB_TUNE, or qb_tune_mode): 1 measure on first use (default); 2 use only choices already known (from
 // this process or a loaded cache file), else the family's default; 0 always the default. A stream that is
@@ -128,22 +128,14 @@ int tune_choose(const char* family, const std::string& key, int n, int fallback,
     float best = 0.0f;
     try {
         for (int i = 0; i < n; ++i) {
-            // warm-up (module load, first touch of the tables), itself timed: a candidate whose warm-up already
-            // takes 1.5x the best average is not timed further (its warm-up time is what is kept for it)
+            run(i);   // warm-up: module load, first touch of the tables
             cuda_check(cudaEventRecord(e0, st), "event");
-            run(i);
+            for (int r = 0; r < 3; ++r) run(i);
             cuda_check(cudaEventRecord(e1, st), "event");
             cuda_check(cudaEventSynchronize(e1), "tune");
             float ms = 0.0f;
             cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
-            if (i == 0 || ms < 1.5f * best) {
-                cuda_check(cudaEventRecord(e0, st), "event");
-                for (int r = 0; r < 3; ++r) run(i);
-                cuda_check(cudaEventRecord(e1, st), "event");
-                cuda_check(cudaEventSynchronize(e1), "tune");
-                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
-                ms /= 3.0f;
-            }
+            ms /= 3.0f;
             c.ms.push_back(ms);
             // a candidate must beat the current pick by 3% to replace it (lower indices are the defaults)
             if (i == 0 || ms < 0.97f * best) {
