@@ -258,7 +258,7 @@ def main():
     ap.add_argument("--e0-6x6", action="store_true",
                     help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
                          "(FP64, and FP32 storage + FP64 refinement), one JSON line")
-    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36", "ftlm4"], default=None,
+    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36", "ftlm4", "chain20"], default=None,
                     help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing; "
                          "ftlm4: batched FTLM (40 samples, depth 100) on the four largest N = 24 XXZ blocks")
     ap.add_argument("--profile-lane", choices=["walk", "csr", "c64", "c128"], default="walk",
@@ -819,6 +819,23 @@ def profile_case(args):
         r = D.ftlm_blocks(secs, P, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas, dtype=dt)
         print(json.dumps({"profile_case": "ftlm4", "dtype": dt, "dims": [s.dim for s in secs],
                           "s": time.perf_counter() - t, "phases": r["stats"]}))
+        return
+    if args.profile_case == "chain20":
+        # a small sector (9,252 states) in FP64, the tuner on: the shape one vector takes on a small sector
+        spec = lat.chain_sector(20, 10, 0)
+        prog = ops.row_program(ops.from_products(20, ops.heisenberg_products(lat.chain_bonds(20))))
+        S, P = D.Sector(spec), D.Program(prog)
+        x = torch.randn(S.dim, dtype=torch.complex128, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(args.warmup):
+            D.matvec(S, S, P, [x], [y])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            D.matvec(S, S, P, [x], [y])
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "chain20", "dim": S.dim, "ms_per_matvec": (time.perf_counter() - t) /
+                          args.steps * 1e3, "tuned_shapes": D.tune_entries()}))
         return
     if args.profile_case == "chain32":
         spec, prog, _ = workload()
