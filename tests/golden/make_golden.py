@@ -3,12 +3,15 @@
 Run in a tree where the reference sources are present (it reads them and its compiled CPU engine,
 oracle/_ref/libqed_ref.so, built by `make -C oracle`):
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py [REFERENCE_ROOT] [--json-only]
+
+(--json-only rewrites golden.json alone, leaving fixtures.npz as it is.)
 
 Writes
   golden.json   energies the reference recorded in its own golden suite
                 (tests/python/golden/refs/api-2026-09/cpu.json.gz, tier "exact" 1e-10), for the chain models
-                whose fixed-S^z spectra the sector tests reassemble, plus the N = 12 Heisenberg ring E0.
+                whose fixed-S^z spectra the sector tests reassemble, plus the N = 12 Heisenberg ring E0; and the
+                exact thermodynamics (T, E, C, S) it recorded for the J1-J2 chain N = 12.
   fixtures.npz  outputs of the reference engine itself on small seeded cases: representatives and 1/norms,
                 row programs, y = H x, the merged CSR pattern and its spmv of x, the k = 4 lane's levels, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
                 curves and continued-fraction spectra.
@@ -45,6 +48,10 @@ RECORDS = {
     "xy_chain10": ["xy_chain10/api/eigs/sz=5/k=4"],
 }
 
+# exact thermodynamics of the whole Hilbert space (every block solved densely: the thermal verb's exact method, and
+# its FTLM method with the default dense limit of 512 states, which every block of a 12-site chain is under)
+THERMAL = {"j1j2_chain12": ["j1j2_chain12/api/thermal/exact/auto", "j1j2_chain12/api/thermal/ftlm/auto"]}
+
 # small seeded cases run through the reference engine: (name, N, n_up, group, products)
 def cases():
     out = []
@@ -63,7 +70,7 @@ def cases():
     return out
 
 
-def main(ref_root: str):
+def main(ref_root: str, json_only: bool = False):
     golden = {"source": "tests/python/golden/refs/api-2026-09/cpu.json.gz (the reference's golden suite)",
               "tier_exact_tol": 1e-10, "models": {}, "known": {}}
     recs = json.load(gzip.open(os.path.join(ref_root, "tests/python/golden/refs/api-2026-09/cpu.json.gz")))["records"]
@@ -76,6 +83,15 @@ def main(ref_root: str):
         }
     # the N = 12 Heisenberg ring, k = 0 (a textbook value; the reference's k = 1 lane reproduces it)
     golden["known"]["heis12_k0_e0"] = -5.387390917445
+    golden["thermal"] = {}
+    for name, keys in THERMAL.items():
+        golden["thermal"][name] = {k: {q: recs[k]["values"][q] for q in ("T", "E", "C", "S")} | {"tier": recs[k]["tier"]}
+                                   for k in keys}
+    if json_only:
+        with open(os.path.join(HERE, "golden.json"), "w") as fh:
+            json.dump(golden, fh, indent=1)
+        print("wrote", os.path.join(HERE, "golden.json"))
+        return
 
     fx = {}
     for name, spec, prods in cases():
@@ -124,4 +140,5 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else "/root/reference", json_only="--json-only" in sys.argv[1:])

@@ -123,6 +123,40 @@ def test_golden_fixed_sz_spectra(golden, model):
         np.testing.assert_allclose(levels[: len(ref)], ref, rtol=0, atol=1e-10)
 
 
+def test_golden_exact_thermodynamics(golden):
+    """The whole Hilbert space's thermodynamics of the J1-J2 chain N = 12 -- every S^z x momentum block's dense
+    spectrum, its exact trace, and the thermal driver's log-space combine -- equal the reference's golden thermal
+    records (its exact method, and its FTLM method, which densifies every block of this size): tier exact,
+    1e-10 relative."""
+    g = golden["models"]["j1j2_chain12"]
+    N = g["n_sites"]
+    prods = [(o, tuple(s), complex(c[0], c[1])) for o, s, c in g["products"]]
+    prog = ops.row_program(ops.from_products(N, prods))
+    recs = golden["thermal"]["j1j2_chain12"]
+    T = np.asarray(recs["j1j2_chain12/api/thermal/exact/auto"]["T"])
+    betas = 1.0 / T
+    curves, n_states = [], 0
+    for n_up in range(N + 1):
+        for k in range(N):
+            lv = _sector_spectrum(lat.chain_sector(N, n_up, k), prog)
+            if len(lv) == 0:
+                continue
+            n_states += len(lv)
+            e0 = lv.min()
+            w = np.exp(-np.outer(betas, lv - e0))
+            z = w.sum(axis=1)
+            m1 = (w * (lv - e0)).sum(axis=1) / z
+            m2 = (w * (lv - e0) ** 2).sum(axis=1) / z
+            curves.append({"lnZ": np.log(z) - betas * e0, "E": e0 + m1, "V": np.maximum(m2 - m1 * m1, 0.0)})
+    assert n_states == 2 ** N
+    tot = O.combine_blocks(curves, betas)
+    for key, rec in recs.items():
+        assert np.allclose(rec["T"], T)
+        for q in ("E", "C", "S"):
+            ref = np.asarray(rec[q])
+            np.testing.assert_allclose(tot[q], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=f"{key} {q}")
+
+
 def test_sublattice_engagement():
     """The key order engages exactly where the reference's relaxed rule does (sublattice_code.h:23-34)."""
     assert O.Sector(lat.chain_sector(20, 1, 0)).sublattice() is None
