@@ -11,7 +11,8 @@ Writes
   golden.json   energies the reference recorded in its own golden suite
                 (tests/python/golden/refs/api-2026-09/cpu.json.gz, tier "exact" 1e-10), for the chain models
                 whose fixed-S^z spectra the sector tests reassemble, plus the N = 12 Heisenberg ring E0; and the
-                exact thermodynamics (T, E, C, S) it recorded for the J1-J2 chain N = 12.
+                exact thermodynamics (T, E, C, S) and the T = 0 S^z(pi) spectrum it recorded for the J1-J2 chain
+                N = 12.
   fixtures.npz  outputs of the reference engine itself on small seeded cases: representatives and 1/norms,
                 row programs, y = H x, the merged CSR pattern and its spmv of x, the k = 4 lane's levels, Lanczos alpha/beta, the k = 1 lane's E0, FTLM
                 curves and continued-fraction spectra.
@@ -52,6 +53,10 @@ RECORDS = {
 # its FTLM method with the default dense limit of 512 states, which every block of a 12-site chain is under)
 THERMAL = {"j1j2_chain12": ["j1j2_chain12/api/thermal/exact/auto", "j1j2_chain12/api/thermal/ftlm/auto"]}
 
+# T = 0 dynamics of S^z(q = pi) = N^-1/2 sum_i e^{i pi i} S^z_i on 41 frequencies in [-1, 4], eta 0.15, Krylov 80
+# (the golden harness's dynamics case, tests/python/golden/cases.py:175-190), with and without symmetry sectors
+DYNAMICS = {"j1j2_chain12": ["j1j2_chain12/api/dynamics/T=0/auto/SzQ", "j1j2_chain12/api/dynamics/T=0/none/SzQ"]}
+
 # small seeded cases run through the reference engine: (name, N, n_up, group, products)
 def cases():
     out = []
@@ -87,6 +92,11 @@ def main(ref_root: str, json_only: bool = False):
     for name, keys in THERMAL.items():
         golden["thermal"][name] = {k: {q: recs[k]["values"][q] for q in ("T", "E", "C", "S")} | {"tier": recs[k]["tier"]}
                                    for k in keys}
+    golden["dynamics"] = {}
+    for name, keys in DYNAMICS.items():
+        golden["dynamics"][name] = {"omega": [-1.0, 4.0, 41], "eta": 0.15, "krylov": 80, "q": "pi",
+                                    "records": {k: recs[k]["values"]["S"] for k in keys},
+                                    "tiers": {k: recs[k]["tier"] for k in keys}}
     if json_only:
         with open(os.path.join(HERE, "golden.json"), "w") as fh:
             json.dump(golden, fh, indent=1)

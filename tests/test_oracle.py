@@ -157,6 +157,54 @@ def test_golden_exact_thermodynamics(golden):
             np.testing.assert_allclose(tot[q], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=f"{key} {q}")
 
 
+def test_golden_t0_dynamics(golden):
+    """The T = 0 S^z(pi) spectrum of the J1-J2 chain N = 12 equals the reference's golden records (tier exact,
+    1e-10): for each ground state -- this chain sits at the Majumdar-Ghosh point, so its ground manifold is the
+    two dimer states, one at momentum 0 and one at pi -- phi = S^z(pi) psi0 through the oracle's cross-sector
+    gather into the block at momentum k + pi, then the oracle's continued fraction shifted by E0 (80 steps span
+    every block here, so the fraction is exact); the spectra averaged over the ground manifold, which is what
+    the reference's verb returns for a degenerate ground state."""
+    g = golden["models"]["j1j2_chain12"]
+    N = g["n_sites"]
+    prods = [(o, tuple(s), complex(c[0], c[1])) for o, s, c in g["products"]]
+    H = ops.from_products(N, prods)
+    prog = ops.row_program(H)
+    dyn = golden["dynamics"]["j1j2_chain12"]
+    lo, hi, n_om = dyn["omega"]
+    omega = np.linspace(lo, hi, n_om)
+    eta, depth, m = dyn["eta"], dyn["krylov"], N // 2   # q = pi = 2 pi m / N
+    Sq = ops.from_products(N, ops.sz_q_products(N, np.pi))
+    ground = []   # (energy, n_up, k, vector in the block's basis)
+    for n_up in range(N + 1):
+        for k in range(N):
+            spec = lat.chain_sector(N, n_up, k)
+            So = O.Sector(spec)
+            d = So.dim
+            if d == 0:
+                continue
+            P = O.Program(prog)
+            Hb = np.zeros((d, d), complex)
+            for j in range(d):
+                e = np.zeros(d, complex)
+                e[j] = 1.0
+                Hb[:, j] = So.gather(P, e)
+            w, V = np.linalg.eigh(Hb)
+            ground += [(w[i], n_up, k, V[:, i]) for i in range(d) if w[i] < w[0] + 1e-9]
+    e0 = min(x[0] for x in ground)
+    ground = [x for x in ground if x[0] < e0 + 1e-9]
+    assert len(ground) == 2 and abs(e0 + 4.5) < 1e-12   # the two dimer states, E0 = -3N/8
+    total = np.zeros(len(omega))
+    for _, n_up, k, psi in ground:
+        src, tgt = lat.chain_sector(N, n_up, k), lat.chain_sector(N, n_up, (k + m) % N)
+        S_src, S_tgt = O.Sector(src), O.Sector(tgt)
+        phi = S_tgt.gather(O.Program(ops.cross_row_program(Sq, tgt, src)), psi, col=S_src)
+        S, _ = S_tgt.cf(O.Program(prog), phi, depth, omega, eta, shift=e0)
+        total += S
+    total /= len(ground)
+    for key, ref in dyn["records"].items():
+        np.testing.assert_allclose(total, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=key)
+
+
 def test_sublattice_engagement():
     """The key order engages exactly where the reference's relaxed rule does (sublattice_code.h:23-34)."""
     assert O.Sector(lat.chain_sector(20, 1, 0)).sublattice() is None
