@@ -42,6 +42,47 @@ ZOO = {
                      + ops.heisenberg_products(lat.chain_bonds(12, 2), 0.5)),
     "xy_chain10": (10, lambda: ops.xxz_products(lat.chain_bonds(10), 1.0, 0.0)),
 }
+
+
+def triangular_torus(Lx: int, Ly: int):
+    """The triangular torus of the golden harness's tri_chiral4x3 (tests/python/support/models.py:439-464): site
+    (x, y) is x + Lx y; nearest neighbours at (1, 0), (0, 1), (-1, 1), next-nearest at (1, 1), (-2, 1), (1, -2), each
+    unordered pair once; counter-clockwise up triangles (x, y), (x+1, y), (x, y+1) and down triangles (x+1, y),
+    (x+1, y+1), (x, y+1)."""
+    def idx(x, y):
+        return (x % Lx) + Lx * (y % Ly)
+
+    def once(bonds):
+        seen, out = set(), []
+        for i, j in bonds:
+            key = (min(i, j), max(i, j))
+            if i != j and key not in seen:
+                seen.add(key)
+                out.append((i, j))
+        return out
+
+    nn, nnn, tri = [], [], []
+    for y in range(Ly):
+        for x in range(Lx):
+            i = idx(x, y)
+            nn += [(i, idx(x + 1, y)), (i, idx(x, y + 1)), (i, idx(x - 1, y + 1))]
+            nnn += [(i, idx(x + 1, y + 1)), (i, idx(x - 2, y + 1)), (i, idx(x + 1, y - 2))]
+            tri += [(i, idx(x + 1, y), idx(x, y + 1)), (idx(x + 1, y), idx(x + 1, y + 1), idx(x, y + 1))]
+    return once(nn), once(nnn), tri
+
+
+def _tri_chiral4x3():
+    nn, nnn, tri = triangular_torus(4, 3)
+    return ops.heisenberg_products(nn) + ops.heisenberg_products(nnn, 0.2) + ops.chiral_products(tri, 0.5)
+
+
+# 12-site models whose whole spectrum the thermal test rebuilds block by block (models.py:577-591): the square
+# 4x3 torus's nearest-neighbour Heisenberg model, and the triangular 4x3 torus with J2 = 0.2 and chirality 0.5
+ZOO2D = {
+    "square4x3": (12, lambda: ops.heisenberg_products(lat.square_j1j2_bonds(4, 3)[0])),
+    "tri_chiral4x3": (12, _tri_chiral4x3),
+}
+
 RECORDS = {
     "chain4": ["chain4/api/eigs/sz=2/k=4"],
     "chain5_odd": ["chain5_odd/api/eigs/sz=2/k=4"],
@@ -51,7 +92,9 @@ RECORDS = {
 
 # exact thermodynamics of the whole Hilbert space (every block solved densely: the thermal verb's exact method, and
 # its FTLM method with the default dense limit of 512 states, which every block of a 12-site chain is under)
-THERMAL = {"j1j2_chain12": ["j1j2_chain12/api/thermal/exact/auto", "j1j2_chain12/api/thermal/ftlm/auto"]}
+THERMAL = {"j1j2_chain12": ["j1j2_chain12/api/thermal/exact/auto", "j1j2_chain12/api/thermal/ftlm/auto"],
+           "square4x3": ["square4x3/api/thermal/exact/auto", "square4x3/api/thermal/exact/none"],
+           "tri_chiral4x3": ["tri_chiral4x3/api/thermal/exact/auto", "tri_chiral4x3/api/thermal/exact/none"]}
 
 # T = 0 dynamics of S^z(q = pi) = N^-1/2 sum_i e^{i pi i} S^z_i on 41 frequencies in [-1, 4], eta 0.15, Krylov 80
 # (the golden harness's dynamics case, tests/python/golden/cases.py:175-190), with and without symmetry sectors
@@ -85,6 +128,12 @@ def main(ref_root: str, json_only: bool = False):
             "n_sites": N,
             "products": [[o, list(s), [complex(c).real, complex(c).imag]] for o, s, c in prods()],
             "records": {k: recs[k]["values"]["energies"] for k in keys},
+        }
+    for name, (N, prods) in ZOO2D.items():
+        golden["models"][name] = {
+            "n_sites": N,
+            "products": [[o, list(s), [complex(c).real, complex(c).imag]] for o, s, c in prods()],
+            "records": {},
         }
     # the N = 12 Heisenberg ring, k = 0 (a textbook value; the reference's k = 1 lane reproduces it)
     golden["known"]["heis12_k0_e0"] = -5.387390917445

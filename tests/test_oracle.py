@@ -157,6 +157,40 @@ def test_golden_exact_thermodynamics(golden):
             np.testing.assert_allclose(tot[q], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=f"{key} {q}")
 
 
+@pytest.mark.parametrize("model", ["square4x3", "tri_chiral4x3"])
+def test_golden_exact_thermodynamics_2d(golden, model):
+    """The whole spectrum of a 12-site torus model -- the square lattice's Heisenberg model, the triangular
+    lattice's with next-nearest exchange and scalar chirality (three-body terms) -- rebuilt block by block (each
+    S^z block densely, with the trivial group), traced exactly and combined in log space, equals the
+    reference's golden exact thermodynamics (with and without its symmetry sectors): E, C, S within 1e-10."""
+    g = golden["models"][model]
+    N = g["n_sites"]
+    prods = [(o, tuple(s), complex(c[0], c[1])) for o, s, c in g["products"]]
+    prog = ops.row_program(ops.from_products(N, prods))
+    recs = golden["thermal"][model]
+    T = np.asarray(next(iter(recs.values()))["T"])
+    betas = 1.0 / T
+    curves, n_states = [], 0
+    for n_up in range(N + 1):
+        spec = lat.SectorSpec(n_sites=N, n_up=n_up, perms=np.arange(N, dtype=np.int32)[None, :],
+                              chars=np.array([1.0 + 0.0j]))
+        lv = _sector_spectrum(spec, prog)
+        n_states += len(lv)
+        e0 = lv.min()
+        w = np.exp(-np.outer(betas, lv - e0))
+        z = w.sum(axis=1)
+        m1 = (w * (lv - e0)).sum(axis=1) / z
+        m2 = (w * (lv - e0) ** 2).sum(axis=1) / z
+        curves.append({"lnZ": np.log(z) - betas * e0, "E": e0 + m1, "V": np.maximum(m2 - m1 * m1, 0.0)})
+    assert n_states == 2 ** N
+    tot = O.combine_blocks(curves, betas)
+    for key, rec in recs.items():
+        assert np.allclose(rec["T"], T)
+        for q in ("E", "C", "S"):
+            ref = np.asarray(rec[q])
+            np.testing.assert_allclose(tot[q], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=f"{key} {q}")
+
+
 def test_golden_t0_dynamics(golden):
     """The T = 0 S^z(pi) spectrum of the J1-J2 chain N = 12 equals the reference's golden records (tier exact,
     1e-10): for each ground state -- this chain sits at the Majumdar-Ghosh point, so its ground manifold is the
