@@ -206,7 +206,7 @@ int qb_ground_state(const qb_sector* sec, const qb_program* prog, int max_steps,
                     int* certified, void* vec_device, double* vec_host, int* matvecs);
 
 /* The k > 1 lane (krylov_schur_lane, src/engine/block_solve.cpp:433-510, over krylov_schur_kernel,
- * include/ed/krylov/krylov_schur.h:95-330): thick-restart Krylov-Schur with full CGS2 from
+ * include/ed/krylov/krylov_schur.h:95-312): thick-restart Krylov-Schur with full CGS2 from
  * staged_seed(0x51ED0B70), cycles of min(2k + 60, 2p + 20, n) vectors keeping p = k + max(k/2, 8), lock
  * tolerance 1e-10 * scale, fresh deflated starts after an invariant subspace, and the degeneracy probe.
  * values: the k lowest, ascending (NaN past n_found). max_iter: matvec budget (0: max(200k, 2000)).

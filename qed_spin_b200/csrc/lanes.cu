@@ -6,7 +6,7 @@
 //                    on the way or from a replay of the recurrence, then H u: the Rayleigh quotient and
 //                    the residual; restarted from u until ||H u - E u|| <= 1e-9 * scale.
 //   qb_eigs_k        the k > 1 lane (krylov_schur_lane, block_solve.cpp:433-510, over krylov_schur_kernel,
-//                    include/ed/krylov/krylov_schur.h:95-330): thick-restart Krylov-Schur with full CGS2,
+//                    include/ed/krylov/krylov_schur.h:95-312): thick-restart Krylov-Schur with full CGS2,
 //                    exact pairs of an invariant subspace kept, fresh deflated starts, a degeneracy probe.
 //   qb_dynamics_t0   T = 0 dynamics of a cross-sector operator (src/engine/dynamics.cpp:442-566): the
 //                    source's ground state, phi = O psi0 on the target sector, the continued fraction of
@@ -484,7 +484,7 @@ KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std:
         if (found_vals.size() < k) fresh_seed(fresh_gen);
     }
     bool converged = !stalled && found_vals.size() >= k;
-    // the degeneracy probe (krylov_schur.h:296-318)
+    // the degeneracy probe (krylov_schur.h:272-302)
     if (!found_vals.empty() && !exhausted) {
         std::mt19937_64 probe_gen(0xDE6E4E7AULL);
         for (std::size_t round = 0; round < k; ++round) {
