@@ -239,6 +239,47 @@ def test_golden_t0_dynamics(golden):
         np.testing.assert_allclose(total, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=key)
 
 
+def _translation_invariant_models(N, seed):
+    """Translation-invariant N-site rings: Heisenberg with next-nearest exchange, XXZ in a field, Heisenberg
+    with scalar chirality (three-body terms), and random complex exchange (the same couplings on every bond, so
+    translations stay a symmetry; no time reversal)."""
+    rng = np.random.default_rng(seed)
+    ring = lat.chain_bonds(N)
+    c = complex(rng.normal(), rng.normal()) * 0.5
+    jz = float(rng.normal())
+    rand = []
+    for i, j in ring:
+        rand += [("+-", (i, j), c), ("-+", (i, j), np.conj(c)), ("zz", (i, j), complex(jz))]
+    return {
+        "j1j2": ops.heisenberg_products(ring) + ops.heisenberg_products(lat.chain_bonds(N, 2), 0.4),
+        "xxz_field": ops.xxz_products(ring, 1.0, 0.6) + ops.zeeman_z_products(N, 0.3),
+        "chiral": ops.heisenberg_products(ring) + ops.chiral_products([(i, (i + 1) % N, (i + 2) % N)
+                                                                       for i in range(N)], 0.7),
+        "random_complex": rand,
+    }
+
+
+@pytest.mark.parametrize("N", [8, 9])
+def test_momentum_blocks_tile_the_spectrum(N):
+    """For a translation-invariant ring, the spectra of the N momentum blocks of a fixed S^z, each built by the
+    oracle's sector walk (representatives, characters, 1/norms, phases), together equal the spectrum of the
+    whole S^z block built by the same walk with the trivial group (no characters, phases or norms): every level,
+    with multiplicity, within 1e-12 of the coupling scale (the reference checks every sector lane against the dense block of H the same way,
+    tests/unit/test_row_walk.cpp:386-481)."""
+    for name, prods in _translation_invariant_models(N, seed=N).items():
+        H = ops.from_products(N, prods)
+        prog = ops.row_program(H)
+        scale = sum(abs(c) for _, _, c in prods)
+        for n_up in range(N + 1):
+            levels = np.sort(np.concatenate([_sector_spectrum(lat.chain_sector(N, n_up, k), prog) for k in range(N)]))
+            states = [s for s in range(1 << N) if bin(s).count("1") == n_up]
+            full = lat.SectorSpec(n_sites=N, n_up=n_up, perms=np.arange(N, dtype=np.int32)[None, :],
+                                  chars=np.array([1.0 + 0.0j]))
+            direct = _sector_spectrum(full, prog)
+            assert len(levels) == len(direct) == len(states), (name, n_up)
+            np.testing.assert_allclose(levels, direct, rtol=0, atol=1e-12 * scale, err_msg=f"{name} n_up={n_up}")
+
+
 def test_sublattice_engagement():
     """The key order engages exactly where the reference's relaxed rule does (sublattice_code.h:23-34)."""
     assert O.Sector(lat.chain_sector(20, 1, 0)).sublattice() is None
