@@ -280,6 +280,43 @@ def test_momentum_blocks_tile_the_spectrum(N):
             np.testing.assert_allclose(levels, direct, rtol=0, atol=1e-12 * scale, err_msg=f"{name} n_up={n_up}")
 
 
+def test_flip_and_torus_blocks_tile_the_spectrum():
+    """Two more abelian groups whose one-dimensional irreps tile a fixed-S^z space: the ring's translations times
+    the spin flip at half filling (momentum x flip parity, on the flip-symmetric J1-J2 and XXZ rings; the flip
+    enters as an XOR mask of every element), and the translations of a 4x2 square torus (momentum (kx, ky), on
+    the J1-J2 model). The blocks' spectra together equal the whole S^z block's, within 1e-12 of the scale."""
+    def check(N, n_up, prog, scale, specs, what):
+        levels = np.sort(np.concatenate([_sector_spectrum(sp, prog) for sp in specs]))
+        full = lat.SectorSpec(n_sites=N, n_up=n_up, perms=np.arange(N, dtype=np.int32)[None, :],
+                              chars=np.array([1.0 + 0.0j]))
+        direct = _sector_spectrum(full, prog)
+        assert len(levels) == len(direct), what
+        np.testing.assert_allclose(levels, direct, rtol=0, atol=1e-12 * scale, err_msg=what)
+
+    N = 8
+    flip_symmetric = {"j1j2": _translation_invariant_models(N, seed=3)["j1j2"],
+                      "xxz": ops.xxz_products(lat.chain_bonds(N), 1.0, 0.6)}   # no field: the flip stays a symmetry
+    for name, prods in flip_symmetric.items():
+        prog = ops.row_program(ops.from_products(N, prods))
+        perms, flips = lat.with_spin_flip(lat.chain_translations(N), N)
+        specs = [lat.SectorSpec(N, N // 2, perms, np.concatenate([lat.momentum_chars(N, k),
+                                                                  par * lat.momentum_chars(N, k)]), flips)
+                 for k in range(N) for par in (1.0, -1.0)]
+        check(N, N // 2, prog, sum(abs(c) for _, _, c in prods), specs, f"{name} with the flip")
+
+    Lx, Ly = 4, 2
+    nn, nnn = lat.square_j1j2_bonds(Lx, Ly)
+    prods = ops.heisenberg_products(nn) + ops.heisenberg_products(nnn, 0.5)
+    prog = ops.row_program(ops.from_products(Lx * Ly, prods))
+    perms = lat.square_translations(Lx, Ly)
+    a = np.array([e % Lx for e in range(Lx * Ly)])
+    b = np.array([e // Lx for e in range(Lx * Ly)])
+    for n_up in (2, 3, 4):
+        specs = [lat.SectorSpec(Lx * Ly, n_up, perms, np.exp(-2j * np.pi * (kx * a / Lx + ky * b / Ly)))
+                 for kx in range(Lx) for ky in range(Ly)]
+        check(Lx * Ly, n_up, prog, sum(abs(c) for _, _, c in prods), specs, f"4x2 torus n_up={n_up}")
+
+
 def test_sublattice_engagement():
     """The key order engages exactly where the reference's relaxed rule does (sublattice_code.h:23-34)."""
     assert O.Sector(lat.chain_sector(20, 1, 0)).sublattice() is None
