@@ -240,9 +240,11 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
             int n_beta, int dtype, double* lnZ, double* E, double* V, double* e_min);
 
 /* FTLM over many blocks, the sampled per-block path of the thermal driver (src/engine/thermal.cpp:155-340
- * over the blocks of one call): every block uses the call's base seed, so sample s of block b is the first
- * dim_b draws of sample_engine(seed, s) (thermal.cpp:363, sample_seed.h:37-89); one table of those streams,
- * drawn once, serves every block. Blocks run largest first on a few streams; each block's samples advance
+ * over the blocks of one call): every block uses the call's seed, so sample s of block b is the first dim_b
+ * draws of sample_engine(seed, s) (sample_seed.h:37-89); one table of those streams, drawn once, serves every
+ * block. (The reference's driver advances the seed by a 64-bit LCG step before each sampled block,
+ * thermal.cpp:470-471: a one-block call given the advanced seed draws its vectors exactly; over many blocks the
+ * two agree in distribution, not draw for draw.) Blocks run largest first on a few streams; each block's samples advance
  * together as one block matvec, on the block's reduced CSR (built inside the call) when use_csr != 0 and it
  * fits, else on the row walk. Outputs per block b and beta t at [b * n_beta + t]: lnZ, E, V; e_min[b].
  * stats (NULL or 4 doubles): seconds spent drawing the samples, building the CSRs, running the recurrences,

@@ -53,11 +53,13 @@ namespace qb {
 namespace {
 
 // ---- FTLM: sample tables, the block recurrence of one sector's samples, the curves ----
-// The sample vectors of a call: sample s of every block is the first n_b draws of sample_engine(seed, s)
-// (the reference gives every block of a thermal call the same base seed, src/engine/thermal.cpp:363, and
-// draws a block's vector as gaussian_vector(n_b, gen), include/ed/thermal/sample_seed.h:84-89). So one table
-// of k streams, as long as the largest block, holds every block's samples as prefixes; a block normalises its
-// prefix. The table is drawn on host threads with the reference's own generator and distribution.
+// The sample vectors of a call: sample s of every block is the first n_b draws of sample_engine(seed, s), drawn
+// as the reference draws a block's vector (gaussian_vector(n_b, gen), include/ed/thermal/sample_seed.h:84-89). So
+// one table of k streams, as long as the largest block, holds every block's samples as prefixes; a block
+// normalises its prefix. The table is drawn on host threads with the reference's own generator and distribution.
+// The reference's thermal driver instead advances the seed by a 64-bit LCG step before each sampled block
+// (src/engine/thermal.cpp:470-471), so its blocks draw distinct streams: a one-block call given the advanced
+// seed draws exactly the reference's vectors; over many blocks the two agree in distribution, not draw for draw.
 std::vector<std::complex<double>> sample_table(std::uint64_t seed, int k, std::uint64_t len) {
     std::vector<std::complex<double>> G(static_cast<std::size_t>(k) * len);
     auto draw = [&](int s) {

@@ -96,6 +96,10 @@ THERMAL = {"j1j2_chain12": ["j1j2_chain12/api/thermal/exact/auto", "j1j2_chain12
            "square4x3": ["square4x3/api/thermal/exact/auto", "square4x3/api/thermal/exact/none"],
            "tri_chiral4x3": ["tri_chiral4x3/api/thermal/exact/auto", "tri_chiral4x3/api/thermal/exact/none"]}
 
+# FTLM without symmetry sectors: one block of all 2^12 states, 8 samples, Krylov 40, seed 11 (the golden
+# harness's thermal case, tests/python/golden/cases.py:142-162)
+SAMPLED = {"j1j2_chain12": "j1j2_chain12/api/thermal/ftlm/none"}
+
 # T = 0 dynamics of S^z(q = pi) = N^-1/2 sum_i e^{i pi i} S^z_i on 41 frequencies in [-1, 4], eta 0.15, Krylov 80
 # (the golden harness's dynamics case, tests/python/golden/cases.py:175-190), with and without symmetry sectors
 DYNAMICS = {"j1j2_chain12": ["j1j2_chain12/api/dynamics/T=0/auto/SzQ", "j1j2_chain12/api/dynamics/T=0/none/SzQ"]}
@@ -141,6 +145,11 @@ def main(ref_root: str, json_only: bool = False):
     for name, keys in THERMAL.items():
         golden["thermal"][name] = {k: {q: recs[k]["values"][q] for q in ("T", "E", "C", "S")} | {"tier": recs[k]["tier"]}
                                    for k in keys}
+    golden["thermal_sampled"] = {}
+    for name, key in SAMPLED.items():
+        golden["thermal_sampled"][name] = {"record": key, "samples": 8, "krylov": 40, "seed": 11,
+                                           "tier": recs[key]["tier"]} | {q: recs[key]["values"][q]
+                                                                         for q in ("T", "E", "C", "S")}
     golden["dynamics"] = {}
     for name, keys in DYNAMICS.items():
         golden["dynamics"][name] = {"omega": [-1.0, 4.0, 41], "eta": 0.15, "krylov": 80, "q": "pi",

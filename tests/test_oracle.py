@@ -191,6 +191,61 @@ def test_golden_exact_thermodynamics_2d(golden, model):
             np.testing.assert_allclose(tot[q], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=f"{key} {q}")
 
 
+def test_golden_sampled_ftlm(golden):
+    """The reference's golden FTLM record of the J1-J2 chain N = 12 without symmetry sectors -- one block of all
+    4096 states, 8 samples, Krylov 40, seed 11 -- reproduced within 1e-10: the block's seed is the call's seed
+    advanced once by the thermal driver's 64-bit LCG step (src/engine/thermal.cpp:470-471); sample s is the
+    oracle's restatement of sample_engine(seed, s) (include/ed/thermal/sample_seed.h:37-89); the Lanczos run keeps
+    the local reorthogonalisation against the previous vector (include/ed/krylov/lanczos.h:189-193); the oracle's
+    sample moments, then the samples combined about their least minimum (include/ed/thermal/ftlm.h:199-235)."""
+    g = golden["models"]["j1j2_chain12"]
+    N = g["n_sites"]
+    prods = [(o, tuple(s), complex(c[0], c[1])) for o, s, c in g["products"]]
+    H = ops.from_products(N, prods).to_dense()
+    rec = golden["thermal_sampled"]["j1j2_chain12"]
+    T = np.asarray(rec["T"])
+    betas = 1.0 / T
+    k, depth, n = rec["samples"], rec["krylov"], H.shape[0]
+    seed = (rec["seed"] * 6364136223846793005 + 1442695040888963407) % (1 << 64)
+    moms = []
+    for s in range(k):
+        v = O.sample_vector(seed, s, n)
+        v = v / np.linalg.norm(v)
+        vp = np.zeros_like(v)
+        alpha, beta = [], [0.0]
+        for j in range(depth):
+            w = H @ v - beta[-1] * vp
+            a = np.vdot(v, w).real
+            w = w - a * v
+            o = np.vdot(v, w)
+            if j > 0 and abs(o) > 1.49011611938476562e-08:
+                w = w - o * v
+            b = np.linalg.norm(w)
+            alpha.append(a)
+            beta.append(b)
+            vp, v = v, w / b
+        moms.append(O.sample_moments(alpha, beta, betas))
+    e_ref = min(m[0] for m in moms)
+    E, C, S = [], [], []
+    for t, bt in enumerate(betas):
+        zz = e1 = e2 = 0.0
+        for em, Z, E1, E2 in moms:
+            dd = em - e_ref
+            r = np.exp(-bt * dd)
+            zz += Z[t] * r
+            e1 += (E1[t] + dd * Z[t]) * r
+            e2 += (E2[t] + 2.0 * dd * E1[t] + dd * dd * Z[t]) * r
+        zz, e1, e2 = zz / k, e1 / k, e2 / k
+        m1, m2 = e1 / zz, e2 / zz
+        lnZ = np.log(n) + np.log(zz) - bt * e_ref
+        E.append(e_ref + m1)
+        C.append(bt * bt * (m2 - m1 * m1))
+        S.append(lnZ + bt * (e_ref + m1))
+    for q, got in (("E", E), ("C", C), ("S", S)):
+        ref = np.asarray(rec[q])
+        np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max(), err_msg=q)
+
+
 def test_golden_t0_dynamics(golden):
     """The T = 0 S^z(pi) spectrum of the J1-J2 chain N = 12 equals the reference's golden records (tier exact,
     1e-10): for each ground state -- this chain sits at the Majumdar-Ghosh point, so its ground manifold is the
