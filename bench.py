@@ -1,18 +1,22 @@
 """Benchmark of the symmetry-sector matvec and its Lanczos recurrence on B200.
 
-Workload: the periodic XXZ chain N = 32 (J = 1, Delta = 0.7) in the sector S^z = 0, k = 0, reflection-even,
-spin-flip-even (group D_32 x Z_2, 128 elements; 4,707,969 representatives found on the device). Synthetic
-input: a seeded complex Gaussian vector. One step = one H.v on device-resident vectors with FP32 storage
-(FP64 arithmetic) through the lane the engine picks for a sector whose merged CSR fits the device: the
-reduced CSR, built once on the device from the row walk (its build time is reported). The on-the-fly walk,
-the FP64-storage applies and time-to-E0 (FP64 plain vs FP32 storage + FP64 refinement) are reported beside it.
+Workload (the default line): the 6x6 periodic square lattice, J1-J2 Heisenberg (J1 = 1 on the 72 nearest-
+neighbour bonds, J2 = 0.5 on the 72 diagonal bonds), sector S^z = 0, momentum (0, 0) under the 36 translations
+(252,091,362 representatives, uint64 states, found on the device). Synthetic input: a seeded complex Gaussian
+vector. One step = one H.v on device-resident vectors with FP32 storage (FP64 arithmetic) through the lane the
+engine picks for a sector whose merged CSR fits the device: the reduced CSR, built once on the device from the row
+walk (its build time is reported). Reported beside it: the FP64-storage apply, the on-the-fly walk, e2e through
+qb_lanczos with host buffers, time-to-E0 (FP64 CSR, FP32 CSR + FP64 refinement, the plain FP64 walk), and the
+XXZ chain N = 32 sector (4,707,969 states) as a secondary workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 N > 1 runs N independent replicas (one process per GPU, launched by torchrun): the path has no
 cross-GPU exchange, so the metric is the sum over replicas and the time the max over ranks.
-`--impl reference` times the reference engine's own CPU matvec (oracle/_ref) on the host cores: its
-default host lane, the merged reduced CSR (built once, outside the timed region) and its OpenMP spmv.
+`--impl reference` times the reference engine's own CPU matvec (oracle/_ref) on the host cores on the same
+sector: its host lane for a real sector whose CSR fits host memory (the merged reduced CSR, applied to real
+vectors), on a bounded sample of the rows (four contiguous blocks of 1/256 of the rows each, built outside the
+timed region), scaled to one whole H.v.
 """
 from __future__ import annotations
 
@@ -41,7 +45,18 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def sq36_workload():
+    """6x6 J1-J2 (J1 = 1, J2 = 0.5), S^z = 0 (18 up), momentum (0, 0) under the 36 translations."""
+    from qed_spin_b200 import lattice as lat
+    from qed_spin_b200 import operators as ops
+    nn, nnn = lat.square_j1j2_bonds(6, 6)
+    spec = lat.square_k0_sector(6, 6, 18)
+    prods = ops.heisenberg_products(nn, 1.0) + ops.heisenberg_products(nnn, 0.5)
+    return spec, ops.row_program(ops.from_products(36, prods)), prods
+
+
 def workload():
+    """XXZ chain N = 32 (J = 1, Delta = 0.7), S^z = 0, k = 0, reflection-even, flip-even (D32 x Z2)."""
     from qed_spin_b200 import lattice as lat
     from qed_spin_b200 import operators as ops
     N = 32
@@ -51,13 +66,20 @@ def workload():
     return spec, prog, prods
 
 
-# DRAM bytes (read + write) of one spmv1<complex64> launch on this workload, measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch, cold L2).
-SPMV1_CHAIN32_DRAM_BYTES = 596.873472e6 + 38.907392e6
+CONFIG = {"workload": "6x6 periodic square J1-J2 Heisenberg, J1=1 J2=0.5, Sz=0, momentum (0,0) under the 36 "
+                      "translations", "n_sites": 36, "n_up": 18, "group_size": 36}
+CHAIN32 = "XXZ chain N=32 J=1 Delta=0.7, Sz=0 k=0 reflection-even flip-even (D32 x Z2)"
 
-CONFIG = {"workload": "XXZ chain N=32 J=1 Delta=0.7, Sz=0 k=0 reflection-even flip-even (D32 x Z2)",
-          "n_sites": 32, "group_size": 128}
+# The reference arm's sample of the 6x6 sector: SQ36_BLOCKS contiguous blocks of dim / SQ36_BLOCK_DIV rows each,
+# centred at (2i + 1) / (2 SQ36_BLOCKS) of the row range.
+SQ36_BLOCKS, SQ36_BLOCK_DIV = 4, 256
 
+
+
+# DRAM bytes (read + write) of one spmv1<complex64> launch on the 6x6 workload (None: not captured); the source says how
+# the figure was taken.
+SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH = None
+SPMV1_SQ36_TRAFFIC_SOURCE = "not captured"
 
 class Clocks:
     """SM clock, power and clock-event-reason samples (NVML, read only) taken every 10 ms while the timed
@@ -147,6 +169,8 @@ class Clocks:
                 "samples": len(sm), "power_w_median": statistics.median(pw) if pw else None, "source": "NVML"}
 
 
+
+
 def dist_init():
     from qed_spin_b200 import replicas
     return replicas.init("nccl")
@@ -162,25 +186,61 @@ def barrier(world):
     replicas.barrier(world)
 
 
-def _reference_lane(threads):
-    """The reference engine on the workload: its sector, its row program and its merged reduced CSR (the
-    host lane RepSectorMatVec applies through), with the build times."""
+def reference_sq36(steps: int, warmup: int, threads: int) -> dict:
+    """The reference engine's host lane on the 6x6 sector, on the host cores: its own orbit scan builds the sector,
+    its build_cross_csr the merged rows of SQ36_BLOCKS contiguous row blocks (outside the timed region), and each
+    step applies those rows to a real vector through RealCsrView::spmv -- the lane RepSectorMatVec takes for a real
+    sector of a real H (is_real, with_backend). A step's time scaled by dim / (rows sampled) is one whole H.v."""
     from oracle import ref as R
-    spec, prog, prods = workload()
+    spec, _, prods = sq36_workload()
     R.set_threads(threads)
-    t0 = time.time()
+    t0 = time.perf_counter()
     rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
-    sector_s = time.time() - t0
+    scan_s = time.perf_counter() - t0
+    n = rs.dim
     rp = R.Operator(spec.n_sites, prods).row_program()
-    t0 = time.time()
-    csr = R.Csr(rs, rp)
-    csr_s = time.time() - t0
-    return rs, rp, csr, sector_s, csr_s
+    B = n // SQ36_BLOCK_DIV
+    t0 = time.perf_counter()
+    blocks = []
+    for i in range(SQ36_BLOCKS):
+        r0 = (2 * i + 1) * n // (2 * SQ36_BLOCKS) - B // 2
+        blocks.append(R.Csr(rs, rp, rows=(r0, B)))
+    build_s = time.perf_counter() - t0
+    nnz = sum(b.nnz for b in blocks)
+    x = np.random.default_rng(1).normal(size=n)
+    ys = [np.zeros(B) for _ in blocks]
+    real = all(b.spmv_real(x, y) for b, y in zip(blocks, ys))
+    assert real, "the 6x6 k=0 sector of the J1-J2 model is real"
+    for _ in range(warmup):
+        for b, y in zip(blocks, ys):
+            b.spmv_real(x, y)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        for b, y in zip(blocks, ys):
+            b.spmv_real(x, y)
+        times.append(time.perf_counter() - t)
+    rows = SQ36_BLOCKS * B
+    per_hv = sum(times) / steps * n / rows
+    # the complex lane on the same rows (the reference's device-less lane for a complex sector), for context
+    xc = (x + 1j * np.random.default_rng(2).normal(size=n)).astype(np.complex128)
+    yc = [np.zeros(B, np.complex128) for _ in blocks]
+    t = time.perf_counter()
+    for b, y in zip(blocks, yc):
+        b.spmv(xc, y)
+    per_hv_c = (time.perf_counter() - t) * n / rows
+    for b in blocks:
+        b.close()
+    return {"value": 1.0 / per_hv, "unit": "H.v/s", "cores": threads, "kind": "reference",
+            "sample": f"{SQ36_BLOCKS} contiguous blocks of {B} rows ({rows} of {n} rows, {nnz} merged entries), "
+                      f"{steps} timed applies through RealCsrView::spmv (real vectors), scaled by dim / rows",
+            "dim": n, "ms_per_hv": 1e3 * per_hv, "complex_lane_hv_per_s": 1.0 / per_hv_c,
+            "scan_s": scan_s, "block_csr_build_s": build_s, "sample_nnz": nnz}
 
 
 def run_reference(args, world, rank):
-    """The reference engine's own CPU matvec (oracle/_ref) on the host cores: H.v/s on the same workload,
-    through its default host lane (ReducedSymmetryCsr::spmv over the CSR build_sector_csr made)."""
+    """The reference engine's own CPU matvec (oracle/_ref) on the host cores, rank 0 only: H.v/s on the 6x6
+    sector through its host CSR lane, on the row sample described in reference_sq36."""
     if rank != 0:
         return None
     from oracle import ref as R
@@ -188,64 +248,82 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU engine was not built into oracle/_ref"}))
         return None
     threads = os.cpu_count() or 1
-    rs, rp, csr, sector_s, csr_s = _reference_lane(threads)
-    x = R.staged_seed(1, rs.dim)
-    y = np.zeros(rs.dim, np.complex128)
-    for _ in range(args.warmup):
-        csr.spmv(x, y)
-    times = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        csr.spmv(x, y)
-        times.append(time.perf_counter() - t)
-    tot = sum(times)
-    v = args.steps / tot
+    r = reference_sq36(args.steps, args.warmup, threads)
+    v = r["value"]
     line = {"impl": "reference", "metric": "H.v/s", "value": v, "unit": "H.v/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_hv"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CONFIG, dim=rs.dim, nnz=csr.nnz, csr_bytes=csr.bytes,
-                           lane="reduced CSR (build_sector_csr + ReducedSymmetryCsr::spmv, OpenMP)"),
-            "cpu_baseline": {"value": v, "unit": "H.v/s", "cores": threads, "kind": "reference",
-                             "sample": f"{args.steps} full H.v on the {rs.dim}-state sector"},
+            "config": dict(CONFIG, dim=r["dim"], lane="host reduced CSR on real vectors (build_cross_csr + "
+                                                        "RealCsrView::spmv, OpenMP), sampled rows"),
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": v, "unit": "H.v/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_sector_build_s": sector_s, "reference_csr_build_s": csr_s}
+            "reference_detail": {k: r[k] for k in ("complex_lane_hv_per_s", "scan_s", "block_csr_build_s",
+                                                   "sample_nnz")}}
     print(json.dumps(line))
     return line
 
 
-def cpu_baseline_sample(dim_gpu):
-    """The reference engine's CPU matvec on a bounded sample: full H.v through its reduced CSR for about
-    10 s, plus a few through its on-the-fly host walk (sector_gather)."""
+def reference_chain32(threads: int) -> dict:
+    """The reference engine's host lane on the chain-32 sector: its merged CSR built whole, applied to real vectors
+    (RealCsrView::spmv) for about 10 s, and once to complex ones."""
     from oracle import ref as R
-    if not R.available():
-        return None
-    threads = os.cpu_count() or 1
-    rs, rp, csr, sector_s, csr_s = _reference_lane(threads)
-    assert rs.dim == dim_gpu
-    x = R.staged_seed(1, rs.dim)
-    y = np.zeros(rs.dim, np.complex128)
-    csr.spmv(x, y)
+    spec, _, prods = workload()
+    R.set_threads(threads)
+    rs = R.Sector(spec.n_sites, spec.n_up, spec.perms, spec.chars, flips=spec.flips, slc_mode=-1)
+    rp = R.Operator(spec.n_sites, prods).row_program()
+    t0 = time.perf_counter()
+    csr = R.Csr(rs, rp)
+    csr_s = time.perf_counter() - t0
+    x = np.random.default_rng(1).normal(size=rs.dim)
+    y = np.zeros(rs.dim)
+    assert csr.spmv_real(x, y)
     n, t0 = 0, time.perf_counter()
     while n < 3 or (time.perf_counter() - t0 < 10.0 and n < 200):
-        csr.spmv(x, y)
+        csr.spmv_real(x, y)
         n += 1
     dt = time.perf_counter() - t0
+    xc = (x + 1j * x[::-1]).astype(np.complex128)
+    yc = np.zeros(rs.dim, np.complex128)
     t = time.perf_counter()
-    rs.gather(rp, x)
-    walk_s = time.perf_counter() - t
+    csr.spmv(xc, yc)
+    c_s = time.perf_counter() - t
+    csr.close()
     return {"value": n / dt, "unit": "H.v/s", "cores": threads, "kind": "reference",
-            "sample": f"{n} full H.v through the reference's reduced CSR (its default host lane) on the "
-                      f"{rs.dim}-state sector",
-            "csr_build_s": csr_s, "sector_build_s": sector_s, "walk_hv_per_s": 1.0 / walk_s}
+            "sample": f"{n} whole H.v through the reference's reduced CSR on real vectors (its host lane for a real "
+                      f"sector) on the {rs.dim}-state sector", "csr_build_s": csr_s,
+            "complex_lane_hv_per_s": 1.0 / c_s}
+
+
+def time_applies(fn, steps, warm, stream, world):
+    """Device time per call of fn (CUDA events on `stream`, after `warm` untimed calls), max over ranks."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    barrier(world)
+    return dist_max(ms, world) / steps
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e0", action="store_true", help="leave the 6x6 time-to-E0 runs out of the line")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="leave the chain-32, k > 1, FTLM and served-stream measurements out of the line")
     ap.add_argument("--no-ftlm", action="store_true", help="leave the batched FTLM measurement out of the line")
     ap.add_argument("--ftlm", action="store_true",
                     help="batched FTLM over the 600 blocks of the XXZ chain N=24 (every S^z x 24 momenta), one "
@@ -255,12 +333,11 @@ def main():
                          "N = 16..30): p50/p99 latency and solves/s of the server against one solve at a time")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--no-serve", action="store_true", help="leave the served-stream measurement out of the line")
-    ap.add_argument("--e0-6x6", action="store_true",
-                    help="time-to-E0 on the 6x6 J1-J2 k=(0,0) sector: the plain FP64 walk against the CSR lane "
-                         "(FP64, and FP32 storage + FP64 refinement), one JSON line")
-    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36", "ftlm4", "chain20"], default=None,
+    ap.add_argument("--profile-case", choices=["chain32", "sq30", "sq36", "sq36n11", "sq36n12", "ftlm4", "chain20"],
+                    default=None,
                     help="profiling run: build one sector and apply H (complex64) warmup + steps times, print timing; "
-                         "ftlm4: batched FTLM (40 samples, depth 100) on the four largest N = 24 XXZ blocks")
+                         "sq36n11 / sq36n12: the 6x6 J1-J2 k=0 sector at 11 / 12 up spins; ftlm4: batched FTLM (40 "
+                         "samples, depth 100) on the four largest N = 24 XXZ blocks")
     ap.add_argument("--profile-lane", choices=["walk", "csr", "c64", "c128"], default="walk",
                     help="the lane of the profiling run: the on-the-fly walk or the device reduced CSR; for ftlm4 "
                          "the storage type")
@@ -268,9 +345,6 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         profile_case(args)
-        return
-    if args.e0_6x6:
-        e0_6x6(args)
         return
     if args.ftlm:
         ftlm_config(args)
@@ -289,12 +363,14 @@ def main():
 
     from qed_spin_b200 import build
     from qed_spin_b200 import device as D
+    from qed_spin_b200 import replicas
     build.build()
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
     stream = torch.cuda.current_stream()
+    hbm, peak_kind = peaks()
 
-    spec, prog, prods = workload()
+    spec, prog, prods = sq36_workload()
     t0 = time.perf_counter()
     S = D.Sector(spec)
     torch.cuda.synchronize()
@@ -302,45 +378,10 @@ def main():
     P = D.Program(prog)
     n = S.dim
     info = S.info()
-
-    rng = np.random.default_rng(1)
-    x64 = torch.from_numpy(rng.normal(size=n) + 1j * rng.normal(size=n)).to(dev)
-    x32 = x64.to(torch.complex64)
-    y32 = torch.empty_like(x32)
-    y64 = torch.empty_like(x64)
-    e_bar = emitted_per_row(S.reps()[0], prog)
-    hbm, peak_kind = peaks()
-
-    def time_apply(x, y, dt, steps, warm):
-        for _ in range(warm):
-            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
-        torch.cuda.synchronize()
-        barrier(world)
-        torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(steps):
-            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        barrier(world)
-        return dist_max(ms, world) / steps
-
-    # the on-the-fly walk: 8 rep + 8 inv_norm + S_out per row, S_in per emitted entry
-    def walk_bytes(sb):
-        return n * (8 + 8 + sb) + n * e_bar * sb
-
-    walk_steps = max(5, args.steps // 10)
-    walk32 = time_apply(x32, y32, "c64", walk_steps, 3)
-    walk64 = time_apply(x64, y64, "c128", walk_steps, 3)
-
-    # time to E0 on the plain FP64 lane (the walk), before the CSR exists
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    r_plain = D.eigs_lowest(S, P, dtype="c128")
-    t_plain = time.perf_counter() - t
+    reps, _ = S.reps()
+    sample = reps[::64].copy()
+    del reps
+    e_bar = emitted_per_row(sample, prog)
 
     # the reduced CSR, built on the device from the walk, attached to the program
     torch.cuda.synchronize()
@@ -351,108 +392,202 @@ def main():
     A.attach(P)
     cinfo = A.info()
 
-    # the CSR matvec: the CSR streamed once, x read (each element at least once) and y written
-    def csr_bytes(sb):
-        return cinfo["bytes"] + 2 * n * sb
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    x32 = torch.randn(n, dtype=torch.complex64, device="cuda", generator=g)
+    y32 = torch.empty_like(x32)
+
+    def apply32():
+        D.matvec(S, S, P, [x32], [y32], dtype="c64", stream=stream)
 
     with Clocks(dev) as clk:
-        per32 = time_apply(x32, y32, "c64", args.steps, args.warmup)
-    per64 = time_apply(x64, y64, "c128", max(10, args.steps // 2), 3)
-    ach32 = csr_bytes(8) / (per32 * 1e-3) / 1e9
-    ach64 = csr_bytes(16) / (per64 * 1e-3) / 1e9
+        per32 = time_applies(apply32, args.steps, args.warmup, stream, world)
+    x64 = x32.to(torch.complex128)
+    y64 = torch.empty_like(x64)
+    per64 = time_applies(lambda: D.matvec(S, S, P, [x64], [y64], dtype="c128", stream=stream),
+                         max(3, args.steps // 4), 2, stream, world)
 
-    # end to end through the public C-ABI: host start vector in, alpha/beta out, K Lanczos steps
-    v0 = (rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex128)
-    D.lanczos(S, P, v0, 8, dtype="c64")
+    def b_alg(sb):   # the per-H.v algorithmic bytes: rep + 1/norm + y per row, one x element per emitted entry
+        return n * (8 + 8 + sb) + n * e_bar * sb
+
+    def csr_stream(sb):   # the CSR streamed once, x read once, y written once
+        return cinfo["bytes"] + 2 * n * sb
+
+    ach32 = b_alg(8) / (per32 * 1e-3) / 1e9
+    ach64 = b_alg(16) / (per64 * 1e-3) / 1e9
+
+    # end to end through the public C-ABI: a host complex128 start vector in, alpha / beta out, K Lanczos steps on
+    # FP32 storage through the attached CSR
+    v0 = x64.cpu().numpy()
+    D.lanczos(S, P, v0, 4, dtype="c64")
     torch.cuda.synchronize()
     barrier(world)
     t = time.perf_counter()
-    a, b = D.lanczos(S, P, v0, args.steps, dtype="c64")
-    e2e_s = time.perf_counter() - t
-    e2e_s = dist_max(e2e_s, world)
+    D.lanczos(S, P, v0, args.steps, dtype="c64")
+    e2e_s = dist_max(time.perf_counter() - t, world)
+    del v0
 
-    # time to E0 on the CSR lane: FP64 storage, and FP32 storage + FP64 refinement
+    # the on-the-fly walk (the CSR detached)
+    D.detach_csr(P)
+    walk32 = time_applies(apply32, 1, 1, stream, world)
+    walk64 = time_applies(lambda: D.matvec(S, S, P, [x64], [y64], dtype="c128", stream=stream), 1, 1, stream,
+                          world)
+    del x32, y32, x64, y64
     torch.cuda.synchronize()
-    t = time.perf_counter()
-    r64 = D.eigs_lowest(S, P, dtype="c128")
-    t64 = time.perf_counter() - t
-    t = time.perf_counter()
-    r32 = D.eigs_lowest(S, P, dtype="c64", refine=True)
-    t32 = time.perf_counter() - t
+
+    e0 = None
+    if not args.no_e0:
+        e0 = {}
+        A.attach(P)
+        t = time.perf_counter()
+        r = D.eigs_lowest(S, P, dtype="c128")
+        e0["csr_fp64"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"], "matvecs": r["matvecs"]}
+        t = time.perf_counter()
+        r = D.eigs_lowest(S, P, dtype="c64", refine=True)
+        e0["csr_fp32_refined"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
+                                  "matvecs": r["matvecs"], "converged": r["converged"]}
+        A.close()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = D.eigs_lowest(S, P, dtype="c128")
+        e0["plain_fp64_walk"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
+                                 "matvecs": r["matvecs"]}
+        e_ref = e0["csr_fp64"]["e0"]
+        e0["csr_build_s"] = csr_build_s
+        e0["rel_err_fp32_refined_vs_fp64"] = abs(e0["csr_fp32_refined"]["e0"] - e_ref) / abs(e_ref)
+        e0["rel_err_plain_walk_vs_csr_fp64"] = abs(e0["plain_fp64_walk"]["e0"] - e_ref) / abs(e_ref)
+        e0["speedup_fp32_refined_vs_fp64_same_lane"] = e0["csr_fp64"]["s"] / e0["csr_fp32_refined"]["s"]
+        e0["speedup_fp32_refined_incl_build_vs_plain_walk"] = e0["plain_fp64_walk"]["s"] / (
+            e0["csr_fp32_refined"]["s"] + csr_build_s)
+    A.close()
+    S.close()
+    P.close()
+    torch.cuda.synchronize()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_sample(n)
+            cpu = reference_sq36(10, 1, os.cpu_count() or 1)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"unavailable": str(e)}
-    # config 2's two lowest levels (the k > 1 lane on the CSR lane, FP64) and config 1 (chain-20, four levels)
-    levels = None
-    if rank == 0 and world == 1:
-        try:
-            levels = levels_measure(S, P, args)
-        except Exception as e:
-            levels = {"unavailable": str(e)}
-    # the served request stream, rank 0 at N = 1
-    serve = None
-    if rank == 0 and world == 1 and not args.no_serve:
-        try:
-            serve = serve_measure(args)
-        except Exception as e:
-            serve = {"unavailable": str(e)}
-    # the batched FTLM workload (every block of the N = 24 chain), rank 0 at N = 1
-    ftlm = None
-    if rank == 0 and world == 1 and not args.no_ftlm:
-        try:
-            ftlm = ftlm_measure(args, with_cpu=not args.no_cpu_baseline)
-        except Exception as e:
-            ftlm = {"unavailable": str(e)}
 
-    from qed_spin_b200 import replicas
+    secondary = {}
+    if rank == 0 and world == 1 and not args.no_secondary:
+        for key, fn in (("chain32", lambda: chain32_measure(args, stream)), ("levels", lambda: levels_measure(args)),
+                        ("ftlm", lambda: None if args.no_ftlm else ftlm_measure(args, not args.no_cpu_baseline)),
+                        ("serve", lambda: None if args.no_serve else serve_measure(args))):
+            try:
+                secondary[key] = fn()
+            except Exception as e:
+                secondary[key] = {"unavailable": str(e)}
+
     if rank != 0:
-        A.close()
         replicas.finish(world)
         return
     value = replicas.whole_job_rate(1.0, world, per32 * 1e-3)
     line = {
         "metric": "H.v/s", "value": value, "unit": "H.v/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per32, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64 arithmetic, complex64 (FP32) vector storage", "data": "synthetic",
         "config": dict(CONFIG, dim=n, lane="device reduced CSR (built from the row walk)", nnz=cinfo["nnz"],
-                       csr_bytes=cinfo["bytes"], n_dict=cinfo["n_dict"], emitted_per_row=e_bar,
+                       csr_bytes=cinfo["bytes"], n_dict=cinfo["n_dict"],
+                       emitted_per_row=e_bar, emitted_per_row_sample="every 64th representative",
                        storage="complex64 vectors, FP64 arithmetic", lookup=info["lookup"],
                        sublattice=[info["slc_L"], info["slc_m"]],
-                       l2=f"inputs larger than the 126 MB L2 (CSR {cinfo['bytes'] / 1e6:.0f} MB streamed per step), "
-                          "no flush",
+                       l2=f"inputs larger than the 126 MB L2 (CSR {cinfo['bytes'] / 1e9:.1f} GB streamed per step, "
+                          f"x {8 * n / 1e9:.2f} GB), no flush",
                        parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": hbm, "unit": "GB/s", "frac": ach32 / hbm,
-                     "traffic": SPMV1_CHAIN32_DRAM_BYTES, "traffic_source": "ncu capture of one spmv1 launch on this workload",
+                     "traffic": SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH, "traffic_source": SPMV1_SQ36_TRAFFIC_SOURCE,
                      "peak_kind": peak_kind, "kernel": "spmv1<complex64>",
-                     "alg_bytes_per_launch": csr_bytes(8)},
+                     "alg_bytes_per_launch": b_alg(8),
+                     "alg_bytes_rule": "D*(8 rep + 8 inv_norm + 8 y) + D*e_bar*8 (one complex64 x element per "
+                                       "emitted entry)",
+                     "csr_stream_bytes_per_launch": csr_stream(8),
+                     "csr_stream_frac": csr_stream(8) / (per32 * 1e-3) / 1e9 / hbm},
         "fp64": {"ms_per_hv": per64, "hv_per_s": 1e3 / per64, "achieved_gbs": ach64, "frac": ach64 / hbm},
         "csr_build_s": csr_build_s,
-        "walk": {"ms_per_hv_fp32": walk32, "hv_per_s_fp32": 1e3 / walk32, "ms_per_hv_fp64": walk64,
-                 "achieved_gbs_fp32": walk_bytes(8) / (walk32 * 1e-3) / 1e9,
-                 "frac_fp32": walk_bytes(8) / (walk32 * 1e-3) / 1e9 / hbm},
-        "e2e": {"value": world * args.steps / e2e_s, "unit": "H.v/s", "h2d_bytes_per_step": 16 * n / args.steps,
-                "d2h_bytes_per_step": 16, "path": "qb_lanczos (host v0 in, alpha/beta out, FP32 storage, CSR lane)"},
-        "time_to_e0": {"plain_fp64_walk_s": t_plain, "plain_e0": r_plain["e0"], "plain_iters": r_plain["iters"],
-                       "csr_build_s": csr_build_s,
-                       "csr_fp64_s": t64, "csr_fp64_e0": r64["e0"],
-                       "csr_fp32_refined_s": t32, "csr_fp32_refined_e0": r32["e0"], "fp32_matvecs": r32["matvecs"],
-                       "rel_err_vs_plain": abs(r32["e0"] - r_plain["e0"]) / abs(r_plain["e0"]),
-                       "speedup_vs_plain_incl_build": t_plain / (t32 + csr_build_s)},
         "enumeration_s": enum_s,
+        "walk": {"ms_per_hv_fp32": walk32, "ms_per_hv_fp64": walk64, "hv_per_s_fp32": 1e3 / walk32,
+                 "frac_fp32": b_alg(8) / (walk32 * 1e-3) / 1e9 / hbm},
+        "e2e": {"value": world * args.steps / e2e_s, "unit": "H.v/s", "h2d_bytes_per_step": 16 * n / args.steps,
+                "d2h_bytes_per_step": 16, "path": "qb_lanczos (host complex128 v0 in, alpha/beta out, FP32 storage, "
+                                                  "CSR lane)"},
+        "time_to_e0": e0,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
-        "levels": levels,
-        "ftlm": ftlm,
-        "serve": serve,
     }
+    line.update(secondary)
     print(json.dumps(line), flush=True)
-    A.close()
     replicas.finish(world)
+
+
+def chain32_measure(args, stream):
+    """The XXZ chain N = 32 sector (4,707,969 states): FP32 / FP64 CSR applies, the walk, e2e, time-to-E0 and the
+    reference engine's host lane on the whole sector."""
+    import torch
+
+    from qed_spin_b200 import device as D
+    spec, prog, prods = workload()
+    t0 = time.perf_counter()
+    S = D.Sector(spec)
+    torch.cuda.synchronize()
+    enum_s = time.perf_counter() - t0
+    P = D.Program(prog)
+    n = S.dim
+    e_bar = emitted_per_row(S.reps()[0], prog)
+    hbm, _ = peaks()
+    rng = np.random.default_rng(1)
+    x64 = torch.from_numpy(rng.normal(size=n) + 1j * rng.normal(size=n)).cuda()
+    x32 = x64.to(torch.complex64)
+    y32, y64 = torch.empty_like(x32), torch.empty_like(x64)
+    walk32 = time_applies(lambda: D.matvec(S, S, P, [x32], [y32], dtype="c64", stream=stream), 10, 3, stream, 1)
+    t = time.perf_counter()
+    r_plain = D.eigs_lowest(S, P, dtype="c128")
+    t_plain = time.perf_counter() - t
+    t = time.perf_counter()
+    A = D.Csr(S, S, P)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t
+    A.attach(P)
+    cinfo = A.info()
+    per32 = time_applies(lambda: D.matvec(S, S, P, [x32], [y32], dtype="c64", stream=stream), 200, 5, stream, 1)
+    per64 = time_applies(lambda: D.matvec(S, S, P, [x64], [y64], dtype="c128", stream=stream), 100, 3, stream, 1)
+    b_alg = n * (8 + 8 + 8) + n * e_bar * 8
+    v0 = x64.cpu().numpy()
+    D.lanczos(S, P, v0, 8, dtype="c64")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    D.lanczos(S, P, v0, 20, dtype="c64")
+    e2e_s = time.perf_counter() - t
+    t = time.perf_counter()
+    r64 = D.eigs_lowest(S, P, dtype="c128")
+    t64 = time.perf_counter() - t
+    t = time.perf_counter()
+    r32 = D.eigs_lowest(S, P, dtype="c64", refine=True)
+    t32 = time.perf_counter() - t
+    t = time.perf_counter()
+    r2 = D.eigs(S, P, 2)
+    k2_s = time.perf_counter() - t
+    out = {"workload": CHAIN32, "dim": n, "enumeration_s": enum_s, "csr_build_s": build_s, "nnz": cinfo["nnz"],
+           "csr_bytes": cinfo["bytes"], "emitted_per_row": e_bar,
+           "csr_ms_per_hv_fp32": per32, "hv_per_s_fp32": 1e3 / per32, "frac_fp32": b_alg / (per32 * 1e-3) / 1e9 / hbm,
+           "csr_ms_per_hv_fp64": per64, "walk_ms_per_hv_fp32": walk32,
+           "e2e_hv_per_s_20_steps": 20 / e2e_s,
+           "time_to_e0": {"plain_fp64_walk_s": t_plain, "csr_fp64_s": t64, "csr_fp32_refined_s": t32,
+                          "rel_err_fp32_refined": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]),
+                          "e0": r64["e0"], "plain_e0": r_plain["e0"]},
+           "k2": {"s": k2_s, "values": list(map(float, r2["values"])), "converged": r2["converged"],
+                  "matvecs": r2["matvecs"], "lane": "Krylov-Schur on the CSR"}}
+    A.close()
+    S.close()
+    if not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = reference_chain32(os.cpu_count() or 1)
+        except Exception as e:
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
 
 
 FTLM_N, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED = 24, 40, 100, 20240601
@@ -549,10 +684,9 @@ def ftlm_measure(args, with_cpu=True):
     return out
 
 
-def levels_measure(S, P, args):
-    """The k > 1 lane: config 2's two lowest levels on the attached CSR (FP64), and config 1 (the Heisenberg chain
-    N = 20, Sz = 0, k = 0, lowest four) on the device against the reference engine's krylov_schur_kernel on the
-    host cores."""
+def levels_measure(args):
+    """Config 1: the Heisenberg chain N = 20, Sz = 0, k = 0, lowest four levels (the k > 1 lane) on the device
+    against the reference engine's krylov_schur_kernel on the host cores; and the CUDA-graph comparison."""
     import torch
 
     from qed_spin_b200 import device as D
@@ -560,10 +694,6 @@ def levels_measure(S, P, args):
     from qed_spin_b200 import operators as ops
     out = {}
     torch.cuda.synchronize()
-    t = time.perf_counter()
-    r2 = D.eigs(S, P, 2)
-    out["chain32_k2"] = {"s": time.perf_counter() - t, "values": list(map(float, r2["values"])),
-                         "converged": r2["converged"], "matvecs": r2["matvecs"], "lane": "Krylov-Schur on the CSR"}
     spec = lat.chain_sector(20, 10, 0)
     prods = ops.heisenberg_products(lat.chain_bonds(20))
     prog = ops.row_program(ops.from_products(20, prods))
@@ -721,80 +851,6 @@ def serve_measure(args):
     return out
 
 
-def e0_6x6(args):
-    """Time to E0 on the 6x6 periodic J1-J2 lattice (J1 = 1, J2 = 0.5), S^z = 0, momentum (0, 0) under the 36
-    translations (252,091,362 representatives): the plain FP64 lane (the on-the-fly walk, no CSR) against the
-    device reduced CSR with FP64 storage and with FP32 storage + FP64 refinement; the CSR build is counted."""
-    import torch
-
-    from qed_spin_b200 import build
-    from qed_spin_b200 import device as D
-    from qed_spin_b200 import lattice as lat
-    from qed_spin_b200 import operators as ops
-    build.build()
-    nn, nnn = lat.square_j1j2_bonds(6, 6)
-    spec = lat.square_k0_sector(6, 6, 18)
-    prog = ops.row_program(ops.from_products(36, ops.heisenberg_products(nn, 1.0) + ops.heisenberg_products(nnn, 0.5)))
-    t = time.perf_counter()
-    S = D.Sector(spec)
-    torch.cuda.synchronize()
-    enum_s = time.perf_counter() - t
-    P = D.Program(prog)
-    n = S.dim
-    out = {"workload": "6x6 J1-J2 (J2/J1 = 0.5) Sz=0 k=(0,0), translations only", "dim": n, "enumeration_s": enum_s}
-    stream = torch.cuda.current_stream()
-
-    def per_apply(dt, steps):
-        x = torch.randn(n, dtype=torch.complex64 if dt == "c64" else torch.complex128, device="cuda")
-        y = torch.empty_like(x)
-        D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
-        torch.cuda.synchronize()
-        e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0_.record(stream)
-        for _ in range(steps):
-            D.matvec(S, S, P, [x], [y], dtype=dt, stream=stream)
-        e1_.record(stream)
-        torch.cuda.synchronize()
-        del x, y
-        return e0_.elapsed_time(e1_) / steps
-
-    out["walk_ms_per_hv_fp64"] = per_apply("c128", 2)
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    r = D.eigs_lowest(S, P, dtype="c128")
-    out["plain_fp64_walk"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
-                              "matvecs": r["matvecs"], "converged": r["converged"]}
-    t = time.perf_counter()
-    A = D.Csr(S, S, P)
-    torch.cuda.synchronize()
-    out["csr_build_s"] = time.perf_counter() - t
-    out["csr"] = A.info()
-    A.attach(P)
-    out["csr_ms_per_hv_fp32"] = per_apply("c64", 5)
-    out["csr_ms_per_hv_fp64"] = per_apply("c128", 5)
-    hbm, kind = peaks()
-    for dt, sb in (("fp32", 8), ("fp64", 16)):
-        ms = out[f"csr_ms_per_hv_{dt}"]
-        alg = out["csr"]["bytes"] + 2 * n * sb
-        # each x load fetches a whole 32-byte DRAM sector when x is far larger than L2
-        sectors = out["csr"]["bytes"] + out["csr"]["nnz"] * 32 + n * sb
-        out[f"roofline_{dt}"] = {"alg_bytes": alg, "alg_frac": alg / (ms * 1e-3) / 1e9 / hbm,
-                                 "sector_bytes_model": sectors, "sector_frac": sectors / (ms * 1e-3) / 1e9 / hbm,
-                                 "peak_gbs": hbm, "peak_kind": kind}
-    t = time.perf_counter()
-    r = D.eigs_lowest(S, P, dtype="c128")
-    out["csr_fp64"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"], "matvecs": r["matvecs"]}
-    t = time.perf_counter()
-    r = D.eigs_lowest(S, P, dtype="c64", refine=True)
-    out["csr_fp32_refined"] = {"s": time.perf_counter() - t, "e0": r["e0"], "iters": r["iters"],
-                               "matvecs": r["matvecs"], "converged": r["converged"]}
-    e_ref = out["plain_fp64_walk"]["e0"]
-    out["rel_err_fp32_refined_vs_plain"] = abs(out["csr_fp32_refined"]["e0"] - e_ref) / abs(e_ref)
-    out["speedup_fp32_refined_incl_build_vs_plain"] = out["plain_fp64_walk"]["s"] / (out["csr_fp32_refined"]["s"]
-                                                                                      + out["csr_build_s"])
-    print(json.dumps(out))
-    A.close()
-
 
 def profile_case(args):
     """The small profiling workloads of the ncu summaries under profiles/: the sector is built on the device,
@@ -841,8 +897,9 @@ def profile_case(args):
         spec, prog, _ = workload()
     else:
         Ly = 5 if args.profile_case == "sq30" else 6
+        n_up = {"sq36n11": 11, "sq36n12": 12}.get(args.profile_case, 3 * Ly)
         nn, nnn = lat.square_j1j2_bonds(6, Ly)
-        spec = lat.square_k0_sector(6, Ly, 3 * Ly)
+        spec = lat.square_k0_sector(6, Ly, n_up)
         prog = ops.row_program(ops.from_products(6 * Ly, ops.heisenberg_products(nn, 1.0)
                                                  + ops.heisenberg_products(nnn, 0.5)))
     S = D.Sector(spec)

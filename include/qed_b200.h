@@ -109,6 +109,16 @@ int qb_sector_info(const qb_sector* s, uint64_t* device_bytes, int* slc_L, int* 
  * include/ed/matvec/rep_symmetry_basis_policy.h:221-241), for n states at once (host arrays). */
 int qb_index_and_projection(const qb_sector* s, const uint64_t* states, uint64_t n, int64_t* index, double* proj);
 
+/* The sublattice key order a sector of this descriptor canonicalises in (host work only; no device needed):
+ * the rule of include/ed/basis/sublattice_code.h:23-34 and 164-191 under desc->sublattice_mode -- a block
+ * system of the group's site permutations with L sites in each of m blocks, block j holding key bits
+ * [N - (j + 1) L, N - j L) -- and its tables: lead[j * 2^L + x], the least leading block an element reaches from
+ * pattern x of block j, and cand[cand_off[j * 2^L + x] ...], the elements that reach it, ascending. *L = *m = 0:
+ * no code (the plain order). Sizes: key_bit n_sites, lead m 2^L, cand_off m 2^L + 1, cand *n_cand; any output
+ * array may be NULL (call once with NULLs for the sizes). */
+int qb_key_order(const qb_sector_desc* desc, int* L, int* m, uint64_t* n_cand, int32_t* key_bit, uint16_t* lead,
+                 uint32_t* cand_off, uint16_t* cand);
+
 /* ---- sectors by content ----------------------------------------------------------------------
  * qb_sector_acquire returns the one device sector of a descriptor (the device, group, characters,
  * representative order and lookup), enumerating it on first use: repeated requests share it, as the
@@ -205,14 +215,21 @@ int qb_eigs_lowest(const qb_sector* sec, const qb_program* prog, int max_iter, i
 int qb_ground_state(const qb_sector* sec, const qb_program* prog, int max_steps, double* e0, double* residual,
                     int* certified, void* vec_device, double* vec_host, int* matvecs);
 
-/* The k > 1 lane (krylov_schur_lane, src/engine/block_solve.cpp:433-510, over krylov_schur_kernel,
- * include/ed/krylov/krylov_schur.h:95-312): thick-restart Krylov-Schur with full CGS2 from
- * staged_seed(0x51ED0B70), cycles of min(2k + 60, 2p + 20, n) vectors keeping p = k + max(k/2, 8), lock
- * tolerance 1e-10 * scale, fresh deflated starts after an invariant subspace, and the degeneracy probe.
- * values: the k lowest, ascending (NaN past n_found). max_iter: matvec budget (0: max(200k, 2000)).
- * vecs_device: NULL, or k device pointers (each n complex128, or NULL) for the eigenvectors. */
+/* The k > 1 lane: the k lowest levels of a sector (the contract of krylov_schur_lane,
+ * src/engine/block_solve.cpp:433-510: the k lowest levels ascending, each converged to a residual of
+ * 1e-10 * (sum |coeff|), multiplicities resolved, from the staged Gaussian start of seed 0x51ED0B70) by
+ * thick-restart Lanczos with full reorthogonalisation, its scalars kept on the device and read once per
+ * restart cycle; a fresh start deflated against the found levels then searches below the k-th for
+ * further members of a multiplet. values: the k lowest, ascending (NaN past n_found). max_iter: matvec
+ * budget (0: max(200k, 2000)). vecs_device: NULL, or k device pointers (each n complex128, or NULL) for
+ * the eigenvectors. qb_eigs_k is qb_eigs_levels with dtype QB_C128. */
 int qb_eigs_k(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, double* values, int* n_found,
               int* converged, int* matvecs, void* const* vecs_device);
+/* The same with the Lanczos vectors stored as dtype: QB_C64 stores them as complex64 (FP64 arithmetic and
+ * scalars) and converges to 1e-6 * scale; refine != 0 then refines the returned pairs in FP64 (Rayleigh-Ritz
+ * on the pairs and their residuals, repeated) to the 1e-10 * scale residual. */
+int qb_eigs_levels(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, int dtype, int refine,
+                   double* values, int* n_found, int* converged, int* matvecs, void* const* vecs_device);
 
 /* T = 0 dynamics of an operator O from sector src to sector tgt (src/engine/dynamics.cpp:442-566): the
  * certified ground state psi0 of h_src, phi = O psi0 (op: the cross row program, rows in tgt, columns in

@@ -93,13 +93,15 @@ inline std::shared_ptr<qb_program> upload_program(const ed::ops::MaskedProgram& 
 class B200SectorMatVec final : public ed::LinearOperator {
 public:
     using Complex = std::complex<double>;
+    // norm_bound(): the sum of |coefficient| over the program's terms, the bound the reference's sector
+    // operators report and its Krylov drivers scale their breakdown, cluster and degeneracy tolerances by.
     B200SectorMatVec(const ed::symmetry::RepSectorData& rd, const ed::ops::MaskedProgram& rows)
-        : row_(upload_sector(rd)), col_(row_), prog_(upload_program(rows)), dim_(rd.reps.size()) {
-        for (const auto& c : rows.term_coeff) norm_bound_ += std::abs(c);
-    }
+        : row_(upload_sector(rd)), col_(row_), prog_(upload_program(rows)), dim_(rd.reps.size()),
+          norm_bound_(coeff_sum(rows)) {}
     B200SectorMatVec(const ed::symmetry::RepSectorData& row, const ed::symmetry::RepSectorData& col,
                      const ed::ops::MaskedProgram& rows)
-        : row_(upload_sector(row)), col_(upload_sector(col)), prog_(upload_program(rows)), dim_(row.reps.size()) {}
+        : row_(upload_sector(row)), col_(upload_sector(col)), prog_(upload_program(rows)), dim_(row.reps.size()),
+          norm_bound_(coeff_sum(rows)) {}
 
     void apply(const Complex* in, Complex* out, std::size_t n) const override {
         if (n != dim_) throw std::invalid_argument("B200SectorMatVec: length != sector dim");
@@ -128,13 +130,20 @@ public:
     [[nodiscard]] MultiMatvecFn bind_cuda_multi() const override {
         auto row = row_, col = col_;
         auto prog = prog_;
-        return [row, col, prog](const Complex* const* ins, Complex* const* outs, std::size_t, std::size_t k) {
+        const std::size_t dim = dim_;
+        return [row, col, prog, dim](const Complex* const* ins, Complex* const* outs, std::size_t n, std::size_t k) {
+            if (n != dim) throw std::invalid_argument("B200SectorMatVec: length != sector dim");
             check(qb_matvec(row.get(), col.get(), prog.get(), reinterpret_cast<const void* const*>(ins),
                             reinterpret_cast<void* const*>(outs), static_cast<int>(k), QB_C128, nullptr));
         };
     }
 
 private:
+    static double coeff_sum(const ed::ops::MaskedProgram& P) {
+        double s = 0.0;
+        for (const auto& c : P.term_coeff) s += std::abs(c);
+        return s;
+    }
     std::shared_ptr<qb_sector> row_, col_;
     std::shared_ptr<qb_program> prog_;
     std::size_t dim_ = 0;

@@ -59,7 +59,10 @@ def lib():
     L.qref_index_and_projection.restype = C.c_int64
     L.qref_index_and_projection.argtypes = [vp, C.c_uint64, _f64p]
     L.qref_gather.argtypes = [vp, vp, _f64p, _f64p]
+    L.qref_key_order.argtypes = [C.c_int, C.c_int, _i32p, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_uint64), vp, vp, vp, vp]
     L.qref_cross_gather.argtypes = [vp, vp, vp, _f64p, _f64p]
+    L.qref_gather_rows.argtypes = [vp, vp, _f64p, _u64p, C.c_uint64, _f64p]
     L.qref_csr_build.restype = vp
     L.qref_csr_build.argtypes = [vp, vp]
     L.qref_csr_free.argtypes = [vp]
@@ -67,6 +70,9 @@ def lib():
     L.qref_csr_nnz.argtypes = [vp]
     L.qref_csr_get.argtypes = [vp, _u64p, _u32p, _f64p]
     L.qref_csr_spmv.argtypes = [vp, _f64p, _f64p]
+    L.qref_csr_spmv_real.argtypes = [vp, _f64p, _f64p]
+    L.qref_csr_build_rows.restype = vp
+    L.qref_csr_build_rows.argtypes = [vp, vp, C.c_uint64, C.c_uint64]
     L.qref_ftlm_blocks.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint64, _f64p, C.c_int, _f64p, _f64p,
                                    _f64p, _f64p]
     L.qref_csr_bytes.restype = C.c_uint64
@@ -199,6 +205,14 @@ class Sector:
         _check(lib().qref_gather(self.h, prog.h, x.view(np.float64), y.view(np.float64)))
         return y
 
+    def gather_rows(self, prog: Program, x: np.ndarray, rows: np.ndarray) -> np.ndarray:
+        """Rows `rows` of O x by the reference's row walk (for_each_sector_entry), OpenMP over the rows."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        rows = np.ascontiguousarray(rows, dtype=np.uint64)
+        y = np.zeros(len(rows), np.complex128)
+        _check(lib().qref_gather_rows(self.h, prog.h, x.view(np.float64), rows, len(rows), y.view(np.float64)))
+        return y
+
     def csr(self, prog: Program, x=None):
         """The merged reduced CSR (row_ptr, col, val); with x, also the reference's CSR spmv of x."""
         L = lib()
@@ -283,6 +297,28 @@ def staged_seed(seed: int, n: int) -> np.ndarray:
     return out.view(np.complex128)
 
 
+def key_order(n_sites, perms, flips=None, mode=-1):
+    """The reference's sublattice code of a group and its tables (SublatticeCode), or None."""
+    L = lib()
+    perms = np.ascontiguousarray(perms, np.int32)
+    fl = None if flips is None else np.ascontiguousarray(flips, np.uint64)
+    G = perms.shape[0]
+    Lb, mb, nc = C.c_int(), C.c_int(), C.c_uint64()
+    fp = None if fl is None else fl.ctypes.data
+    _check(L.qref_key_order(n_sites, G, perms.reshape(-1), fp, mode, C.byref(Lb), C.byref(mb), C.byref(nc), None,
+                            None, None, None))
+    if Lb.value == 0:
+        return None
+    P = mb.value << Lb.value
+    kb = np.zeros(n_sites, np.int32)
+    lead = np.zeros(P, np.uint16)
+    off = np.zeros(P + 1, np.uint32)
+    cand = np.zeros(max(1, nc.value), np.uint16)
+    _check(L.qref_key_order(n_sites, G, perms.reshape(-1), fp, mode, C.byref(Lb), C.byref(mb), C.byref(nc),
+                            kb.ctypes.data, lead.ctypes.data, off.ctypes.data, cand.ctypes.data))
+    return {"L": Lb.value, "m": mb.value, "key_bit": kb, "lead": lead, "cand_off": off, "cand": cand[: nc.value]}
+
+
 def tridiag_eig(alpha, beta, vectors=True):
     a = np.ascontiguousarray(alpha, dtype=np.float64)
     m = len(a)
@@ -305,10 +341,16 @@ def max_threads() -> int:
 class Csr:
     """The reference's ReducedSymmetryCsr of a program on one sector, kept for repeated spmv."""
 
-    def __init__(self, sector: "Sector", prog: Program):
+    def __init__(self, sector: "Sector", prog: Program, rows=None):
+        """rows: None for every row, or (r0, n) for the merged rows r0 .. r0 + n - 1 alone (columns over the
+        whole sector)."""
         L = lib()
-        self.dim = sector.dim
-        self.h = L.qref_csr_build(sector.h, prog.h)
+        if rows is None:
+            self.dim = sector.dim
+            self.h = L.qref_csr_build(sector.h, prog.h)
+        else:
+            self.dim = int(rows[1])
+            self.h = L.qref_csr_build_rows(sector.h, prog.h, int(rows[0]), int(rows[1]))
         if not self.h:
             raise RuntimeError(L.qref_last_error().decode())
 
@@ -322,6 +364,10 @@ class Csr:
 
     def spmv(self, x: np.ndarray, y: np.ndarray) -> None:
         _check(lib().qref_csr_spmv(self.h, x.view(np.float64), y.view(np.float64)))
+
+    def spmv_real(self, x: np.ndarray, y: np.ndarray) -> bool:
+        """y = Re(A) x on float64 vectors (the host lane of a real sector); False when A is not real."""
+        return lib().qref_csr_spmv_real(self.h, x, y) == 0
 
     def close(self):
         if getattr(self, "h", None):

@@ -359,6 +359,33 @@ std::int64_t qref_index_and_projection(void* s, std::uint64_t state, double* pro
     return k;
 }
 
+// The reference's sublattice code of a group (SublatticeCode::of, include/ed/basis/sublattice_code.h:164-191)
+// under a mode: 1 forced, 0 off, -1 the size rule with the relaxed hint (16 permutations), -2 the strict one
+// (64). Outputs as qb_key_order: *L = *m = 0 when there is no code; arrays filled when non-null.
+int qref_key_order(int n_sites, int G, const int* perms, const std::uint64_t* flips, int mode, int* L, int* m,
+                   std::uint64_t* n_cand, int* key_bit, std::uint16_t* lead, std::uint32_t* cand_off,
+                   std::uint16_t* cand) {
+    return guarded([&] {
+        std::optional<bool> om;
+        if (mode == 1) om = true;
+        if (mode == 0) om = false;
+        const ed::symmetry::SublatticeRuleScope scope(mode != -2);
+        const auto c = ed::symmetry::SublatticeCode::of(perms, flips, G, n_sites, om);
+        *L = *m = 0;
+        *n_cand = 0;
+        if (!c) return;
+        const auto v = c->view();
+        *L = v.L;
+        *m = v.m;
+        const std::size_t P = static_cast<std::size_t>(v.m) << v.L;
+        *n_cand = v.cand_off[P];
+        if (key_bit) std::copy(c->key_bit().begin(), c->key_bit().end(), key_bit);
+        if (lead) std::copy(v.lead, v.lead + P, lead);
+        if (cand_off) std::copy(v.cand_off, v.cand_off + P + 1, cand_off);
+        if (cand) std::copy(v.cand, v.cand + v.cand_off[P], cand);
+    });
+}
+
 // ---------------- matvecs ----------------
 // out = O in on one sector by the row walk (sector_gather, include/ed/matvec/sector_rows.h:137-140).
 int qref_gather(void* sec, void* prog, const double* in, double* out) {
@@ -368,6 +395,29 @@ int qref_gather(void* sec, void* prog, const double* in, double* out) {
         const auto pol = S->rd.make_policy();
         ed::matvec::sector_gather(P->view(), pol, S->rd.dim(), reinterpret_cast<const Complex*>(in),
                                   reinterpret_cast<Complex*>(out));
+    });
+}
+
+// out[i] = row rows[i] of O in on one sector, for n listed rows: the body of sector_gather
+// (for_each_sector_entry, sector_rows.h:58-63, summed as cross_gather does at sector_rows.h:128-132),
+// OpenMP over the listed rows. The sampled form of the host walk lane for sectors whose full apply
+// is too long to time or check whole.
+int qref_gather_rows(void* sec, void* prog, const double* in, const std::uint64_t* rows, std::uint64_t n,
+                     double* out) {
+    return guarded([&] {
+        const auto* S = static_cast<RefSector*>(sec);
+        const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
+        const auto pol = S->rd.make_policy();
+        const auto view = P->view();
+        const Complex* x = reinterpret_cast<const Complex*>(in);
+        Complex* y = reinterpret_cast<Complex*>(out);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < static_cast<long long>(n); ++i) {
+            Complex acc(0.0, 0.0);
+            ed::matvec::for_each_sector_entry(view, pol, rows[i],
+                                              [&](std::uint64_t c, const Complex& v) { acc += v * x[c]; });
+            y[i] = acc;
+        }
     });
 }
 
@@ -432,6 +482,53 @@ int qref_csr_spmv(void* c, const double* in, double* out) {
     return guarded([&] {
         static_cast<RefCsr*>(c)->csr.spmv(reinterpret_cast<const Complex*>(in), reinterpret_cast<Complex*>(out));
     });
+}
+
+// out = Re(A) in on real vectors (RealCsrView::spmv, include/ed/matvec/reduced_csr.h:111-135): the host lane
+// of a real symmetry sector of a real H (RepSectorMatVec::is_real, src/engine/internal.h:264-283, chosen by
+// with_backend, include/ed/core/select_backend.h:186). Returns 1 when the CSR is not real (nothing applied).
+int qref_csr_spmv_real(void* c, const double* in, double* out) {
+    const auto& m = static_cast<RefCsr*>(c)->csr;
+    const auto view = ed::matvec::RealCsrView::of(m, ed::numerics::kRealBlockRel);
+    if (!view) return 1;
+    view->spmv(in, out);
+    return 0;
+}
+
+namespace {
+// Rows [r0, r0 + n) of a one-dimensional-irrep sector as a row policy of their own (row j is the sector's row
+// r0 + j; columns stay the whole sector's). Lets build_cross_csr build the merged rows of a contiguous block.
+struct RowBlock {
+    const ed::matvec::basis::RepSymmetryBasisPolicy* p;
+    std::uint64_t r0, n;
+    int irrep_dim = 1;
+    std::uint64_t dim() const noexcept { return n; }
+    std::uint64_t state_of(std::uint64_t j) const noexcept { return p->state_of(r0 + j); }
+    double inv_norm_of(std::uint64_t j) const noexcept { return p->inv_norm_of(r0 + j); }
+    std::uint64_t first_state_of(std::uint64_t j) const noexcept { return j; }
+    int rank_of(std::uint64_t) const noexcept { return 1; }
+    const Complex* C_of(std::uint64_t) const noexcept { return nullptr; }   // (the d > 1 branch, never taken)
+};
+}  // namespace
+
+// The merged CSR of rows [r0, r0 + n) of O on one sector (build_cross_csr, sector_rows.h:223-404, over the
+// block's rows, columns the whole sector): the reference's host CSR lane on a contiguous sample of rows, for
+// sectors whose whole CSR is too large to build for a bounded timing. The diagonal goes through the lookup
+// (the cross form), which gives the same entries up to the rounding of inv_norm * projection.
+void* qref_csr_build_rows(void* sec, void* prog, std::uint64_t r0, std::uint64_t n) {
+    try {
+        const auto* S = static_cast<RefSector*>(sec);
+        const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
+        if (S->rd.irrep_dim != 1 || r0 + n > S->rd.dim()) throw std::invalid_argument("qref_csr_build_rows: bad rows");
+        const auto pol = S->rd.make_policy();
+        const RowBlock rows{&pol, r0, n};
+        auto* c = new RefCsr;
+        c->csr = ed::matvec::build_cross_csr(P->view(), rows, pol, false, n);
+        return c;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
 }
 
 // ---------------- seeds ----------------

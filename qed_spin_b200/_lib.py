@@ -20,13 +20,13 @@ QB_NOALLOC_MAX_ITER = 1024
 EXPORTS = [
     "qb_last_error", "qb_device_count",
     "qb_sector_create", "qb_sector_create_from_reps", "qb_sector_destroy", "qb_sector_dim", "qb_sector_download",
-    "qb_sector_info", "qb_index_and_projection",
+    "qb_sector_info", "qb_index_and_projection", "qb_key_order",
     "qb_program_create", "qb_program_destroy",
     "qb_matvec", "qb_matvec_block", "qb_matvec_host",
     "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
-    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_dynamics_t0", "qb_dense_levels",
+    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_eigs_levels", "qb_dynamics_t0", "qb_dense_levels",
     "qb_dense_levels_blocks",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
     "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_sector_save",
@@ -111,6 +111,7 @@ def lib():
     L.qb_sector_download.argtypes = [vp, vp, vp]
     L.qb_sector_info.argtypes = [vp, C.POINTER(u64), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.qb_index_and_projection.argtypes = [vp, vp, u64, vp, vp]
+    L.qb_key_order.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(u64), vp, vp, vp, vp]
     L.qb_program_create.argtypes = [C.POINTER(ProgramDesc), C.POINTER(vp)]
     L.qb_program_destroy.argtypes = [vp]
     L.qb_matvec.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
@@ -128,6 +129,7 @@ def lib():
     L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]
     L.qb_ground_state.argtypes = [vp, vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i), vp, vp, C.POINTER(i)]
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
+    L.qb_eigs_levels.argtypes = [vp, vp, i, u64, i, i, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
     L.qb_dense_levels.argtypes = [vp, vp, vp]
     L.qb_dense_levels_blocks.argtypes = [vp, vp, i, vp]

@@ -1,0 +1,711 @@
+// =============================================================================
+// eigs_k.cu -- the k > 1 lane: the k lowest levels of a sector, and their vectors, on the device.
+//
+// Method: thick-restart Lanczos (K. Wu and H. Simon, SIAM J. Matrix Anal. Appl. 22 (2000) 602-616).
+//   - A cycle extends a basis of m vectors by Lanczos steps, each fully reorthogonalised by two classical
+//     Gram-Schmidt passes against the cycle's basis and the locked vectors. The step's scalars (alpha, beta)
+//     are written to device memory by the kernels themselves; a breakdown (beta below 64 eps times the
+//     scale) is marked on the device and the columns after it are zeroed. Nothing is read back inside a
+//     cycle: its kernels are queued back to back and the host reads the cycle's scalars once at its end.
+//   - At a restart the host solves the cycle's projected problem -- an arrowhead (the kept Ritz values and
+//     their couplings to the residual direction) followed by the new tridiagonal -- and the device rotates
+//     the basis onto the p lowest Ritz vectors; the last residual direction becomes column p.
+//   - Once the `want` lowest Ritz pairs have residual bounds below the tolerance, they are formed and locked.
+//   - Multiplicity: a Krylov space of one start holds one vector of each eigenspace. After the k lowest are
+//     locked, a fresh random start orthogonalised against them searches once more below the k-th level; a
+//     level found there joins the locked set (the highest then leaves it), until a search finds none.
+//   - An invariant subspace (breakdown) gives exact pairs; a fresh deflated start then continues the search.
+//
+// FP32 storage (dtype QB_C64): the basis and the locked vectors are stored as complex64 (the arithmetic and
+// all scalars stay FP64) and converged to 1e-6 of the scale, the level the storage rounding allows. With
+// refine != 0 the returned pairs are then refined in FP64: Rayleigh-Ritz on the span of the pairs and their
+// residuals (a block step of the LOBPCG family without its previous-direction block), repeated until every
+// residual is below the lock tolerance.
+//
+// The contract is the reference's krylov_schur_lane (src/engine/block_solve.cpp:433-510): the k lowest
+// levels of the block, ascending, each converged to a residual of kLockRel (1e-10) times the coefficient sum,
+// multiplicities resolved, from the staged Gaussian start of seed 0x51ED0B70 (block_solve.cpp:263); the
+// method and its code are this file's own.
+// =============================================================================
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <limits>
+#include <memory>
+#include <random>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "qb_krylov.cuh"
+
+namespace qb {
+namespace {
+
+using cd = std::complex<double>;
+
+constexpr std::uint64_t kStartSeed = 0x51ED0B70ULL;      // staged_seed of the k > 1 lane (block_solve.cpp:263)
+constexpr std::uint64_t kFreshSeed = 0x7E57A27ULL;        // fresh starts of this lane (any seed serves)
+constexpr double kLockTol = 1e-10;                       // kLockRel (include/ed/core/numerics.h:25)
+constexpr double kLockTolF32 = 1e-6;                     // the FP32-storage phase, before the FP64 refinement
+constexpr double kFloorRel = 64.0 * std::numeric_limits<double>::epsilon();   // kBreakdownRel (numerics.h:23)
+constexpr int kRefineMax = 6;                            // FP64 refinement rounds at most
+
+// ---- kernels ----
+
+// alpha[j] = -Re coef[j] (first pass) or alpha[j] -= Re coef[j] (second pass): the diagonal of the step.
+__global__ void k_take_alpha(const double2* coef, int at, int j, int first, double* alpha) {
+    if (first)
+        alpha[j] = -coef[at].x;
+    else
+        alpha[j] -= coef[at].x;
+}
+
+// out = w / beta stored as T; a beta at or below floor marks a breakdown at step j (the smallest j wins) and
+// zeroes the column, so the rest of the cycle runs on zeros.
+template <class T>
+__global__ void k_next_col(std::uint64_t n, const double2* w, T* out, const double* beta, double floor, int* brk,
+                           int j) {
+    const double b = *beta;
+    const bool broken = !(b > floor);
+    if (broken && blockIdx.x == 0 && threadIdx.x == 0) atomicMin(brk, j);
+    const double s = broken ? 0.0 : 1.0 / b;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const double2 a = w[i];
+        V<T>::st(out, i, a.x * s, a.y * s);
+    }
+}
+
+// out = x / *nrm stored as T (a start vector).
+template <class T> __global__ void k_unit_into(std::uint64_t n, const double2* x, T* out, const double* nrm) {
+    const double s = 1.0 / *nrm;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const double2 a = x[i];
+        V<T>::st(out, i, a.x * s, a.y * s);
+    }
+}
+
+// out[:, c] = sum_r V[:, r] S[r, c] for c in [c0, c0 + kRotW) and c < cols: V columns of stride n stored as T,
+// S real column-major mm x cols, out columns of stride n stored as T.
+constexpr int kRotW = 8;
+template <class T>
+__global__ void k_rotate_real(std::uint64_t n, int mm, int cols, int c0, const T* Vb, const double* S, T* out) {
+    extern __shared__ double Ss[];
+    const int nc = min(kRotW, cols - c0);
+    for (int t = threadIdx.x; t < mm * nc; t += blockDim.x) Ss[t] = S[static_cast<std::size_t>(c0) * mm + t];
+    __syncthreads();
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        double2 acc[kRotW];
+#pragma unroll
+        for (int c = 0; c < kRotW; ++c) acc[c] = make_double2(0.0, 0.0);
+        for (int r = 0; r < mm; ++r) {
+            const double2 v = V<T>::ld(Vb + static_cast<std::size_t>(r) * n, i);
+#pragma unroll
+            for (int c = 0; c < kRotW; ++c)
+                if (c < nc) {
+                    const double s = Ss[c * mm + r];
+                    acc[c].x += s * v.x;
+                    acc[c].y += s * v.y;
+                }
+        }
+#pragma unroll
+        for (int c = 0; c < kRotW; ++c)
+            if (c < nc) V<T>::st(out + static_cast<std::size_t>(c0 + c) * n, i, acc[c].x, acc[c].y);
+    }
+}
+
+// out_c = sum_r in_r Y[r, c] for every c < cols (FP64 columns; Y complex column-major nin x cols, nin * cols <=
+// kRotMaxCoef).
+constexpr int kRotMaxCoef = 32 * 32;
+__global__ void k_rotate_cplx(std::uint64_t n, int nin, int cols, const double2* const* in, const double2* Y,
+                              double2* const* out) {
+    __shared__ double2 Ys[kRotMaxCoef];
+    for (int t = threadIdx.x; t < nin * cols; t += blockDim.x) Ys[t] = Y[t];
+    __syncthreads();
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        for (int c = 0; c < cols; ++c) {
+            double re = 0.0, im = 0.0;
+            for (int r = 0; r < nin; ++r) {
+                const double2 a = in[r][i], y = Ys[c * nin + r];
+                re += a.x * y.x - a.y * y.y;
+                im += a.x * y.y + a.y * y.x;
+            }
+            out[c][i] = make_double2(re, im);
+        }
+    }
+}
+
+// R_c = AX_c - theta_c X_c for c < k.
+__global__ void k_residuals(std::uint64_t n, int k, const double2* const* X, const double2* const* AX,
+                            const double* theta, double2* const* R) {
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x)
+        for (int c = 0; c < k; ++c) {
+            const double2 a = AX[c][i], x = X[c][i];
+            R[c][i] = make_double2(a.x - theta[c] * x.x, a.y - theta[c] * x.y);
+        }
+}
+
+// x /= *nrm in place (FP64).
+__global__ void k_unit_inplace(std::uint64_t n, double2* x, const double* nrm) {
+    const double s = 1.0 / *nrm;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        x[i].x *= s;
+        x[i].y *= s;
+    }
+}
+
+// ---- small dense problems on the host ----
+
+// Eigenpairs of a Hermitian m x m matrix (column-major): cyclic Jacobi, each rotation made real by a phase
+// on its second index first; values ascending, vectors column-major.
+void hermitian_eig(std::vector<cd> A, int m, std::vector<double>& vals, std::vector<cd>& vecs) {
+    auto at = [&](int r, int c) -> cd& { return A[static_cast<std::size_t>(c) * m + r]; };
+    std::vector<cd> Q(static_cast<std::size_t>(m) * m, cd(0.0, 0.0));
+    for (int i = 0; i < m; ++i) Q[static_cast<std::size_t>(i) * m + i] = 1.0;
+    double fro = 0.0;
+    for (const cd& z : A) fro += std::norm(z);
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0;
+        for (int c = 0; c < m; ++c)
+            for (int r = 0; r < c; ++r) off += std::norm(at(r, c));
+        if (off == 0.0 || off <= 1e-30 * fro) break;
+        for (int p = 0; p + 1 < m; ++p)
+            for (int q = p + 1; q < m; ++q) {
+                const double mag = std::abs(at(p, q));
+                if (mag == 0.0) continue;
+                const cd ph = at(p, q) / mag;                 // a_pq = mag * ph
+                const double app = at(p, p).real(), aqq = at(q, q).real();
+                const double th = (aqq - app) / (2.0 * mag);
+                const double t = (th >= 0.0 ? 1.0 : -1.0) / (std::abs(th) + std::sqrt(th * th + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                const cd phc = std::conj(ph);
+                for (int r = 0; r < m; ++r) {             // A <- A D R, D = diag(1, conj(ph)) on (p, q)
+                    const cd x = at(r, p), y = at(r, q) * phc;
+                    at(r, p) = c * x - s * y;
+                    at(r, q) = s * x + c * y;
+                }
+                for (int r = 0; r < m; ++r) {             // A <- R^T D^H A
+                    const cd x = at(p, r), y = at(q, r) * ph;
+                    at(p, r) = c * x - s * y;
+                    at(q, r) = s * x + c * y;
+                }
+                at(p, q) = at(q, p) = cd(0.0, 0.0);
+                for (int r = 0; r < m; ++r) {             // Q <- Q D R
+                    cd& qp = Q[static_cast<std::size_t>(p) * m + r];
+                    cd& qq = Q[static_cast<std::size_t>(q) * m + r];
+                    const cd x = qp, y = qq * phc;
+                    qp = c * x - s * y;
+                    qq = s * x + c * y;
+                }
+            }
+    }
+    std::vector<int> order(m);
+    for (int i = 0; i < m; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return at(a, a).real() < at(b, b).real(); });
+    vals.resize(m);
+    vecs.assign(static_cast<std::size_t>(m) * m, cd(0.0, 0.0));
+    for (int c = 0; c < m; ++c) {
+        vals[c] = at(order[c], order[c]).real();
+        std::copy(Q.begin() + static_cast<std::size_t>(order[c]) * m,
+                  Q.begin() + static_cast<std::size_t>(order[c] + 1) * m, vecs.begin() + static_cast<std::size_t>(c) * m);
+    }
+}
+
+// Eigenpairs of a real symmetric m x m matrix (column-major), ascending, through the Hermitian solver.
+void symmetric_eig(const std::vector<double>& A, int m, std::vector<double>& vals, std::vector<double>& vecs) {
+    std::vector<cd> Ac(A.begin(), A.end());
+    std::vector<cd> vc;
+    hermitian_eig(std::move(Ac), m, vals, vc);
+    vecs.resize(vc.size());
+    for (std::size_t i = 0; i < vc.size(); ++i) vecs[i] = vc[i].real();   // real to rounding for a real matrix
+}
+
+// ---- the lane ----
+
+struct LevelsOut {
+    std::vector<double> values;
+    std::vector<DevBuf<double2>> vectors;   // FP64 copies, filled when asked
+    bool converged = false;
+    int matvecs = 0, cycles = 0, refine_rounds = 0;
+    double max_residual = 0.0;
+};
+
+template <class T> constexpr int dtype_of();
+template <> constexpr int dtype_of<double2>() { return QB_C128; }
+template <> constexpr int dtype_of<float2>() { return QB_C64; }
+
+template <class T> class ThickRestart {
+public:
+    ThickRestart(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t budget)
+        : sec_(sec), prog_(prog), n_(sec->dim), k_(k), budget_(budget), scale_(norm_bound(prog)),
+          floor_(kFloorRel * norm_bound(prog)), nb_(red_blocks(sec->dim)) {
+        const std::size_t es = sizeof(T);
+        // the cycle: m vectors, about 2k + 40 (at least k + 24), within 85% of the free memory
+        std::size_t m = std::max<std::size_t>(2 * static_cast<std::size_t>(k) + 40, static_cast<std::size_t>(k) + 24);
+        m = static_cast<std::size_t>(std::min<std::uint64_t>(m, n_));
+        const double free_b = 0.85 * static_cast<double>(available_bytes());
+        auto need = [&](std::size_t mm) {   // basis + kept Ritz vectors + locked + the FP64 work vector
+            return (static_cast<double>(mm + 1 + keep_for(mm) + 2 * static_cast<std::size_t>(k)) * es + 16.0) *
+                   static_cast<double>(n_);
+        };
+        while (m > static_cast<std::size_t>(k) + 4 && m > 2 && need(m) > free_b) --m;
+        if (need(m) > free_b)
+            throw Error(QB_ENOMEM, "eigs: " + std::to_string(m) + " Lanczos vectors of dimension " + std::to_string(n_) +
+                                       " do not fit the free device memory");
+        m_ = std::max<std::size_t>(1, m);
+        p_ = keep_for(m_);
+        Vb_.alloc((m_ + 1) * n_);
+        U_.alloc(std::max<std::size_t>(p_, 1) * n_);
+        w_.alloc(n_);
+        const std::size_t cap = m_ + 1 + 2 * static_cast<std::size_t>(k) + 8;
+        ptrs_.alloc(cap);
+        coef_.alloc(cap);
+        part_.alloc(static_cast<std::size_t>(kMaxRedBlocks) + cap * static_cast<std::size_t>(dot_chunks(n_, 1)));
+        alpha_.alloc(m_ + 1);
+        beta_.alloc(m_ + 2);
+        slots_.alloc(8);
+        brk_.alloc(1);
+        red_part_.alloc(4 * kMaxRedBlocks);
+        red_cnt_.alloc(1);
+        cuda_check(cudaMemset(red_cnt_.p, 0, sizeof(unsigned)), "zero");
+        S_.alloc(m_ * m_);
+    }
+
+    // The k lowest pairs: values ascending (fewer when the block is smaller); vectors kept as T.
+    void run(LevelsOut& out) {
+        start_from_host(staged_seed(n_, kStartSeed));
+        std::mt19937_64 fresh(kFreshSeed);
+        int null_starts = 0;
+        bool stalled = false;
+        // the main search and, after an invariant subspace, fresh deflated starts for what is left
+        while (static_cast<int>(locked_vals_.size()) < k_) {
+            const int got = search(k_ - static_cast<int>(locked_vals_.size()), std::numeric_limits<double>::infinity());
+            if (exhausted_) break;
+            if (got < 0) {   // the start vanished against the locked vectors: the block is exhausted
+                if (++null_starts >= 2) break;
+            } else if (got == 0 || budget_exhausted()) {
+                stalled = static_cast<int>(locked_vals_.size()) < k_ && !exhausted_;
+                break;
+            }
+            if (static_cast<int>(locked_vals_.size()) < k_) start_fresh(fresh);
+        }
+        // multiplicity: search below the k-th level from fresh deflated starts until nothing is found
+        for (int round = 0; round < k_ && !locked_vals_.empty() && !exhausted_ && !budget_exhausted(); ++round) {
+            const double top = *std::max_element(locked_vals_.begin(), locked_vals_.end());
+            const double gap = std::max(10.0 * tol(), 1e-8 * std::abs(top));
+            start_fresh(fresh);
+            const std::size_t before = locked_vals_.size();
+            const int got = search(1, top - gap);
+            if (got <= 0 || locked_vals_.size() == before) break;
+            if (locked_vals_.back() >= top - gap) {   // not below: the level was already there
+                drop_locked(locked_vals_.size() - 1);
+                break;
+            }
+            while (static_cast<int>(locked_vals_.size()) > k_) {
+                const auto hi = std::max_element(locked_vals_.begin(), locked_vals_.end()) - locked_vals_.begin();
+                drop_locked(static_cast<std::size_t>(hi));
+            }
+        }
+        std::vector<std::size_t> order(locked_vals_.size());
+        for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) { return locked_vals_[a] < locked_vals_[b]; });
+        for (std::size_t i : order) {
+            if (static_cast<int>(out.values.size()) >= k_) break;
+            out.values.push_back(locked_vals_[i]);
+            sorted_.push_back(locked_[i].p);
+        }
+        out.converged = !stalled && (static_cast<int>(out.values.size()) >= k_ || exhausted_);
+        out.matvecs += matvecs_;
+        out.cycles += cycles_;
+    }
+
+    // The returned vectors in ascending order of their levels (valid while this object lives).
+    const std::vector<T*>& sorted_vectors() const { return sorted_; }
+
+private:
+    static std::size_t keep_for(std::size_t m) {   // kept Ritz vectors at a restart: about a third of the cycle
+        if (m <= 2) return 1;
+        return std::min<std::size_t>(m - 1, std::max<std::size_t>(m / 3, 4));
+    }
+    double tol() const { return (std::is_same<T, float2>::value ? kLockTolF32 : kLockTol) * scale_; }
+    bool budget_exhausted() const { return static_cast<std::uint64_t>(matvecs_) >= budget_; }
+    T* col(std::size_t j) { return Vb_.p + j * n_; }
+    Scal red() { return Scal{nullptr, nullptr, nullptr, red_part_.p, red_cnt_.p}; }
+
+    void start_from_host(const std::vector<cd>& v) {
+        cuda_check(cudaMemcpy(w_.p, v.data(), n_ * 16, cudaMemcpyHostToDevice), "start upload");
+        have_start_ = true;
+    }
+    void start_fresh(std::mt19937_64& gen) {
+        std::vector<cd> v(n_);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        for (auto& z : v) {
+            const double re = nd(gen);
+            z = cd(re, nd(gen));
+        }
+        start_from_host(v);
+    }
+
+    // Device pointer table: the locked vectors, then the cycle's columns 0..m.
+    void write_ptrs() {
+        std::vector<const void*> h;
+        for (const auto& b : locked_) h.push_back(b.p);
+        for (std::size_t j = 0; j <= m_; ++j) h.push_back(col(j));
+        cuda_check(cudaMemcpy(ptrs_.p, h.data(), h.size() * sizeof(void*), cudaMemcpyHostToDevice), "pointers");
+    }
+    const T* const* basis() const { return reinterpret_cast<const T* const*>(ptrs_.p); }
+
+    // Two classical Gram-Schmidt passes of w against the first nb entries of the table; with at >= 0 the
+    // negated overlap with entry `at` goes to alpha[j] (summed over both passes).
+    void cgs2(int nb, int at, int j) {
+        if (nb == 0) return;
+        for (int pass = 0; pass < 2; ++pass) {
+            dot_many<T>(n_, nb, basis(), w_.p, coef_.p, part_.p, nullptr, nullptr);
+            k_axpy_many<T><<<nb_, kThreads>>>(n_, nb, basis(), coef_.p, w_.p, nullptr);
+            if (at >= 0) k_take_alpha<<<1, 1>>>(coef_.p, at, j, pass == 0 ? 1 : 0, alpha_.p);
+        }
+    }
+
+    // One search from the start in w_: lock up to `want` of the lowest pairs. Returns the number locked, or -1
+    // when the start is null against the locked vectors. give_up: a first cycle whose lowest Ritz value is at
+    // or above it ends the search with nothing locked.
+    int search(int want, double give_up) {
+        if (!have_start_) return -1;
+        have_start_ = false;
+        write_ptrs();
+        const int L = static_cast<int>(locked_.size());
+        cgs2(L, -1, 0);
+        k_norm_to<<<nb_, kThreads>>>(n_, w_.p, red(), slots_.p, nullptr);
+        double nrm = 0.0;
+        cuda_check(cudaMemcpy(&nrm, slots_.p, 8, cudaMemcpyDeviceToHost), "start norm");
+        if (!(nrm > 1e-13 * std::max(1.0, std::sqrt(static_cast<double>(n_))))) return -1;
+        k_unit_into<T><<<nb_, kThreads>>>(n_, w_.p, col(0), slots_.p);
+        std::size_t p = 0;
+        std::vector<double> theta, arrow;
+        for (bool first = true;; first = false) {
+            // extend the basis from column p to m, all scalars on the device
+            const int big = std::numeric_limits<int>::max();
+            cuda_check(cudaMemcpy(brk_.p, &big, sizeof(int), cudaMemcpyHostToDevice), "breakdown marker");
+            std::size_t steps = m_ - p;
+            if (budget_ > 0)
+                steps = static_cast<std::size_t>(std::min<std::uint64_t>(steps, budget_ - std::min<std::uint64_t>(budget_, matvecs_)));
+            if (steps == 0) return 0;
+            const std::size_t mend = p + steps;
+            for (std::size_t j = p; j < mend; ++j) {
+                launch_walk_mixed(sec_, sec_, prog_, col(j), w_.p, dtype_of<T>(), QB_C128, nullptr);
+                cgs2(L + static_cast<int>(j) + 1, L + static_cast<int>(j), static_cast<int>(j));
+                k_norm_to<<<nb_, kThreads>>>(n_, w_.p, red(), beta_.p + j + 1, nullptr);
+                k_next_col<T><<<nb_, kThreads>>>(n_, w_.p, col(j + 1), beta_.p + j + 1, floor_, brk_.p, static_cast<int>(j));
+            }
+            cuda_check(cudaGetLastError(), "lanczos cycle");
+            matvecs_ += static_cast<int>(steps);
+            ++cycles_;
+            std::vector<double> a(mend), b(mend + 1);
+            int brk = 0;
+            cuda_check(cudaMemcpy(a.data(), alpha_.p, mend * 8, cudaMemcpyDeviceToHost), "alpha");
+            cuda_check(cudaMemcpy(b.data(), beta_.p, (mend + 1) * 8, cudaMemcpyDeviceToHost), "beta");
+            cuda_check(cudaMemcpy(&brk, brk_.p, sizeof(int), cudaMemcpyDeviceToHost), "breakdown");
+            // the projected matrix: arrowhead (theta, arrow) then the tridiagonal of this cycle
+            const std::size_t mm = brk < big ? static_cast<std::size_t>(brk) + 1 : mend;
+            const double beta_last = brk < big ? 0.0 : b[mend];
+            std::vector<double> Tm(mm * mm, 0.0);
+            auto at = [&](std::size_t r, std::size_t c) -> double& { return Tm[c * mm + r]; };
+            for (std::size_t i = 0; i < p; ++i) {
+                at(i, i) = theta[i];
+                at(i, p) = at(p, i) = arrow[i];
+            }
+            for (std::size_t j = p; j < mm; ++j) {
+                at(j, j) = a[j];
+                if (j + 1 < mm) at(j, j + 1) = at(j + 1, j) = b[j + 1];
+            }
+            std::vector<double> vals, vecs;
+            symmetric_eig(Tm, static_cast<int>(mm), vals, vecs);
+            if (first && vals[0] >= give_up) return 0;
+            const std::size_t top = std::min<std::size_t>(static_cast<std::size_t>(want), mm);
+            std::size_t conv = 0;
+            while (conv < top && std::abs(beta_last * vecs[conv * mm + (mm - 1)]) < tol()) ++conv;
+            const bool invariant = brk < big;
+            if (invariant && mm == n_ - locked_.size()) exhausted_ = true;   // the whole (deflated) block is spanned
+            if (conv == top || invariant || budget_exhausted()) {
+                lock(vecs, mm, invariant ? top : conv, vals);
+                return static_cast<int>(invariant ? top : conv);
+            }
+            // thick restart: the p lowest Ritz vectors, then the residual direction v_mm
+            p = std::min(p_, mm - 1);
+            rotate(vecs, mm, p, U_.p);
+            cuda_check(cudaMemcpy(col(0), U_.p, p * n_ * sizeof(T), cudaMemcpyDeviceToDevice), "restart");
+            cuda_check(cudaMemcpy(col(p), col(mm), n_ * sizeof(T), cudaMemcpyDeviceToDevice), "residual direction");
+            theta.assign(vals.begin(), vals.begin() + static_cast<std::ptrdiff_t>(p));
+            arrow.resize(p);
+            for (std::size_t i = 0; i < p; ++i) arrow[i] = beta_last * vecs[i * mm + (mm - 1)];
+        }
+    }
+
+    void rotate(const std::vector<double>& Y, std::size_t mm, std::size_t cols, T* out) {
+        cuda_check(cudaMemcpy(S_.p, Y.data(), mm * cols * 8, cudaMemcpyHostToDevice), "rotation");
+        for (std::size_t c0 = 0; c0 < cols; c0 += kRotW)
+            k_rotate_real<T><<<nb_, kThreads, mm * kRotW * 8>>>(n_, static_cast<int>(mm), static_cast<int>(cols),
+                                                                static_cast<int>(c0), Vb_.p, S_.p, out);
+        cuda_check(cudaGetLastError(), "rotate");
+    }
+
+    void lock(const std::vector<double>& Y, std::size_t mm, std::size_t cnt, const std::vector<double>& vals) {
+        if (cnt == 0) return;
+        rotate(Y, mm, cnt, U_.p);
+        for (std::size_t i = 0; i < cnt; ++i) {
+            DevBuf<T> x(n_);
+            cuda_check(cudaMemcpy(x.p, U_.p + i * n_, n_ * sizeof(T), cudaMemcpyDeviceToDevice), "lock");
+            locked_.push_back(std::move(x));
+            locked_vals_.push_back(vals[i]);
+        }
+    }
+    void drop_locked(std::size_t i) {
+        locked_.erase(locked_.begin() + static_cast<std::ptrdiff_t>(i));
+        locked_vals_.erase(locked_vals_.begin() + static_cast<std::ptrdiff_t>(i));
+    }
+
+    const qb_sector* sec_;
+    const qb_program* prog_;
+    std::uint64_t n_;
+    int k_;
+    std::uint64_t budget_;
+    double scale_, floor_;
+    int nb_;
+    std::size_t m_ = 0, p_ = 0;
+    DevBuf<T> Vb_, U_;
+    DevBuf<double2> w_, coef_, part_;
+    DevBuf<void*> ptrs_;
+    DevBuf<double> alpha_, beta_, slots_, red_part_, S_;
+    DevBuf<unsigned> red_cnt_;
+    DevBuf<int> brk_;
+    std::vector<DevBuf<T>> locked_;
+    std::vector<double> locked_vals_;
+    std::vector<T*> sorted_;
+    bool have_start_ = false, exhausted_ = false;
+    int matvecs_ = 0, cycles_ = 0;
+};
+
+// FP64 refinement of k approximate pairs (X: k FP64 columns, orthonormalised here): Rayleigh-Ritz on span{X, R},
+// R the residuals, until every residual is at most tol; the values and X are updated in place.
+void refine_pairs(const qb_sector* sec, const qb_program* prog, std::vector<DevBuf<double2>>& X,
+                  std::vector<double>& values, double tol, LevelsOut& out) {
+    const std::uint64_t n = sec->dim;
+    const int k = static_cast<int>(X.size());
+    if (k == 0) return;
+    const int nb = red_blocks(n);
+    std::vector<DevBuf<double2>> AX(k), R(k), AR(k), T1(2 * k);
+    for (int c = 0; c < k; ++c) {
+        AX[c].alloc(n);
+        R[c].alloc(n);
+        AR[c].alloc(n);
+    }
+    for (auto& t : T1) t.alloc(n);
+    DevBuf<void*> ptr(8 * static_cast<std::size_t>(k) + 8);
+    DevBuf<double2> coef(2 * static_cast<std::size_t>(k) + 2),
+        part(static_cast<std::size_t>(2 * k + 2) * static_cast<std::size_t>(dot_chunks(n, 1)) + kMaxRedBlocks), Yd(kRotMaxCoef);
+    DevBuf<double> slots(4 * static_cast<std::size_t>(k) + 4), red_part(4 * kMaxRedBlocks), th(2 * static_cast<std::size_t>(k));
+    DevBuf<unsigned> red_cnt(1);
+    cuda_check(cudaMemset(red_cnt.p, 0, sizeof(unsigned)), "zero");
+    const Scal red{nullptr, nullptr, nullptr, red_part.p, red_cnt.p};
+    auto set_ptrs = [&](std::size_t at, const std::vector<double2*>& v) {
+        cuda_check(cudaMemcpy(static_cast<void**>(ptr.p) + at, v.data(), v.size() * sizeof(void*), cudaMemcpyHostToDevice),
+                   "pointers");
+    };
+    auto dptr = [&](std::size_t at) { return reinterpret_cast<const double2* const*>(static_cast<void**>(ptr.p) + at); };
+    auto optr = [&](std::size_t at) { return reinterpret_cast<double2* const*>(static_cast<void**>(ptr.p) + at); };
+    // orthonormalise the columns in place (two Gram-Schmidt passes each; a vanishing column is an error)
+    auto orthonormalise = [&](std::vector<DevBuf<double2>*> cols, std::vector<DevBuf<double2>*> against) {
+        for (std::size_t c = 0; c < cols.size(); ++c) {
+            std::vector<double2*> prev;
+            for (auto* a : against) prev.push_back(a->p);
+            for (std::size_t d = 0; d < c; ++d) prev.push_back(cols[d]->p);
+            if (!prev.empty()) {
+                set_ptrs(0, prev);
+                for (int pass = 0; pass < 2; ++pass) {
+                    dot_many<double2>(n, static_cast<int>(prev.size()), dptr(0), cols[c]->p, coef.p, part.p, nullptr, nullptr);
+                    k_axpy_many<double2><<<nb, kThreads>>>(n, static_cast<int>(prev.size()), dptr(0), coef.p, cols[c]->p,
+                                                           nullptr);
+                }
+            }
+            k_norm_to<<<nb, kThreads>>>(n, cols[c]->p, red, slots.p, nullptr);
+            double nrm = 0.0;
+            cuda_check(cudaMemcpy(&nrm, slots.p, 8, cudaMemcpyDeviceToHost), "norm");
+            if (!(nrm > 0.0)) throw Error(QB_ECUDA, "refinement: a vanishing direction");
+            k_unit_inplace<<<nb, kThreads>>>(n, cols[c]->p, slots.p);
+        }
+    };
+    // G = Q^H (A Q), Hermitian, from the columns of Q and AQ (FP64)
+    auto gram = [&](const std::vector<double2*>& Q, const std::vector<double2*>& AQ) {
+        const int q = static_cast<int>(Q.size());
+        set_ptrs(0, Q);
+        std::vector<cd> G(static_cast<std::size_t>(q) * q);
+        std::vector<double2> h(q);
+        for (int c = 0; c < q; ++c) {
+            dot_many<double2>(n, q, dptr(0), AQ[c], coef.p, part.p, nullptr, nullptr);
+            cuda_check(cudaMemcpy(h.data(), coef.p, q * 16, cudaMemcpyDeviceToHost), "gram");
+            for (int r = 0; r < q; ++r) G[static_cast<std::size_t>(c) * q + r] = cd(-h[r].x, -h[r].y);
+        }
+        for (int c = 0; c < q; ++c)   // Hermitian part (the two triangles differ by rounding)
+            for (int r = 0; r < c; ++r) {
+                const cd a = 0.5 * (G[static_cast<std::size_t>(c) * q + r] + std::conj(G[static_cast<std::size_t>(r) * q + c]));
+                G[static_cast<std::size_t>(c) * q + r] = a;
+                G[static_cast<std::size_t>(r) * q + c] = std::conj(a);
+            }
+        for (int c = 0; c < q; ++c) G[static_cast<std::size_t>(c) * q + c] = G[static_cast<std::size_t>(c) * q + c].real();
+        return G;
+    };
+    auto rotate = [&](const std::vector<double2*>& in, const std::vector<cd>& Y, int cols, const std::vector<double2*>& outv) {
+        const int nin = static_cast<int>(in.size());
+        if (nin * cols > kRotMaxCoef) throw Error(QB_EINVAL, "refinement: too many vectors");
+        set_ptrs(0, in);
+        set_ptrs(in.size(), outv);
+        std::vector<double2> y(static_cast<std::size_t>(nin) * cols);
+        for (int c = 0; c < cols; ++c)
+            for (int r = 0; r < nin; ++r) {
+                const cd z = Y[static_cast<std::size_t>(c) * nin + r];
+                y[static_cast<std::size_t>(c) * nin + r] = make_double2(z.real(), z.imag());
+            }
+        cuda_check(cudaMemcpy(Yd.p, y.data(), y.size() * 16, cudaMemcpyHostToDevice), "rotation");
+        k_rotate_cplx<<<nb, kThreads>>>(n, nin, cols, dptr(0), Yd.p, optr(in.size()));
+        cuda_check(cudaGetLastError(), "rotate");
+    };
+    auto colsp = [](std::vector<DevBuf<double2>>& v, int cnt) {
+        std::vector<double2*> o;
+        for (int c = 0; c < cnt; ++c) o.push_back(v[c].p);
+        return o;
+    };
+    std::vector<DevBuf<double2>*> xs;
+    for (auto& x : X) xs.push_back(&x);
+    orthonormalise(xs, {});
+    for (int c = 0; c < k; ++c) launch_walk_mixed(sec, sec, prog, X[c].p, AX[c].p, QB_C128, QB_C128, nullptr);
+    out.matvecs += k;
+    // Rayleigh-Ritz on span{X} first: its values are already accurate to the square of the residual
+    {
+        const std::vector<cd> G = gram(colsp(X, k), colsp(AX, k));
+        std::vector<double> vals;
+        std::vector<cd> Y;
+        hermitian_eig(G, k, vals, Y);
+        rotate(colsp(X, k), Y, k, colsp(T1, k));
+        rotate(colsp(AX, k), Y, k, colsp(R, k));
+        for (int c = 0; c < k; ++c) {
+            std::swap(X[c], T1[c]);
+            std::swap(AX[c], R[c]);
+        }
+        values = vals;
+    }
+    for (int round = 0;; ++round) {
+        // residuals and their norms
+        cuda_check(cudaMemcpy(th.p, values.data(), k * 8, cudaMemcpyHostToDevice), "theta");
+        std::vector<double2*> xp = colsp(X, k), axp = colsp(AX, k), rp = colsp(R, k);
+        set_ptrs(0, xp);
+        set_ptrs(k, axp);
+        set_ptrs(2 * k, rp);
+        k_residuals<<<nb, kThreads>>>(n, k, dptr(0), dptr(k), th.p, optr(2 * k));
+        double worst = 0.0;
+        for (int c = 0; c < k; ++c) k_norm_to<<<nb, kThreads>>>(n, R[c].p, red, slots.p + c, nullptr);
+        std::vector<double> rn(k);
+        cuda_check(cudaMemcpy(rn.data(), slots.p, k * 8, cudaMemcpyDeviceToHost), "residual norms");
+        for (double r : rn) worst = std::max(worst, r);
+        out.max_residual = worst;
+        if (worst <= tol || round >= kRefineMax) {
+            out.refine_rounds = round;
+            return;
+        }
+        // Rayleigh-Ritz on span{X, R}: R orthonormalised against X and itself, A R, the 2k x 2k problem
+        std::vector<DevBuf<double2>*> rs;
+        for (auto& r : R) rs.push_back(&r);
+        orthonormalise(rs, xs);
+        for (int c = 0; c < k; ++c) launch_walk_mixed(sec, sec, prog, R[c].p, AR[c].p, QB_C128, QB_C128, nullptr);
+        out.matvecs += k;
+        std::vector<double2*> Q = colsp(X, k), AQ = colsp(AX, k);
+        for (int c = 0; c < k; ++c) {
+            Q.push_back(R[c].p);
+            AQ.push_back(AR[c].p);
+        }
+        const std::vector<cd> G = gram(Q, AQ);
+        std::vector<double> vals;
+        std::vector<cd> Y;
+        hermitian_eig(G, 2 * k, vals, Y);
+        rotate(Q, Y, k, colsp(T1, k));
+        std::vector<double2*> t2;
+        for (int c = 0; c < k; ++c) t2.push_back(T1[k + c].p);
+        rotate(AQ, Y, k, t2);
+        for (int c = 0; c < k; ++c) {
+            std::swap(X[c], T1[c]);
+            std::swap(AX[c], T1[k + c]);
+        }
+        xs.clear();
+        for (auto& x : X) xs.push_back(&x);
+        values.assign(vals.begin(), vals.begin() + k);
+    }
+}
+
+template <class T>
+LevelsOut levels(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t max_iter, bool refine,
+                 bool want_vectors) {
+    LevelsOut out;
+    const std::uint64_t n = sec->dim;
+    if (n == 0) {
+        out.converged = true;
+        return out;
+    }
+    const std::uint64_t budget = max_iter > 0 ? max_iter : std::max<std::uint64_t>(200ull * k, 2000);
+    std::vector<DevBuf<double2>> X;
+    {
+        ThickRestart<T> tr(sec, prog, k, budget);
+        tr.run(out);
+        if (want_vectors || refine) {
+            for (T* v : tr.sorted_vectors()) {
+                DevBuf<double2> x(n);
+                k_copy_cast<T><<<red_blocks(n), kThreads>>>(n, v, x.p);
+                X.push_back(std::move(x));
+            }
+            cuda_check(cudaGetLastError(), "vectors");
+        }
+    }
+    if (refine && !X.empty()) {
+        refine_pairs(sec, prog, X, out.values, kLockTol * norm_bound(prog), out);
+        if (out.max_residual > kLockTol * norm_bound(prog)) out.converged = false;
+    }
+    if (want_vectors) out.vectors = std::move(X);
+    return out;
+}
+
+}  // namespace
+}  // namespace qb
+
+extern "C" {
+
+int qb_eigs_k(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, double* values, int* n_found,
+              int* converged, int* matvecs, void* const* vecs_device) {
+    return qb_eigs_levels(sec, prog, k, max_iter, QB_C128, 0, values, n_found, converged, matvecs, vecs_device);
+}
+
+int qb_eigs_levels(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, int dtype, int refine,
+                   double* values, int* n_found, int* converged, int* matvecs, void* const* vecs_device) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!sec || !prog || !values || k < 1) throw Error(QB_EINVAL, "bad argument");
+        if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "dtype must be QB_C128 or QB_C64");
+        const bool vecs = vecs_device != nullptr;
+        LevelsOut r = dtype == QB_C64 ? levels<float2>(sec, prog, k, max_iter, refine != 0, vecs)
+                                      : levels<double2>(sec, prog, k, max_iter, false, vecs);
+        for (int i = 0; i < k; ++i) values[i] = i < static_cast<int>(r.values.size()) ? r.values[i] : std::nan("");
+        if (n_found) *n_found = static_cast<int>(r.values.size());
+        if (converged) *converged = r.converged ? 1 : 0;
+        if (matvecs) *matvecs = r.matvecs;
+        if (vecs)
+            for (std::size_t i = 0; i < r.vectors.size(); ++i)
+                if (vecs_device[i])
+                    cuda_check(cudaMemcpy(vecs_device[i], r.vectors[i].p, sec->dim * 16, cudaMemcpyDeviceToDevice),
+                               "vector copy");
+    });
+}
+
+}  // extern "C"

@@ -5,13 +5,10 @@
 //                    reorthogonalisation from staged_seed(0x51ED900D), the Ritz vector from the basis kept
 //                    on the way or from a replay of the recurrence, then H u: the Rayleigh quotient and
 //                    the residual; restarted from u until ||H u - E u|| <= 1e-9 * scale.
-//   qb_eigs_k        the k > 1 lane (krylov_schur_lane, block_solve.cpp:433-510, over krylov_schur_kernel,
-//                    include/ed/krylov/krylov_schur.h:95-312): thick-restart Krylov-Schur with full CGS2,
-//                    exact pairs of an invariant subspace kept, fresh deflated starts, a degeneracy probe.
 //   qb_dynamics_t0   T = 0 dynamics of a cross-sector operator (src/engine/dynamics.cpp:442-566): the
 //                    source's ground state, phi = O psi0 on the target sector, the continued fraction of
 //                    H_target from phi with the source's E0 as the energy shift.
-// The projected eigenproblems are solved on the host (cyclic Jacobi); every vector stays on the device.
+// Every vector stays on the device. (The k > 1 lane, qb_eigs_k / qb_eigs_levels, is in eigs_k.cu.)
 // =============================================================================
 #include <algorithm>
 #include <cmath>
@@ -30,11 +27,9 @@ namespace qb {
 namespace {
 
 constexpr std::uint64_t kGsStartSeed = 0x51ED900DULL;    // block_solve.cpp:264
-constexpr std::uint64_t kKsStartSeed = 0x51ED0B70ULL;    // block_solve.cpp:263
 constexpr int kGsMaxIter = 600;                          // kLgGsMaxIter, src/engine/internal.h:118
 constexpr int kGsRestarts = 4;                           // kLgGsRestarts, internal.h:119
 constexpr double kGsResidRel = 1e-9;                     // include/ed/core/numerics.h:27
-constexpr double kLockRel = 1e-10;                       // numerics.h:25
 constexpr double kBreakdownRel = 64.0 * std::numeric_limits<double>::epsilon();   // numerics.h:23
 
 // Scratch of the deterministic grid reductions of one driver.
@@ -84,87 +79,6 @@ __global__ void k_unit(std::uint64_t n, double2* x, const double* nrm) {
          i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
         x[i].x *= s;
         x[i].y *= s;
-    }
-}
-
-// out[:, c] = sum_r V[:, r] S[r, c] for c in [c0, c0 + kRotCols) and c < cols; V and out column-major with
-// leading dimension n, S column-major mm x cols (real).
-constexpr int kRotCols = 8;
-__global__ void k_rotate(std::uint64_t n, int mm, int cols, int c0, const double2* V, const double* S, double2* out) {
-    extern __shared__ double Ss[];
-    const int nc = min(kRotCols, cols - c0);
-    for (int t = threadIdx.x; t < mm * nc; t += blockDim.x) Ss[t] = S[static_cast<std::size_t>(c0) * mm + t];
-    __syncthreads();
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        double2 acc[kRotCols];
-#pragma unroll
-        for (int c = 0; c < kRotCols; ++c) acc[c] = make_double2(0.0, 0.0);
-        for (int r = 0; r < mm; ++r) {
-            const double2 v = V[static_cast<std::size_t>(r) * n + i];
-#pragma unroll
-            for (int c = 0; c < kRotCols; ++c)
-                if (c < nc) {
-                    const double s = Ss[c * mm + r];
-                    acc[c].x += s * v.x;
-                    acc[c].y += s * v.y;
-                }
-        }
-#pragma unroll
-        for (int c = 0; c < kRotCols; ++c)
-            if (c < nc) out[static_cast<std::size_t>(c0 + c) * n + i] = acc[c];
-    }
-}
-
-// Eigenpairs of a real symmetric m x m matrix (column-major), ascending; vectors column-major (vector c at
-// [c * m, (c + 1) * m)). Cyclic Jacobi rotations to an off-diagonal norm of 1e-15 of the matrix norm.
-void jacobi_eig(std::vector<double> A, int m, std::vector<double>& vals, std::vector<double>& vecs) {
-    std::vector<double> Vm(static_cast<std::size_t>(m) * m, 0.0);
-    for (int i = 0; i < m; ++i) Vm[static_cast<std::size_t>(i) * m + i] = 1.0;
-    auto at = [&](int r, int c) -> double& { return A[static_cast<std::size_t>(c) * m + r]; };
-    double fro = 0.0;
-    for (double x : A) fro += x * x;
-    for (int sweep = 0; sweep < 100; ++sweep) {
-        double off = 0.0;
-        for (int c = 0; c < m; ++c)
-            for (int r = 0; r < c; ++r) off += at(r, c) * at(r, c);
-        if (off <= 1e-30 * fro || off == 0.0) break;
-        for (int p = 0; p < m - 1; ++p)
-            for (int q = p + 1; q < m; ++q) {
-                const double apq = at(p, q);
-                if (apq == 0.0) continue;
-                const double theta = (at(q, q) - at(p, p)) / (2.0 * apq);
-                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
-                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < m; ++k) {   // columns p, q
-                    const double akp = at(k, p), akq = at(k, q);
-                    at(k, p) = c * akp - s * akq;
-                    at(k, q) = s * akp + c * akq;
-                }
-                for (int k = 0; k < m; ++k) {   // rows p, q
-                    const double apk = at(p, k), aqk = at(q, k);
-                    at(p, k) = c * apk - s * aqk;
-                    at(q, k) = s * apk + c * aqk;
-                }
-                at(p, q) = at(q, p) = 0.0;
-                for (int k = 0; k < m; ++k) {
-                    double& vkp = Vm[static_cast<std::size_t>(p) * m + k];
-                    double& vkq = Vm[static_cast<std::size_t>(q) * m + k];
-                    const double a = vkp, b = vkq;
-                    vkp = c * a - s * b;
-                    vkq = s * a + c * b;
-                }
-            }
-    }
-    std::vector<int> order(m);
-    for (int i = 0; i < m; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return at(a, a) < at(b, b); });
-    vals.resize(m);
-    vecs.assign(static_cast<std::size_t>(m) * m, 0.0);
-    for (int c = 0; c < m; ++c) {
-        vals[c] = at(order[c], order[c]);
-        std::copy(Vm.begin() + static_cast<std::size_t>(order[c]) * m,
-                  Vm.begin() + static_cast<std::size_t>(order[c] + 1) * m, vecs.begin() + static_cast<std::size_t>(c) * m);
     }
 }
 
@@ -293,234 +207,6 @@ GsOut gs_vector(const qb_sector* sec, const qb_program* prog, double2* u, int ma
         cuda_check(cudaMemcpy(seed.p, u, n * 16, cudaMemcpyDeviceToDevice), "restart");   // restarted refinement
     }
     return out;
-}
-
-// ---- the k > 1 lane: thick-restart Krylov-Schur ----
-struct KsOut {
-    std::vector<double> values;
-    std::vector<std::unique_ptr<DevBuf<double2>>> vectors;
-    bool converged = false, exhausted = false;
-    int matvecs = 0, restarts = 0;
-};
-
-KsOut krylov_schur(const qb_sector* sec, const qb_program* prog, int k_req, std::uint64_t max_iter) {
-    KsOut R;
-    const std::uint64_t n = sec->dim;
-    if (n == 0) {
-        R.converged = R.exhausted = true;
-        return R;
-    }
-    const std::size_t k = static_cast<std::size_t>(std::max(1, k_req));
-    const double scale = norm_bound(prog);
-    const double tol = kLockRel * scale;
-    const double breakdown = kBreakdownRel * scale;
-    // sizing (krylov_schur_lane, block_solve.cpp:449-468; krylov_subspace_dim, subspace_policy.h:30-39)
-    const std::uint64_t budget = max_iter > 0 ? max_iter : std::max<std::uint64_t>(200 * k, 2000);
-    std::size_t kdim = std::max<std::size_t>(2 * k + 20, 2 * k + 60);
-    kdim = static_cast<std::size_t>(std::min<std::uint64_t>(kdim, n));
-    kdim = std::max(kdim, k + 1);
-    const std::size_t per_cycle = std::min<std::size_t>(kdim, static_cast<std::size_t>(std::max<std::uint64_t>(budget, k + 1)));
-    const std::size_t p_want = k + std::max<std::size_t>(k / 2, 8);
-    const std::size_t fresh_per = std::max<std::size_t>(std::min(per_cycle, 2 * p_want + 20), p_want + 1) - p_want;
-    const std::size_t max_restarts = static_cast<std::size_t>(std::max<std::uint64_t>(1, budget / fresh_per));
-    const std::size_t m = std::max<std::size_t>(1, std::min<std::size_t>({per_cycle, 2 * p_want + 20, static_cast<std::size_t>(n)}));
-    const std::size_t p_keep = std::min(p_want, m > 1 ? m - 1 : std::size_t{1});
-    {
-        const std::size_t free_b = available_bytes();
-        const double need = static_cast<double>(m + 2 + p_keep + k) * n * 16.0;
-        if (need > 0.9 * static_cast<double>(free_b))
-            throw Error(QB_ENOMEM, "eigs: a Krylov-Schur cycle of " + std::to_string(m) + " vectors of dimension " +
-                                       std::to_string(n) + " does not fit the free device memory");
-    }
-    DevBuf<double2> V((m + 1) * n), w(n), U(std::max<std::size_t>(p_keep, k) * n);
-    DevBuf<double> dS(static_cast<std::size_t>(m) * m);
-    DevBuf<void*> dptr(m + 2 * k + 2);
-    DevBuf<double2> dcoef(m + 2 * k + 2), dpart(static_cast<std::size_t>(kMaxRedBlocks) + m + 2 * k + 2);
-    Reducer red;
-    const int nb = red_blocks(n);
-    auto col = [&](std::size_t j) { return V.p + j * n; };
-    std::vector<std::unique_ptr<DevBuf<double2>>> found;
-    std::vector<double> found_vals;
-
-    auto nrm2 = [&](const double2* x) {
-        k_norm_to<<<nb, kThreads>>>(n, x, red.scal(), red.slots.p, nullptr);
-        cuda_check(cudaGetLastError(), "norm");
-        return read_slot(red.slots.p);
-    };
-    auto scale_by = [&](double2* x, double nrm) {
-        cuda_check(cudaMemcpy(red.slots.p + 3, &nrm, 8, cudaMemcpyHostToDevice), "scalar");
-        k_unit<<<nb, kThreads>>>(n, x, red.slots.p + 3);
-    };
-    // CGS2 of x against the first j columns and the found vectors; the coefficients on the columns
-    auto orthogonalize = [&](double2* x, std::size_t j) {
-        std::vector<void*> b;
-        for (std::size_t i = 0; i < j; ++i) b.push_back(col(i));
-        for (const auto& f : found) b.push_back(f->p);
-        std::vector<std::complex<double>> c(b.size(), 0.0);
-        if (b.empty()) return c;
-        cuda_check(cudaMemcpy(dptr.p, b.data(), b.size() * sizeof(void*), cudaMemcpyHostToDevice), "basis");
-        std::vector<double2> h(b.size());
-        for (int pass = 0; pass < 2; ++pass) {
-            dot_many<double2>(n, static_cast<int>(b.size()), reinterpret_cast<const double2* const*>(dptr.p), x, dcoef.p,
-                              dpart.p, nullptr, nullptr);
-            k_axpy_many<double2><<<nb, kThreads>>>(n, static_cast<int>(b.size()),
-                                                   reinterpret_cast<const double2* const*>(dptr.p), dcoef.p, x, nullptr);
-            cuda_check(cudaGetLastError(), "cgs2");
-            cuda_check(cudaMemcpy(h.data(), dcoef.p, b.size() * 16, cudaMemcpyDeviceToHost), "coefficients");
-            for (std::size_t i = 0; i < b.size(); ++i) c[i] -= std::complex<double>(h[i].x, h[i].y);
-        }
-        c.resize(j);
-        return c;
-    };
-    auto rotate = [&](const std::vector<double>& S, std::size_t mm, std::size_t cols, double2* out) {
-        cuda_check(cudaMemcpy(dS.p, S.data(), mm * cols * 8, cudaMemcpyHostToDevice), "rotation");
-        for (std::size_t c0 = 0; c0 < cols; c0 += kRotCols)
-            k_rotate<<<nb, kThreads, mm * kRotCols * 8>>>(n, static_cast<int>(mm), static_cast<int>(cols),
-                                                          static_cast<int>(c0), V.p, dS.p, out);
-        cuda_check(cudaGetLastError(), "rotate");
-    };
-
-    enum Outcome { kConverged = 0, kBudget = 1, kNullSeed = 2, kNothingBelow = 3 };
-    auto search = [&](std::size_t want, std::size_t cycles, double give_up) -> Outcome {
-        orthogonalize(col(0), 0);
-        const double nrm = nrm2(col(0));
-        if (nrm < 1e-13) return kNullSeed;
-        scale_by(col(0), nrm);
-        std::size_t p = 0;
-        std::vector<double> theta, arrow;
-        for (std::size_t cycle = 0; cycle < cycles; ++cycle) {
-            std::vector<double> T(m * m, 0.0);
-            for (std::size_t i = 0; i < p; ++i) {
-                T[i + i * m] = theta[i];
-                T[i + p * m] = T[p + i * m] = arrow[i];
-            }
-            std::size_t mm = m;
-            double beta_last = 0.0;
-            for (std::size_t j = p; j < m; ++j) {
-                launch_walk_mixed(sec, sec, prog, col(j), w.p, QB_C128, QB_C128, nullptr);
-                ++R.matvecs;
-                const auto c = orthogonalize(w.p, j + 1);
-                T[j + j * m] = c[j].real();
-                const double beta = nrm2(w.p);
-                if (beta <= breakdown) {   // an invariant subspace: its Ritz pairs are exact
-                    mm = j + 1;
-                    beta_last = 0.0;
-                    break;
-                }
-                if (j + 1 < m) T[j + (j + 1) * m] = T[(j + 1) + j * m] = beta;
-                cuda_check(cudaMemcpy(col(j + 1), w.p, n * 16, cudaMemcpyDeviceToDevice), "column");
-                scale_by(col(j + 1), beta);
-                beta_last = beta;
-            }
-            ++R.restarts;
-            std::vector<double> Tm(mm * mm);
-            for (std::size_t c = 0; c < mm; ++c)
-                for (std::size_t r = 0; r < mm; ++r) Tm[c * mm + r] = T[c * m + r];
-            std::vector<double> vals, vecs;
-            jacobi_eig(std::move(Tm), static_cast<int>(mm), vals, vecs);
-            if (cycle == 0 && vals[0] >= give_up) return kNothingBelow;
-            const std::size_t top = std::min(want, mm);
-            std::size_t conv = 0;
-            while (conv < top && std::abs(beta_last) * std::abs(vecs[conv * mm + (mm - 1)]) < tol) ++conv;
-            const bool done = conv == top;
-            if (done || cycle + 1 == cycles) {
-                if (conv > 0) {
-                    rotate(vecs, mm, conv, U.p);
-                    for (std::size_t i = 0; i < conv; ++i) {
-                        auto x = std::make_unique<DevBuf<double2>>(n);
-                        cuda_check(cudaMemcpy(x->p, U.p + i * n, n * 16, cudaMemcpyDeviceToDevice), "found");
-                        found_vals.push_back(vals[i]);
-                        found.push_back(std::move(x));
-                    }
-                }
-                return done ? kConverged : kBudget;
-            }
-            // thick restart: the p lowest Ritz vectors, then the residual direction
-            p = std::min(p_keep, mm - 1);
-            rotate(vecs, mm, p, U.p);
-            cuda_check(cudaMemcpy(col(0), U.p, p * n * 16, cudaMemcpyDeviceToDevice), "restart");
-            cuda_check(cudaMemcpy(col(p), col(mm), n * 16, cudaMemcpyDeviceToDevice), "residual");
-            theta.assign(vals.begin(), vals.begin() + static_cast<std::ptrdiff_t>(p));
-            arrow.resize(p);
-            for (std::size_t i = 0; i < p; ++i) arrow[i] = beta_last * vecs[i * mm + (mm - 1)];
-        }
-        return kBudget;
-    };
-
-    // fresh starts: unit-variance complex Gaussians, one stream per purpose (krylov_schur.h:266-274); the
-    // imaginary part of each entry is drawn first, as the reference's Complex(nd(gen), nd(gen)) evaluates
-    std::vector<std::complex<double>> host(n);
-    auto fresh_seed = [&](std::mt19937_64& gen) {
-        std::normal_distribution<double> nd(0.0, 1.0);
-        for (auto& z : host) {
-            const double im = nd(gen);
-            const double re = nd(gen);
-            z = std::complex<double>(re, im);
-        }
-        cuda_check(cudaMemcpy(col(0), host.data(), n * 16, cudaMemcpyHostToDevice), "fresh start");
-    };
-    std::mt19937_64 fresh_gen(0xF8E5A7C3ULL);
-    {
-        const auto v0 = staged_seed(n, kKsStartSeed);
-        cuda_check(cudaMemcpy(col(0), v0.data(), n * 16, cudaMemcpyHostToDevice), "seed upload");
-    }
-    bool exhausted = false, stalled = false;
-    int null_starts = 0;
-    while (found_vals.size() < k && static_cast<std::size_t>(R.restarts) < max_restarts) {
-        const Outcome o = search(k - found_vals.size(), max_restarts - R.restarts, std::numeric_limits<double>::infinity());
-        if (o == kNullSeed) {
-            if (++null_starts >= 2) {
-                exhausted = true;
-                break;
-            }
-            fresh_seed(fresh_gen);
-            continue;
-        }
-        null_starts = 0;
-        if (o == kBudget) {
-            stalled = true;
-            break;
-        }
-        if (found_vals.size() < k) fresh_seed(fresh_gen);
-    }
-    bool converged = !stalled && found_vals.size() >= k;
-    // the degeneracy probe (krylov_schur.h:272-302)
-    if (!found_vals.empty() && !exhausted) {
-        std::mt19937_64 probe_gen(0xDE6E4E7AULL);
-        for (std::size_t round = 0; round < k; ++round) {
-            const double top = *std::max_element(found_vals.begin(), found_vals.end());
-            const double gap = std::max(10.0 * tol, 1e-8 * std::abs(top));
-            fresh_seed(probe_gen);
-            const std::size_t before = found_vals.size();
-            const Outcome o = search(1, std::max<std::size_t>(max_restarts, 1), top - gap);
-            if (o == kNothingBelow || o == kNullSeed) break;
-            if (found_vals.size() == before) {
-                converged = false;
-                break;
-            }
-            if (found_vals.back() >= top - gap) {
-                found_vals.pop_back();
-                found.pop_back();
-                break;
-            }
-            while (found_vals.size() > k) {
-                const auto hi = std::max_element(found_vals.begin(), found_vals.end()) - found_vals.begin();
-                found_vals.erase(found_vals.begin() + hi);
-                found.erase(found.begin() + hi);
-            }
-        }
-    }
-    std::vector<std::size_t> order(found_vals.size());
-    for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) { return found_vals[a] < found_vals[b]; });
-    for (std::size_t i : order) {
-        if (R.values.size() >= k) break;
-        R.values.push_back(found_vals[i]);
-        R.vectors.push_back(std::move(found[i]));
-    }
-    R.converged = (converged || exhausted) && (R.values.size() >= k || exhausted);
-    R.exhausted = exhausted;
-    return R;
 }
 
 // ---- the dense tail: the full spectrum of a small block ----
@@ -676,24 +362,6 @@ int qb_ground_state(const qb_sector* sec, const qb_program* prog, int max_steps,
         if (certified) *certified = g.certified ? 1 : 0;
         if (matvecs) *matvecs = g.matvecs;
         if (vec_host) cuda_check(cudaMemcpy(vec_host, u, sec->dim * 16, cudaMemcpyDeviceToHost), "vector download");
-    });
-}
-
-int qb_eigs_k(const qb_sector* sec, const qb_program* prog, int k, uint64_t max_iter, double* values, int* n_found,
-              int* converged, int* matvecs, void* const* vecs_device) {
-    return qb::guarded([&] {
-        using namespace qb;
-        if (!sec || !prog || !values || k < 1) throw Error(QB_EINVAL, "bad argument");
-        KsOut r = krylov_schur(sec, prog, k, max_iter);
-        for (int i = 0; i < k; ++i) values[i] = i < static_cast<int>(r.values.size()) ? r.values[i] : std::nan("");
-        if (n_found) *n_found = static_cast<int>(r.values.size());
-        if (converged) *converged = r.converged ? 1 : 0;
-        if (matvecs) *matvecs = r.matvecs;
-        if (vecs_device)
-            for (std::size_t i = 0; i < r.vectors.size(); ++i)
-                if (vecs_device[i])
-                    cuda_check(cudaMemcpy(vecs_device[i], r.vectors[i]->p, sec->dim * 16, cudaMemcpyDeviceToDevice),
-                               "vector copy");
     });
 }
 

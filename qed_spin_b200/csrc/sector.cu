@@ -67,129 +67,152 @@ struct SlcHost {
     std::vector<u16> cand;
 };
 
-// The block system with the largest blocks (<= 16 sites, 2..8 equal blocks), first found on ties:
-// the finest group-invariant partition joining sites 0 and b, for every b (sublattice_code.h:232-270).
-std::vector<int> block_system(const std::vector<std::vector<int>>& sp, int N, int& L) {
-    L = 0;
-    std::vector<int> best, parent(N);
-    auto find = [&](int x) {
-        while (parent[x] != x) {
-            parent[x] = parent[parent[x]];
-            x = parent[x];
-        }
-        return x;
-    };
-    for (int b = 1; b < N; ++b) {
-        std::iota(parent.begin(), parent.end(), 0);
-        parent[b] = 0;
-        std::vector<std::pair<int, int>> todo{{0, b}};
-        while (!todo.empty()) {
-            const auto [x, y] = todo.back();
-            todo.pop_back();
-            for (const auto& p : sp) {
-                const int px = p[x], py = p[y];
-                const int u = find(px), v = find(py);
-                if (u == v) continue;
-                parent[std::max(u, v)] = std::min(u, v);
-                todo.emplace_back(px, py);
-            }
-        }
-        std::vector<int> size(N, 0);
-        for (int s = 0; s < N; ++s) ++size[find(s)];
-        const int l = size[0];
-        if (l > 16 || l <= L || N % l != 0 || N / l < 2 || N / l > 8) continue;
-        bool equal = true;
-        for (int s = 0; s < N && equal; ++s) equal = size[find(s)] == l;
-        if (!equal) continue;
-        std::vector<int> root_block(N, -1), block(N);
-        int nb = 0;
-        for (int s = 0; s < N; ++s) {
-            int& rb = root_block[find(s)];
-            if (rb < 0) rb = nb++;
-            block[s] = rb;
-        }
-        L = l;
-        best = std::move(block);
+// ---- the sublattice key order ----------------------------------------------------------------
+// The rule (the reference's, include/ed/basis/sublattice_code.h:23-34 and 164-191; the tables it fixes are
+// what the representatives depend on, the code below is this file's own):
+//   * a block system is a partition of the sites that every element of the group maps block onto block;
+//   * for each site b = 1 .. N-1 in turn, the finest block system in which sites 0 and b share a block is a
+//     candidate; the code takes the first candidate with the largest block size L whose blocks are all of
+//     size L, with L <= 16 and 2 <= N / L <= 8 (none: no code);
+//   * blocks are numbered by their smallest site, and the t-th smallest site of block j takes key bit
+//     N - (j + 1) L + t, so block 0 leads the key;
+//   * an element g brings one block j(g) of the state onto block 0 of the image. For a pattern x of block j
+//     (bit t: the t-th site of the block), lead[j][x] is the least block-0 pattern (flips applied) among the
+//     elements with j(g) = j, and cand[j][x] lists, ascending, the elements that reach it.
+// The code applies only under the size rule of `mode`: 1 whenever a block system exists, -1 for N >= 24 and
+// at least 16 distinct permutations, -2 the same with 64; 0 never; nor for G <= 1, N < 4, N > 64, G > 65535.
+
+// The finest block system in which sites 0 and b share a block: as every element maps a block system onto
+// itself, it is the set of connected components of the graph whose edges are the images of the pair (0, b)
+// under the group. Returns the block of every site, blocks numbered by their smallest site.
+std::vector<int> pair_closure(const std::vector<std::vector<int>>& perms, int N, int b) {
+    std::vector<std::vector<int>> adj(N);
+    for (const auto& p : perms) {
+        adj[p[0]].push_back(p[b]);
+        adj[p[b]].push_back(p[0]);
     }
-    return best;
+    std::vector<int> label(N, -1);
+    int next = 0;
+    std::vector<int> stack;
+    for (int s = 0; s < N; ++s) {   // ascending sites: labels come in order of the blocks' smallest sites
+        if (label[s] >= 0) continue;
+        label[s] = next;
+        stack.assign(1, s);
+        while (!stack.empty()) {
+            const int u = stack.back();
+            stack.pop_back();
+            for (int v : adj[u])
+                if (label[v] < 0) {
+                    label[v] = next;
+                    stack.push_back(v);
+                }
+        }
+        ++next;
+    }
+    return label;
 }
 
-// The sublattice code of the group (sublattice_code.h:164-191 rule, 300-399 tables).
+// The chosen block system (block of every site) and its block size L, or an empty vector.
+std::vector<int> choose_blocks(const std::vector<std::vector<int>>& perms, int N, int& L) {
+    L = 0;
+    std::vector<int> chosen;
+    for (int b = 1; b < N; ++b) {
+        std::vector<int> block = pair_closure(perms, N, b);
+        const int nblocks = *std::max_element(block.begin(), block.end()) + 1;
+        if (N % nblocks != 0) continue;
+        const int l = N / nblocks;
+        if (l <= L || l > 16 || nblocks < 2 || nblocks > 8) continue;
+        std::vector<int> size(nblocks, 0);
+        for (int x : block) ++size[x];
+        if (std::any_of(size.begin(), size.end(), [l](int z) { return z != l; })) continue;
+        L = l;
+        chosen = std::move(block);
+    }
+    return chosen;
+}
+
+// The key-order tables of the group (perms G x N, flips G or null) under `mode`.
 SlcHost build_slc(const int32_t* perms, const u64* flips, int G, int N, int mode) {
     SlcHost c;
     if (mode == 0 || G <= 1 || N < 4 || N > 64 || G > 65535) return c;
-    const std::size_t min_perms = mode == 1 ? 0 : (mode == -1 ? 16 : 64);
-    std::vector<std::vector<int>> sp;
+    std::vector<std::vector<int>> distinct;
     for (int g = 0; g < G; ++g) {
-        std::vector<int> p(perms + g * N, perms + (g + 1) * N);
-        if (std::find(sp.begin(), sp.end(), p) == sp.end()) sp.push_back(std::move(p));
+        std::vector<int> p(perms + static_cast<std::size_t>(g) * N, perms + static_cast<std::size_t>(g + 1) * N);
+        if (std::find(distinct.begin(), distinct.end(), p) == distinct.end()) distinct.push_back(std::move(p));
     }
-    if (min_perms > 0 && (N < 24 || sp.size() < min_perms)) return c;
+    if (mode != 1) {
+        const std::size_t least = mode == -1 ? 16 : 64;
+        if (N < 24 || distinct.size() < least) return c;
+    }
     int L = 0;
-    const std::vector<int> block = block_system(sp, N, L);
+    const std::vector<int> block = choose_blocks(distinct, N, L);
     if (block.empty()) return c;
+    const int m = N / L;
+    // members[j]: block j's sites ascending; slot[s]: the position of site s in its block
+    std::vector<std::vector<int>> members(m);
+    std::vector<int> slot(N);
+    for (int s = 0; s < N; ++s) {
+        slot[s] = static_cast<int>(members[block[s]].size());
+        members[block[s]].push_back(s);
+    }
     c.on = true;
     c.L = L;
-    c.m = N / L;
+    c.m = m;
     const int bpw = (N + 7) / 8;
-    std::vector<int> key_bit(N, 0);
-    std::vector<std::vector<int>> sites(c.m);
-    for (int s = 0; s < N; ++s) sites[block[s]].push_back(s);
-    for (int j = 0; j < c.m; ++j)
-        for (int t = 0; t < L; ++t) key_bit[sites[j][t]] = N - (j + 1) * L + t;
+    std::vector<int> key_bit(N);
+    for (int s = 0; s < N; ++s) key_bit[s] = N - (block[s] + 1) * L + slot[s];
     c.to_key.assign(static_cast<std::size_t>(bpw) * 256, 0ULL);
-    for (int b = 0; b < bpw; ++b)
-        for (int v = 0; v < 256; ++v) {
-            u64 out = 0;
-            for (int t = 0; t < 8 && 8 * b + t < N; ++t)
-                if ((v >> t) & 1) out |= 1ULL << key_bit[8 * b + t];
-            c.to_key[b * 256 + v] = out;
-        }
-    const std::size_t P = std::size_t{1} << L;
-    const u32 lmask = (1u << L) - 1u;
-    std::vector<int> src_block(G), pos_in_block(N, -1);
-    std::vector<std::vector<u32>> e(G, std::vector<u32>(L, 0u));
-    std::vector<u32> fl(G, 0u);
-    for (int j = 0; j < c.m; ++j)
-        for (int t = 0; t < L; ++t) pos_in_block[sites[j][t]] = t;
-    for (int g = 0; g < G; ++g) {
-        const int32_t* p = perms + g * N;
-        src_block[g] = block[p[sites[0][0]]];
-        for (int t = 0; t < L; ++t) {
-            const int i = sites[0][t];
-            e[g][pos_in_block[p[i]]] = 1u << t;
-            if (flips && ((flips[g] >> i) & 1ULL)) fl[g] |= 1u << t;
-        }
-    }
-    const std::size_t M = static_cast<std::size_t>(c.m) * P;
-    c.lead.assign(M, 0xFFFFu);
-    std::vector<u32> img(P), count(M, 0);
-    auto images = [&](int g) {
-        img[0] = 0;
-        for (std::size_t x = 1; x < P; ++x) img[x] = img[x & (x - 1)] | e[g][__builtin_ctzll(x)];
-        for (std::size_t x = 0; x < P; ++x) img[x] = (img[x] ^ fl[g]) & lmask;
+    for (int s = 0; s < N; ++s)   // byte table b, value v: the key bits of the set sites of byte b
+        for (int v = 0; v < 256; ++v)
+            if ((v >> (s & 7)) & 1) c.to_key[static_cast<std::size_t>(s >> 3) * 256 + v] |= 1ULL << key_bit[s];
+    // each element as two byte tables over a source-block pattern, its flip pattern and its source block
+    struct Elem {
+        int src;
+        u32 flip;
+        u32 lo[256], hi[256];
     };
+    std::vector<Elem> el(G);
     for (int g = 0; g < G; ++g) {
-        images(g);
-        u16* row = c.lead.data() + static_cast<std::size_t>(src_block[g]) * P;
-        for (std::size_t x = 0; x < P; ++x)
-            if (img[x] < row[x]) row[x] = static_cast<u16>(img[x]);
+        const int32_t* p = perms + static_cast<std::size_t>(g) * N;
+        Elem& e = el[g];
+        e.src = block[p[members[0][0]]];
+        e.flip = 0;
+        std::fill(e.lo, e.lo + 256, 0u);
+        std::fill(e.hi, e.hi + 256, 0u);
+        for (int t = 0; t < L; ++t) {
+            const int from = slot[p[members[0][t]]];   // image bit t reads source-pattern bit `from`
+            u32* tab = from < 8 ? e.lo : e.hi;
+            for (int v = 0; v < 256; ++v)
+                if ((v >> (from & 7)) & 1) tab[v] |= 1u << t;
+            if (flips && ((flips[g] >> members[0][t]) & 1ULL)) e.flip |= 1u << t;
+        }
     }
-    for (int g = 0; g < G; ++g) {
-        images(g);
-        const std::size_t base = static_cast<std::size_t>(src_block[g]) * P;
-        for (std::size_t x = 0; x < P; ++x) count[base + x] += c.lead[base + x] == img[x] ? 1u : 0u;
+    const std::size_t P = std::size_t{1} << L;
+    c.lead.assign(static_cast<std::size_t>(m) * P, 0);
+    c.cand_off.assign(static_cast<std::size_t>(m) * P + 1, 0);
+    c.cand.clear();
+    std::vector<int> by_src;
+    for (int j = 0; j < m; ++j) {
+        by_src.clear();
+        for (int g = 0; g < G; ++g)
+            if (el[g].src == j) by_src.push_back(g);
+        for (std::size_t x = 0; x < P; ++x) {
+            const std::size_t at = static_cast<std::size_t>(j) * P + x;
+            c.cand_off[at] = static_cast<u32>(c.cand.size());
+            u32 best = 0xFFFFFFFFu;
+            for (int g : by_src) {
+                const Elem& e = el[g];
+                const u32 img = (e.lo[x & 0xFF] | e.hi[(x >> 8) & 0xFF]) ^ e.flip;
+                if (img < best) {
+                    best = img;
+                    c.cand.resize(c.cand_off[at]);
+                }
+                if (img == best) c.cand.push_back(static_cast<u16>(g));
+            }
+            c.lead[at] = static_cast<u16>(best);
+        }
     }
-    c.cand_off.assign(M + 1, 0);
-    for (std::size_t i = 0; i < M; ++i) c.cand_off[i + 1] = c.cand_off[i] + count[i];
-    c.cand.assign(c.cand_off[M], 0);
-    std::vector<u32> fill(c.cand_off.begin(), c.cand_off.end() - 1);
-    for (int g = 0; g < G; ++g) {
-        images(g);
-        const std::size_t base = static_cast<std::size_t>(src_block[g]) * P;
-        for (std::size_t x = 0; x < P; ++x)
-            if (c.lead[base + x] == img[x]) c.cand[fill[base + x]++] = static_cast<u16>(g);
-    }
+    c.cand_off[static_cast<std::size_t>(m) * P] = static_cast<u32>(c.cand.size());
     return c;
 }
 
@@ -700,6 +723,29 @@ int qb_device_count(int* count) {
         const cudaError_t e = cudaGetDeviceCount(&n);
         *count = e == cudaSuccess ? n : 0;
         if (e != cudaSuccess) (void)cudaGetLastError();
+    });
+}
+
+int qb_key_order(const qb_sector_desc* d, int* L, int* m, uint64_t* n_cand, int32_t* key_bit, uint16_t* lead,
+                 uint32_t* cand_off, uint16_t* cand) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (!d || !L || !m || !n_cand || !d->perms || d->n_sites < 1 || d->n_sites > 64 || d->group_size < 1)
+            throw Error(QB_EINVAL, "key order: bad descriptor");
+        const SlcHost c = build_slc(d->perms, reinterpret_cast<const u64*>(d->flips), d->group_size, d->n_sites,
+                                    d->sublattice_mode);
+        *L = c.on ? c.L : 0;
+        *m = c.on ? c.m : 0;
+        *n_cand = c.on ? c.cand.size() : 0;
+        if (!c.on) return;
+        if (key_bit)
+            for (int s = 0; s < d->n_sites; ++s) {   // the key bit of site s: the one bit of its byte table entry
+                const u64 e = c.to_key[static_cast<std::size_t>(s >> 3) * 256 + (1u << (s & 7))];
+                key_bit[s] = __builtin_ctzll(e);
+            }
+        if (lead) std::copy(c.lead.begin(), c.lead.end(), lead);
+        if (cand_off) std::copy(c.cand_off.begin(), c.cand_off.end(), cand_off);
+        if (cand) std::copy(c.cand.begin(), c.cand.end(), cand);
     });
 }
 

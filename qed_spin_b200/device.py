@@ -108,6 +108,26 @@ class Sector:
         return idx, proj.view(np.complex128)
 
 
+def key_order(spec: SectorSpec, sublattice_mode: int = -1) -> dict:
+    """The sublattice key order of a sector descriptor and its tables (host work only, no device needed): None
+    when the plain order applies, else L, m, key_bit, lead, cand_off, cand (qb_key_order)."""
+    keep = []
+    d = _sector_desc(spec, keep)
+    d.sublattice_mode = sublattice_mode
+    L_, m_, nc = C.c_int(), C.c_int(), C.c_uint64()
+    check(lib().qb_key_order(C.byref(d), C.byref(L_), C.byref(m_), C.byref(nc), None, None, None, None))
+    if L_.value == 0:
+        return None
+    P = m_.value << L_.value
+    kb = np.zeros(spec.n_sites, np.int32)
+    lead = np.zeros(P, np.uint16)
+    off = np.zeros(P + 1, np.uint32)
+    cand = np.zeros(max(1, nc.value), np.uint16)
+    check(lib().qb_key_order(C.byref(d), C.byref(L_), C.byref(m_), C.byref(nc), kb.ctypes.data, lead.ctypes.data,
+                             off.ctypes.data, cand.ctypes.data))
+    return {"L": L_.value, "m": m_.value, "key_bit": kb, "lead": lead, "cand_off": off, "cand": cand[: nc.value]}
+
+
 class Program:
     """A row program resident on the device."""
 
@@ -267,17 +287,20 @@ def ground_state(sec: Sector, prog: Program, max_steps: int = 0, vector: bool = 
     return {"e0": e0.value, "residual": res.value, "certified": bool(cert.value), "matvecs": mv.value, "vector": vec}
 
 
-def eigs(sec: Sector, prog: Program, k: int, max_iter: int = 0, vectors: bool = False) -> dict:
-    """The k lowest levels: the k = 1 scan lane for k == 1, thick-restart Krylov-Schur for k > 1."""
+def eigs(sec: Sector, prog: Program, k: int, max_iter: int = 0, vectors: bool = False, dtype="c128",
+         refine: bool = True) -> dict:
+    """The k lowest levels: the k = 1 scan lane for k == 1 (without vectors), thick-restart Lanczos for k > 1.
+    dtype "c64" stores the Lanczos vectors in FP32; refine then polishes every pair in FP64."""
     if k == 1 and not vectors:
-        r = eigs_lowest(sec, prog, max_iter)
+        r = eigs_lowest(sec, prog, max_iter, dtype=dtype, refine=refine)
         return {"values": np.array([r["e0"]]), "converged": r["converged"], "matvecs": r["matvecs"]}
     vals = np.zeros(k)
     nf, cv, mv = C.c_int(), C.c_int(), C.c_int()
     import torch
     vecs = [torch.empty(sec.dim, dtype=torch.complex128, device="cuda") for _ in range(k)] if vectors else None
     ptrs = (C.c_void_p * k)(*[v.data_ptr() for v in vecs]) if vectors else None
-    check(lib().qb_eigs_k(sec.h, prog.h, k, max_iter, vals.ctypes.data, C.byref(nf), C.byref(cv), C.byref(mv), ptrs))
+    check(lib().qb_eigs_levels(sec.h, prog.h, k, max_iter, _dt(dtype), 1 if refine else 0, vals.ctypes.data,
+                               C.byref(nf), C.byref(cv), C.byref(mv), ptrs))
     out = {"values": vals[: nf.value], "converged": bool(cv.value), "matvecs": mv.value}
     if vectors:
         out["vectors"] = [v.cpu().numpy() for v in vecs[: nf.value]]

@@ -3,7 +3,7 @@
 Run in a tree where the reference sources are present (it reads them and its compiled CPU engine,
 oracle/_ref/libqed_ref.so, built by `make -C oracle`):
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT] [--json-only]
+    python tests/golden/make_golden.py REFERENCE_ROOT [--json-only]
 
 (--json-only rewrites golden.json alone, leaving fixtures.npz as it is.)
 
@@ -209,4 +209,6 @@ def main(ref_root: str, json_only: bool = False):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else "/root/reference", json_only="--json-only" in sys.argv[1:])
+    if not args:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [--json-only]")
+    main(args[0], json_only="--json-only" in sys.argv[1:])

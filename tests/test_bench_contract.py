@@ -22,7 +22,7 @@ def test_reference_arm_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["metric"] == "H.v/s" and d["unit"] == "H.v/s"
     assert d["higher_is_better"] is True and d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 3
-    assert d["config"]["workload"] and d["config"]["dim"] == 4707969
+    assert d["config"]["workload"] and d["config"]["dim"] == 252091362
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
     e2e = d["e2e"]

@@ -1,4 +1,4 @@
-"""Every reference citation in this tree's sources and notes (file:line or file:first-last) names a file of
+"""Every reference citation in this tree's sources (file:line or file:first-last) names a file of
 the reference and lines it has: full paths directly, bare file names by their unique name in the reference
 tree. Skipped where the reference sources are absent."""
 import collections
@@ -10,8 +10,7 @@ import pytest
 
 from conftest import ROOT
 
-SOURCES = ("qed_spin_b200", "include", "oracle", "tests", "bench.py", "__graft_entry__.py", "DESIGN.md",
-           "INTEGRATION.md")
+SOURCES = ("qed_spin_b200", "include", "oracle", "tests", "bench.py", "__graft_entry__.py")
 FULL = re.compile(r"\b((?:include|src|python|tests|docs|cmake)/[\w/.\-]+\.(?:h|hpp|cpp|cu|cuh|py)):(\d+)(?:-(\d+))?")
 BARE = re.compile(r"(?<![\w/])([\w\-]+\.(?:h|hpp|cpp|cu|cuh|py)):(\d+)(?:-(\d+))?")
 
@@ -35,7 +34,7 @@ def _files():
             if "_ref" in d or "__pycache__" in d:
                 continue
             for f in fs:
-                if f.endswith((".cu", ".cuh", ".h", ".hpp", ".cpp", ".py", ".md")):
+                if f.endswith((".cu", ".cuh", ".h", ".hpp", ".cpp", ".py")):
                     yield os.path.join(d, f)
 
 

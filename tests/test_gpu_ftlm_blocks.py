@@ -2,7 +2,7 @@
 
 The blocks are every (S^z, momentum) sector of an XXZ chain in a field: the decomposition the thermal driver
 samples (config 3 at N = 12). Each block's curves are checked against the oracle's FTLM of that block with the
-call's base seed (tolerances written per test: 1e-8 relative for FP64 storage, 2e-4 for FP32), and the combined
+call's base seed (tolerances written per test: 1e-8 relative for FP64 storage, 1e-6 for FP32), and the combined
 thermodynamics against the oracle's log-space combine.
 """
 import numpy as np
@@ -59,7 +59,7 @@ def test_blocks_match_oracle(oracle_curves, monkeypatch, dtype, use_csr, pack):
     secs = [D.Sector(s) for s in specs]
     P = D.Program(prog)
     r = D.ftlm_blocks(secs, P, 8, 30, SEED, BETAS, dtype=dtype, use_csr=use_csr)
-    tol = 1e-8 if dtype == "c128" else 2e-4
+    tol = 1e-8 if dtype == "c128" else 1e-6   # FP32 storage: the curves move by ~3e-8 relative
     assert len(curves) == r["lnZ"].shape[0] > 100
     for b, c in enumerate(curves):
         for key in ("lnZ", "E", "V"):

@@ -70,12 +70,15 @@ def test_ground_state(fixtures, name):
     assert res <= 1e-9 * _scale(prog)
 
 
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
 @pytest.mark.parametrize("name", NAMES)
-def test_eigs_k4(fixtures, name):
+def test_eigs_k4(fixtures, name, dtype):
+    """The k > 1 lane in FP64 storage, and in FP32 storage with the FP64 refinement of every pair: the levels
+    within 1e-9 * scale of the reference's and of a dense solve, each vector an eigenvector to 1e-8 * scale."""
     from qed_spin_b200 import device as D
     spec = CASE[name][1]
     prog = _prog(name)
-    r = D.eigs(D.Sector(spec), D.Program(prog), 4, vectors=True)
+    r = D.eigs(D.Sector(spec), D.Program(prog), 4, vectors=True, dtype=dtype, refine=True)
     assert r["converged"] and len(r["values"]) == 4
     sc = _scale(prog)
     np.testing.assert_allclose(r["values"], fixtures[f"{name}/ks4"], rtol=0, atol=1e-9 * sc)
@@ -84,6 +87,25 @@ def test_eigs_k4(fixtures, name):
     np.testing.assert_allclose(r["values"], w, rtol=0, atol=1e-9 * sc)
     for e, v in zip(r["values"], r["vectors"]):   # each returned vector is its level's eigenvector
         assert np.linalg.norm(So.gather(Po, v) - e * v) <= 1e-8 * sc
+
+
+def test_eigs_k6_degenerate_levels():
+    """A block without spatial symmetry (the S^z = 0 states of a Heisenberg ring N = 10, the identity group only):
+    the momenta k and -k make doubly degenerate levels, which one Krylov space cannot resolve; the lane's deflated
+    searches below the k-th level must find both members (against a dense solve, 1e-9 * scale), FP64 and FP32
+    storage."""
+    from qed_spin_b200 import device as D
+    N = 10
+    spec = lat.SectorSpec(N, N // 2, np.arange(N, dtype=np.int32)[None, :], np.ones(1, np.complex128))
+    prog = ops.row_program(ops.from_products(N, ops.heisenberg_products(lat.chain_bonds(N))))
+    So, Po = O.Sector(spec), O.Program(prog)
+    w = np.linalg.eigvalsh(_dense(So, Po))
+    assert np.min(np.diff(w[:6])) < 1e-9   # the block has degenerate levels among its lowest six
+    sc = _scale(prog)
+    for dtype in ("c128", "c64"):
+        r = D.eigs(D.Sector(spec), D.Program(prog), 6, dtype=dtype, refine=True)
+        assert r["converged"], dtype
+        np.testing.assert_allclose(r["values"], w[:6], rtol=0, atol=1e-9 * sc, err_msg=dtype)
 
 
 def test_eigs_k4_chain20():

@@ -195,7 +195,7 @@ def test_ftlm_and_cf(fixtures, name, dtype):
     P = d.Program(_prog(name))
     betas = 1.0 / np.linspace(0.1, 4.0, 40)
     f = d.ftlm(S, P, 8, 60, 20240601, betas, dtype=dtype)
-    tol = 1e-8 if dtype == "c128" else 2e-4
+    tol = 1e-8 if dtype == "c128" else 1e-6   # FP32 storage: the curves move by ~3e-8 relative
     for k in ("lnZ", "E", "V"):
         ref = fixtures[f"{name}/ftlm_{k}"]
         np.testing.assert_allclose(f[k], ref, rtol=tol, atol=tol * np.abs(ref).max())
