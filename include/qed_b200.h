@@ -240,6 +240,18 @@ int qb_dynamics_t0(const qb_sector* src, const qb_program* h_src, const qb_secto
                    const qb_program* op, int depth, const double* omega, int n_omega, double eta, double* S, double* e0,
                    double* conv_change, int* certified);
 
+/* T = 0 dynamics averaged over the ground manifold (src/engine/dynamics.cpp:147-195, 395-566; the ground manifold
+ * is every level within degeneracy_tol * (sum |coeff| of h_srcs[0]) of E0, include/ed/sectors/dynamics.h:17-21):
+ * the lowest level of every source block (the k = 1 lane); in each block at E0, every level within the window
+ * with its vector (the k > 1 lane, k doubled until a level lies above the window); then for each such state a,
+ * the continued fraction of h_tgts[b] from phi = ops[b] |a> in the target block tgts[b] of its source block b
+ * (ops[b]: rows in tgts[b], columns in srcs[b]), shifted by E0; S = the average over the manifold's states.
+ * manifold: the number of states averaged; certified: every solve converged. */
+int qb_dynamics_t0_manifold(int n_src, const qb_sector* const* srcs, const qb_program* const* h_srcs,
+                            const qb_sector* const* tgts, const qb_program* const* h_tgts, const qb_program* const* ops,
+                            int depth, const double* omega, int n_omega, double eta, double degeneracy_tol, double* S,
+                            double* e0, int* manifold, int* certified);
+
 /* The full spectrum of a small block (at most 8192 states), ascending, with multiplicity: the dense tail of
  * the thermal and eigs drivers (blocks up to dense_max_dim are solved exactly, include/ed/sectors/thermal.h:35).
  * The block is assembled on the device from the block matvec on identity columns; the host reduces it by
@@ -257,18 +269,23 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
             int n_beta, int dtype, double* lnZ, double* E, double* V, double* e_min);
 
 /* FTLM over many blocks, the sampled per-block path of the thermal driver (src/engine/thermal.cpp:155-340
- * over the blocks of one call): every block uses the call's seed, so sample s of block b is the first dim_b
- * draws of sample_engine(seed, s) (sample_seed.h:37-89); one table of those streams, drawn once, serves every
- * block. (The reference's driver advances the seed by a 64-bit LCG step before each sampled block,
- * thermal.cpp:470-471: a one-block call given the advanced seed draws its vectors exactly; over many blocks the
- * two agree in distribution, not draw for draw.) Blocks run largest first on a few streams; each block's samples advance
- * together as one block matvec, on the block's reduced CSR (built inside the call) when use_csr != 0 and it
- * fits, else on the row walk. Outputs per block b and beta t at [b * n_beta + t]: lnZ, E, V; e_min[b].
- * stats (NULL or 4 doubles): seconds spent drawing the samples, building the CSRs, running the recurrences,
- * and forming the curves (the per-block build / apply times the thermal driver reports). */
+ * over the blocks of one call). seed_mode picks the sample vectors:
+ *   QB_SEED_PER_BLOCK  the driver's own streams: before each block, in the order given, the seed takes one step
+ *                      of the 64-bit LCG seed * 6364136223846793005 + 1442695040888963407 (thermal.cpp:470-471),
+ *                      and sample s of block b is the first dim_b draws of sample_engine(seed_b, s)
+ *                      (sample_seed.h:37-89): the reference's vectors draw for draw, given the blocks in its
+ *                      order;
+ *   QB_SEED_SHARED     every block uses the call's seed (sample s of block b: the first dim_b draws of
+ *                      sample_engine(seed, s)), so one table of streams, drawn once, serves every block.
+ * Blocks run largest first on a few streams; each block's samples advance together as one block matvec, on the
+ * block's reduced CSR (built inside the call) when use_csr != 0 and it fits, else on the row walk. Outputs per
+ * block b and beta t at [b * n_beta + t]: lnZ, E, V; e_min[b]. stats (NULL or 4 doubles): seconds spent drawing
+ * the samples, building the CSRs, running the recurrences, and forming the curves (the per-block build / apply
+ * times the thermal driver reports). */
+enum { QB_SEED_SHARED = 0, QB_SEED_PER_BLOCK = 1 };
 int qb_ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int samples, int depth,
-                   uint64_t seed, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ, double* E,
-                   double* V, double* e_min, double* stats);
+                   uint64_t seed, int seed_mode, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ,
+                   double* E, double* V, double* e_min, double* stats);
 
 /* The blocks' curves combined in log space (src/engine/thermal.cpp:599-641): lnZ = logsumexp_b(ln w_b +
  * lnZ_b), E = sum_b p_b E_b, C = beta^2 sum_b p_b (V_b + (E_b - E)^2) (the law of total variance), S = lnZ +

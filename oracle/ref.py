@@ -73,6 +73,8 @@ def lib():
     L.qref_csr_spmv_real.argtypes = [vp, _f64p, _f64p]
     L.qref_csr_build_rows.restype = vp
     L.qref_csr_build_rows.argtypes = [vp, vp, C.c_uint64, C.c_uint64]
+    L.qref_csr_build_rowlist.restype = vp
+    L.qref_csr_build_rowlist.argtypes = [vp, vp, _u64p, C.c_uint64]
     L.qref_ftlm_blocks.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint64, _f64p, C.c_int, _f64p, _f64p,
                                    _f64p, _f64p]
     L.qref_csr_bytes.restype = C.c_uint64
@@ -342,12 +344,16 @@ class Csr:
     """The reference's ReducedSymmetryCsr of a program on one sector, kept for repeated spmv."""
 
     def __init__(self, sector: "Sector", prog: Program, rows=None):
-        """rows: None for every row, or (r0, n) for the merged rows r0 .. r0 + n - 1 alone (columns over the
-        whole sector)."""
+        """rows: None for every row, (r0, n) for the merged rows r0 .. r0 + n - 1 alone, or an array of rows
+        (columns over the whole sector)."""
         L = lib()
         if rows is None:
             self.dim = sector.dim
             self.h = L.qref_csr_build(sector.h, prog.h)
+        elif isinstance(rows, np.ndarray):
+            rows = np.ascontiguousarray(rows, np.uint64)
+            self.dim = len(rows)
+            self.h = L.qref_csr_build_rowlist(sector.h, prog.h, rows, len(rows))
         else:
             self.dim = int(rows[1])
             self.h = L.qref_csr_build_rows(sector.h, prog.h, int(rows[0]), int(rows[1]))
@@ -364,6 +370,16 @@ class Csr:
 
     def spmv(self, x: np.ndarray, y: np.ndarray) -> None:
         _check(lib().qref_csr_spmv(self.h, x.view(np.float64), y.view(np.float64)))
+
+    def arrays(self):
+        """row_ptr (rows + 1), columns and values of the CSR."""
+        L = lib()
+        nnz = self.nnz
+        rp = np.zeros(self.dim + 1, np.uint64)
+        col = np.zeros(nnz, np.uint32)
+        val = np.zeros(2 * nnz, np.float64)
+        L.qref_csr_get(self.h, rp, col, val)
+        return rp, col, val.view(np.complex128)
 
     def spmv_real(self, x: np.ndarray, y: np.ndarray) -> bool:
         """y = Re(A) x on float64 vectors (the host lane of a real sector); False when A is not real."""

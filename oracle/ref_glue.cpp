@@ -496,20 +496,43 @@ int qref_csr_spmv_real(void* c, const double* in, double* out) {
 }
 
 namespace {
-// Rows [r0, r0 + n) of a one-dimensional-irrep sector as a row policy of their own (row j is the sector's row
-// r0 + j; columns stay the whole sector's). Lets build_cross_csr build the merged rows of a contiguous block.
+// Rows [r0, r0 + n) of a one-dimensional-irrep sector (or the listed rows, when `list` is set) as a row policy of
+// their own (row j is the sector's row r0 + j, or list[j]; columns stay the whole sector's). Lets
+// build_cross_csr build the merged rows of a block of rows.
 struct RowBlock {
     const ed::matvec::basis::RepSymmetryBasisPolicy* p;
     std::uint64_t r0, n;
+    const std::uint64_t* list = nullptr;
     int irrep_dim = 1;
+    std::uint64_t row(std::uint64_t j) const noexcept { return list ? list[j] : r0 + j; }
     std::uint64_t dim() const noexcept { return n; }
-    std::uint64_t state_of(std::uint64_t j) const noexcept { return p->state_of(r0 + j); }
-    double inv_norm_of(std::uint64_t j) const noexcept { return p->inv_norm_of(r0 + j); }
+    std::uint64_t state_of(std::uint64_t j) const noexcept { return p->state_of(row(j)); }
+    double inv_norm_of(std::uint64_t j) const noexcept { return p->inv_norm_of(row(j)); }
     std::uint64_t first_state_of(std::uint64_t j) const noexcept { return j; }
     int rank_of(std::uint64_t) const noexcept { return 1; }
     const Complex* C_of(std::uint64_t) const noexcept { return nullptr; }   // (the d > 1 branch, never taken)
 };
 }  // namespace
+
+// The merged CSR of the listed rows of O on one sector (the rows in the order listed; columns over the whole
+// sector), as qref_csr_build_rows does for a contiguous block.
+void* qref_csr_build_rowlist(void* sec, void* prog, const std::uint64_t* rows, std::uint64_t n) {
+    try {
+        const auto* S = static_cast<RefSector*>(sec);
+        const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
+        if (S->rd.irrep_dim != 1) throw std::invalid_argument("qref_csr_build_rowlist: d > 1");
+        for (std::uint64_t j = 0; j < n; ++j)
+            if (rows[j] >= S->rd.dim()) throw std::invalid_argument("qref_csr_build_rowlist: row out of range");
+        const auto pol = S->rd.make_policy();
+        RowBlock rb{&pol, 0, n, rows};
+        auto* c = new RefCsr;
+        c->csr = ed::matvec::build_cross_csr(P->view(), rb, pol, false, n);
+        return c;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
 
 // The merged CSR of rows [r0, r0 + n) of O on one sector (build_cross_csr, sector_rows.h:223-404, over the
 // block's rows, columns the whole sector): the reference's host CSR lane on a contiguous sample of rows, for
@@ -521,7 +544,7 @@ void* qref_csr_build_rows(void* sec, void* prog, std::uint64_t r0, std::uint64_t
         const auto* P = static_cast<ed::ops::MaskedProgram*>(prog);
         if (S->rd.irrep_dim != 1 || r0 + n > S->rd.dim()) throw std::invalid_argument("qref_csr_build_rows: bad rows");
         const auto pol = S->rd.make_policy();
-        const RowBlock rows{&pol, r0, n};
+        const RowBlock rows{&pol, r0, n, nullptr};
         auto* c = new RefCsr;
         c->csr = ed::matvec::build_cross_csr(P->view(), rows, pol, false, n);
         return c;

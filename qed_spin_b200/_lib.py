@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libqed_b200.so")
 QB_OK, QB_EINVAL, QB_ENOMEM, QB_ECUDA, QB_EUNSUPPORTED, QB_ETIMEOUT, QB_ENODEV = range(7)
 QB_C128, QB_C64 = 0, 1
 QB_REORTH_NONE, QB_REORTH_FULL, QB_REORTH_LOCAL = 0, 1, 2
+QB_SEED_SHARED, QB_SEED_PER_BLOCK = 0, 1
 QB_LOOKUP_AUTO, QB_LOOKUP_RANK, QB_LOOKUP_BUCKETS, QB_LOOKUP_HASH, QB_LOOKUP_HASH_WIDE = 0, 1, 2, 3, 4
 QB_NOALLOC_MAX_ITER = 1024
 
@@ -26,7 +27,7 @@ EXPORTS = [
     "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
     "qb_program_attach_csr",
     "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
-    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_eigs_levels", "qb_dynamics_t0", "qb_dense_levels",
+    "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_eigs_levels", "qb_dynamics_t0", "qb_dynamics_t0_manifold", "qb_dense_levels",
     "qb_dense_levels_blocks",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
     "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_sector_save",
@@ -129,6 +130,8 @@ def lib():
     L.qb_ftlm.argtypes = [vp, vp, i, i, u64, vp, i, i, vp, vp, vp, C.POINTER(d)]
     L.qb_ground_state.argtypes = [vp, vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i), vp, vp, C.POINTER(i)]
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
+    L.qb_dynamics_t0_manifold.argtypes = [i, vp, vp, vp, vp, vp, i, vp, i, C.c_double, C.c_double, vp, vp,
+                                          C.POINTER(i), C.POINTER(i)]
     L.qb_eigs_levels.argtypes = [vp, vp, i, u64, i, i, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
     L.qb_dense_levels.argtypes = [vp, vp, vp]
@@ -144,7 +147,7 @@ def lib():
     L.qb_server_wait.argtypes = [vp, u64, i, C.POINTER(Result), vp]
     L.qb_server_clock.argtypes = [vp, C.POINTER(d)]
     L.qb_server_destroy.argtypes = [vp]
-    L.qb_ftlm_blocks.argtypes = [vp, vp, i, i, i, u64, vp, i, i, i, vp, vp, vp, vp, vp]
+    L.qb_ftlm_blocks.argtypes = [vp, vp, i, i, i, u64, i, vp, i, i, i, vp, vp, vp, vp, vp]
     L.qb_thermal_combine.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]
     L.qb_cf.argtypes = [vp, vp, vp, i, vp, i, d, d, d, vp, C.POINTER(d)]
     L.qb_lanczos_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, i, vp, vp, C.POINTER(i), vp]

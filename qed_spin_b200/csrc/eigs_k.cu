@@ -18,9 +18,9 @@
 //
 // FP32 storage (dtype QB_C64): the basis and the locked vectors are stored as complex64 (the arithmetic and
 // all scalars stay FP64) and converged to 1e-6 of the scale, the level the storage rounding allows. With
-// refine != 0 the returned pairs are then refined in FP64: Rayleigh-Ritz on the span of the pairs and their
-// residuals (a block step of the LOBPCG family without its previous-direction block), repeated until every
-// residual is below the lock tolerance.
+// refine != 0 each returned pair is then refined in FP64, lowest first: a restarted Lanczos search for one
+// level (cycles of 16 vectors), started from the pair's vector and deflated against the pairs refined before
+// it, to the FP64 lock tolerance. A multiplet's members refine one after another inside their eigenspace.
 //
 // The contract is the reference's krylov_schur_lane (src/engine/block_solve.cpp:433-510): the k lowest
 // levels of the block, ascending, each converged to a residual of kLockRel (1e-10) times the coefficient sum,
@@ -49,7 +49,6 @@ constexpr std::uint64_t kFreshSeed = 0x7E57A27ULL;        // fresh starts of thi
 constexpr double kLockTol = 1e-10;                       // kLockRel (include/ed/core/numerics.h:25)
 constexpr double kLockTolF32 = 1e-6;                     // the FP32-storage phase, before the FP64 refinement
 constexpr double kFloorRel = 64.0 * std::numeric_limits<double>::epsilon();   // kBreakdownRel (numerics.h:23)
-constexpr int kRefineMax = 6;                            // FP64 refinement rounds at most
 
 // ---- kernels ----
 
@@ -114,49 +113,6 @@ __global__ void k_rotate_real(std::uint64_t n, int mm, int cols, int c0, const T
 #pragma unroll
         for (int c = 0; c < kRotW; ++c)
             if (c < nc) V<T>::st(out + static_cast<std::size_t>(c0 + c) * n, i, acc[c].x, acc[c].y);
-    }
-}
-
-// out_c = sum_r in_r Y[r, c] for every c < cols (FP64 columns; Y complex column-major nin x cols, nin * cols <=
-// kRotMaxCoef).
-constexpr int kRotMaxCoef = 32 * 32;
-__global__ void k_rotate_cplx(std::uint64_t n, int nin, int cols, const double2* const* in, const double2* Y,
-                              double2* const* out) {
-    __shared__ double2 Ys[kRotMaxCoef];
-    for (int t = threadIdx.x; t < nin * cols; t += blockDim.x) Ys[t] = Y[t];
-    __syncthreads();
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        for (int c = 0; c < cols; ++c) {
-            double re = 0.0, im = 0.0;
-            for (int r = 0; r < nin; ++r) {
-                const double2 a = in[r][i], y = Ys[c * nin + r];
-                re += a.x * y.x - a.y * y.y;
-                im += a.x * y.y + a.y * y.x;
-            }
-            out[c][i] = make_double2(re, im);
-        }
-    }
-}
-
-// R_c = AX_c - theta_c X_c for c < k.
-__global__ void k_residuals(std::uint64_t n, int k, const double2* const* X, const double2* const* AX,
-                            const double* theta, double2* const* R) {
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x)
-        for (int c = 0; c < k; ++c) {
-            const double2 a = AX[c][i], x = X[c][i];
-            R[c][i] = make_double2(a.x - theta[c] * x.x, a.y - theta[c] * x.y);
-        }
-}
-
-// x /= *nrm in place (FP64).
-__global__ void k_unit_inplace(std::uint64_t n, double2* x, const double* nrm) {
-    const double s = 1.0 / *nrm;
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        x[i].x *= s;
-        x[i].y *= s;
     }
 }
 
@@ -233,7 +189,6 @@ struct LevelsOut {
     std::vector<DevBuf<double2>> vectors;   // FP64 copies, filled when asked
     bool converged = false;
     int matvecs = 0, cycles = 0, refine_rounds = 0;
-    double max_residual = 0.0;
 };
 
 template <class T> constexpr int dtype_of();
@@ -242,12 +197,14 @@ template <> constexpr int dtype_of<float2>() { return QB_C64; }
 
 template <class T> class ThickRestart {
 public:
-    ThickRestart(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t budget)
+    // cycle: the basis length of a cycle (0: about 2k + 40, at least k + 24), shortened to fit 85% of the free
+    // memory.
+    ThickRestart(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t budget, std::size_t cycle = 0)
         : sec_(sec), prog_(prog), n_(sec->dim), k_(k), budget_(budget), scale_(norm_bound(prog)),
           floor_(kFloorRel * norm_bound(prog)), nb_(red_blocks(sec->dim)) {
         const std::size_t es = sizeof(T);
-        // the cycle: m vectors, about 2k + 40 (at least k + 24), within 85% of the free memory
-        std::size_t m = std::max<std::size_t>(2 * static_cast<std::size_t>(k) + 40, static_cast<std::size_t>(k) + 24);
+        std::size_t m = cycle > 0 ? cycle
+                                  : std::max<std::size_t>(2 * static_cast<std::size_t>(k) + 40, static_cast<std::size_t>(k) + 24);
         m = static_cast<std::size_t>(std::min<std::uint64_t>(m, n_));
         const double free_b = 0.85 * static_cast<double>(available_bytes());
         auto need = [&](std::size_t mm) {   // basis + kept Ritz vectors + locked + the FP64 work vector
@@ -328,6 +285,20 @@ public:
     // The returned vectors in ascending order of their levels (valid while this object lives).
     const std::vector<T*>& sorted_vectors() const { return sorted_; }
 
+    // One level refined from an approximate eigenvector (device, FP64): a search for the lowest level of the
+    // space deflated against the levels refined so far, started from x. Returns false when the budget ran out
+    // first (the best pair so far is kept) or x vanishes against the refined levels.
+    bool refine_from(const double2* x) {
+        cuda_check(cudaMemcpy(w_.p, x, n_ * 16, cudaMemcpyDeviceToDevice), "refine start");
+        have_start_ = true;
+        const std::size_t before = locked_vals_.size();
+        const int got = search(1, std::numeric_limits<double>::infinity(), true);
+        return got == 1 && locked_vals_.size() == before + 1;
+    }
+    const std::vector<double>& locked_values() const { return locked_vals_; }
+    const T* locked_vector(std::size_t i) const { return locked_[i].p; }
+    int matvecs() const { return matvecs_; }
+
 private:
     static std::size_t keep_for(std::size_t m) {   // kept Ritz vectors at a restart: about a third of the cycle
         if (m <= 2) return 1;
@@ -375,7 +346,7 @@ private:
     // One search from the start in w_: lock up to `want` of the lowest pairs. Returns the number locked, or -1
     // when the start is null against the locked vectors. give_up: a first cycle whose lowest Ritz value is at
     // or above it ends the search with nothing locked.
-    int search(int want, double give_up) {
+    int search(int want, double give_up, bool lock_best = false) {
         if (!have_start_) return -1;
         have_start_ = false;
         write_ptrs();
@@ -433,8 +404,9 @@ private:
             const bool invariant = brk < big;
             if (invariant && mm == n_ - locked_.size()) exhausted_ = true;   // the whole (deflated) block is spanned
             if (conv == top || invariant || budget_exhausted()) {
-                lock(vecs, mm, invariant ? top : conv, vals);
-                return static_cast<int>(invariant ? top : conv);
+                const std::size_t cnt = invariant ? top : (lock_best ? top : conv);
+                lock(vecs, mm, cnt, vals);
+                return static_cast<int>(invariant || conv == top ? top : conv);
             }
             // thick restart: the p lowest Ritz vectors, then the residual direction v_mm
             p = std::min(p_, mm - 1);
@@ -491,161 +463,6 @@ private:
     int matvecs_ = 0, cycles_ = 0;
 };
 
-// FP64 refinement of k approximate pairs (X: k FP64 columns, orthonormalised here): Rayleigh-Ritz on span{X, R},
-// R the residuals, until every residual is at most tol; the values and X are updated in place.
-void refine_pairs(const qb_sector* sec, const qb_program* prog, std::vector<DevBuf<double2>>& X,
-                  std::vector<double>& values, double tol, LevelsOut& out) {
-    const std::uint64_t n = sec->dim;
-    const int k = static_cast<int>(X.size());
-    if (k == 0) return;
-    const int nb = red_blocks(n);
-    std::vector<DevBuf<double2>> AX(k), R(k), AR(k), T1(2 * k);
-    for (int c = 0; c < k; ++c) {
-        AX[c].alloc(n);
-        R[c].alloc(n);
-        AR[c].alloc(n);
-    }
-    for (auto& t : T1) t.alloc(n);
-    DevBuf<void*> ptr(8 * static_cast<std::size_t>(k) + 8);
-    DevBuf<double2> coef(2 * static_cast<std::size_t>(k) + 2),
-        part(static_cast<std::size_t>(2 * k + 2) * static_cast<std::size_t>(dot_chunks(n, 1)) + kMaxRedBlocks), Yd(kRotMaxCoef);
-    DevBuf<double> slots(4 * static_cast<std::size_t>(k) + 4), red_part(4 * kMaxRedBlocks), th(2 * static_cast<std::size_t>(k));
-    DevBuf<unsigned> red_cnt(1);
-    cuda_check(cudaMemset(red_cnt.p, 0, sizeof(unsigned)), "zero");
-    const Scal red{nullptr, nullptr, nullptr, red_part.p, red_cnt.p};
-    auto set_ptrs = [&](std::size_t at, const std::vector<double2*>& v) {
-        cuda_check(cudaMemcpy(static_cast<void**>(ptr.p) + at, v.data(), v.size() * sizeof(void*), cudaMemcpyHostToDevice),
-                   "pointers");
-    };
-    auto dptr = [&](std::size_t at) { return reinterpret_cast<const double2* const*>(static_cast<void**>(ptr.p) + at); };
-    auto optr = [&](std::size_t at) { return reinterpret_cast<double2* const*>(static_cast<void**>(ptr.p) + at); };
-    // orthonormalise the columns in place (two Gram-Schmidt passes each; a vanishing column is an error)
-    auto orthonormalise = [&](std::vector<DevBuf<double2>*> cols, std::vector<DevBuf<double2>*> against) {
-        for (std::size_t c = 0; c < cols.size(); ++c) {
-            std::vector<double2*> prev;
-            for (auto* a : against) prev.push_back(a->p);
-            for (std::size_t d = 0; d < c; ++d) prev.push_back(cols[d]->p);
-            if (!prev.empty()) {
-                set_ptrs(0, prev);
-                for (int pass = 0; pass < 2; ++pass) {
-                    dot_many<double2>(n, static_cast<int>(prev.size()), dptr(0), cols[c]->p, coef.p, part.p, nullptr, nullptr);
-                    k_axpy_many<double2><<<nb, kThreads>>>(n, static_cast<int>(prev.size()), dptr(0), coef.p, cols[c]->p,
-                                                           nullptr);
-                }
-            }
-            k_norm_to<<<nb, kThreads>>>(n, cols[c]->p, red, slots.p, nullptr);
-            double nrm = 0.0;
-            cuda_check(cudaMemcpy(&nrm, slots.p, 8, cudaMemcpyDeviceToHost), "norm");
-            if (!(nrm > 0.0)) throw Error(QB_ECUDA, "refinement: a vanishing direction");
-            k_unit_inplace<<<nb, kThreads>>>(n, cols[c]->p, slots.p);
-        }
-    };
-    // G = Q^H (A Q), Hermitian, from the columns of Q and AQ (FP64)
-    auto gram = [&](const std::vector<double2*>& Q, const std::vector<double2*>& AQ) {
-        const int q = static_cast<int>(Q.size());
-        set_ptrs(0, Q);
-        std::vector<cd> G(static_cast<std::size_t>(q) * q);
-        std::vector<double2> h(q);
-        for (int c = 0; c < q; ++c) {
-            dot_many<double2>(n, q, dptr(0), AQ[c], coef.p, part.p, nullptr, nullptr);
-            cuda_check(cudaMemcpy(h.data(), coef.p, q * 16, cudaMemcpyDeviceToHost), "gram");
-            for (int r = 0; r < q; ++r) G[static_cast<std::size_t>(c) * q + r] = cd(-h[r].x, -h[r].y);
-        }
-        for (int c = 0; c < q; ++c)   // Hermitian part (the two triangles differ by rounding)
-            for (int r = 0; r < c; ++r) {
-                const cd a = 0.5 * (G[static_cast<std::size_t>(c) * q + r] + std::conj(G[static_cast<std::size_t>(r) * q + c]));
-                G[static_cast<std::size_t>(c) * q + r] = a;
-                G[static_cast<std::size_t>(r) * q + c] = std::conj(a);
-            }
-        for (int c = 0; c < q; ++c) G[static_cast<std::size_t>(c) * q + c] = G[static_cast<std::size_t>(c) * q + c].real();
-        return G;
-    };
-    auto rotate = [&](const std::vector<double2*>& in, const std::vector<cd>& Y, int cols, const std::vector<double2*>& outv) {
-        const int nin = static_cast<int>(in.size());
-        if (nin * cols > kRotMaxCoef) throw Error(QB_EINVAL, "refinement: too many vectors");
-        set_ptrs(0, in);
-        set_ptrs(in.size(), outv);
-        std::vector<double2> y(static_cast<std::size_t>(nin) * cols);
-        for (int c = 0; c < cols; ++c)
-            for (int r = 0; r < nin; ++r) {
-                const cd z = Y[static_cast<std::size_t>(c) * nin + r];
-                y[static_cast<std::size_t>(c) * nin + r] = make_double2(z.real(), z.imag());
-            }
-        cuda_check(cudaMemcpy(Yd.p, y.data(), y.size() * 16, cudaMemcpyHostToDevice), "rotation");
-        k_rotate_cplx<<<nb, kThreads>>>(n, nin, cols, dptr(0), Yd.p, optr(in.size()));
-        cuda_check(cudaGetLastError(), "rotate");
-    };
-    auto colsp = [](std::vector<DevBuf<double2>>& v, int cnt) {
-        std::vector<double2*> o;
-        for (int c = 0; c < cnt; ++c) o.push_back(v[c].p);
-        return o;
-    };
-    std::vector<DevBuf<double2>*> xs;
-    for (auto& x : X) xs.push_back(&x);
-    orthonormalise(xs, {});
-    for (int c = 0; c < k; ++c) launch_walk_mixed(sec, sec, prog, X[c].p, AX[c].p, QB_C128, QB_C128, nullptr);
-    out.matvecs += k;
-    // Rayleigh-Ritz on span{X} first: its values are already accurate to the square of the residual
-    {
-        const std::vector<cd> G = gram(colsp(X, k), colsp(AX, k));
-        std::vector<double> vals;
-        std::vector<cd> Y;
-        hermitian_eig(G, k, vals, Y);
-        rotate(colsp(X, k), Y, k, colsp(T1, k));
-        rotate(colsp(AX, k), Y, k, colsp(R, k));
-        for (int c = 0; c < k; ++c) {
-            std::swap(X[c], T1[c]);
-            std::swap(AX[c], R[c]);
-        }
-        values = vals;
-    }
-    for (int round = 0;; ++round) {
-        // residuals and their norms
-        cuda_check(cudaMemcpy(th.p, values.data(), k * 8, cudaMemcpyHostToDevice), "theta");
-        std::vector<double2*> xp = colsp(X, k), axp = colsp(AX, k), rp = colsp(R, k);
-        set_ptrs(0, xp);
-        set_ptrs(k, axp);
-        set_ptrs(2 * k, rp);
-        k_residuals<<<nb, kThreads>>>(n, k, dptr(0), dptr(k), th.p, optr(2 * k));
-        double worst = 0.0;
-        for (int c = 0; c < k; ++c) k_norm_to<<<nb, kThreads>>>(n, R[c].p, red, slots.p + c, nullptr);
-        std::vector<double> rn(k);
-        cuda_check(cudaMemcpy(rn.data(), slots.p, k * 8, cudaMemcpyDeviceToHost), "residual norms");
-        for (double r : rn) worst = std::max(worst, r);
-        out.max_residual = worst;
-        if (worst <= tol || round >= kRefineMax) {
-            out.refine_rounds = round;
-            return;
-        }
-        // Rayleigh-Ritz on span{X, R}: R orthonormalised against X and itself, A R, the 2k x 2k problem
-        std::vector<DevBuf<double2>*> rs;
-        for (auto& r : R) rs.push_back(&r);
-        orthonormalise(rs, xs);
-        for (int c = 0; c < k; ++c) launch_walk_mixed(sec, sec, prog, R[c].p, AR[c].p, QB_C128, QB_C128, nullptr);
-        out.matvecs += k;
-        std::vector<double2*> Q = colsp(X, k), AQ = colsp(AX, k);
-        for (int c = 0; c < k; ++c) {
-            Q.push_back(R[c].p);
-            AQ.push_back(AR[c].p);
-        }
-        const std::vector<cd> G = gram(Q, AQ);
-        std::vector<double> vals;
-        std::vector<cd> Y;
-        hermitian_eig(G, 2 * k, vals, Y);
-        rotate(Q, Y, k, colsp(T1, k));
-        std::vector<double2*> t2;
-        for (int c = 0; c < k; ++c) t2.push_back(T1[k + c].p);
-        rotate(AQ, Y, k, t2);
-        for (int c = 0; c < k; ++c) {
-            std::swap(X[c], T1[c]);
-            std::swap(AX[c], T1[k + c]);
-        }
-        xs.clear();
-        for (auto& x : X) xs.push_back(&x);
-        values.assign(vals.begin(), vals.begin() + k);
-    }
-}
-
 template <class T>
 LevelsOut levels(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t max_iter, bool refine,
                  bool want_vectors) {
@@ -670,8 +487,29 @@ LevelsOut levels(const qb_sector* sec, const qb_program* prog, int k, std::uint6
         }
     }
     if (refine && !X.empty()) {
-        refine_pairs(sec, prog, X, out.values, kLockTol * norm_bound(prog), out);
-        if (out.max_residual > kLockTol * norm_bound(prog)) out.converged = false;
+        // each pair, lowest first, refined in FP64 against the pairs refined before it
+        const std::uint64_t left = budget > static_cast<std::uint64_t>(out.matvecs) ? budget - out.matvecs : 0;
+        ThickRestart<double2> fine(sec, prog, static_cast<int>(X.size()), std::max<std::uint64_t>(left, 64), 16);
+        bool all = true;
+        for (const auto& x : X) all = fine.refine_from(x.p) && all;
+        out.matvecs += fine.matvecs();
+        out.refine_rounds = static_cast<int>(X.size());
+        const auto& vals = fine.locked_values();
+        std::vector<std::size_t> order(vals.size());
+        for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) { return vals[a] < vals[b]; });
+        out.values.clear();
+        std::vector<DevBuf<double2>> R;
+        for (std::size_t i : order) {
+            out.values.push_back(vals[i]);
+            if (want_vectors) {
+                DevBuf<double2> y(n);
+                cuda_check(cudaMemcpy(y.p, fine.locked_vector(i), n * 16, cudaMemcpyDeviceToDevice), "refined vector");
+                R.push_back(std::move(y));
+            }
+        }
+        X = std::move(R);
+        if (!all || out.values.size() < static_cast<std::size_t>(std::min<std::uint64_t>(k, n))) out.converged = false;
     }
     if (want_vectors) out.vectors = std::move(X);
     return out;

@@ -53,13 +53,16 @@ namespace qb {
 namespace {
 
 // ---- FTLM: sample tables, the block recurrence of one sector's samples, the curves ----
-// The sample vectors of a call: sample s of every block is the first n_b draws of sample_engine(seed, s), drawn
-// as the reference draws a block's vector (gaussian_vector(n_b, gen), include/ed/thermal/sample_seed.h:84-89). So
-// one table of k streams, as long as the largest block, holds every block's samples as prefixes; a block
-// normalises its prefix. The table is drawn on host threads with the reference's own generator and distribution.
-// The reference's thermal driver instead advances the seed by a 64-bit LCG step before each sampled block
-// (src/engine/thermal.cpp:470-471), so its blocks draw distinct streams: a one-block call given the advanced
-// seed draws exactly the reference's vectors; over many blocks the two agree in distribution, not draw for draw.
+// The sample vectors of a call (sample_engine + gaussian_vector, include/ed/thermal/sample_seed.h:37-89), in one of
+// two modes:
+//   QB_SEED_SHARED     sample s of every block is the first n_b draws of sample_engine(seed, s). One table of k
+//                      streams, as long as the largest block, holds every block's samples as prefixes; a block
+//                      normalises its prefix. One draw of the largest block serves the whole call.
+//   QB_SEED_PER_BLOCK  the reference thermal driver's streams (src/engine/thermal.cpp:470-471): before each sampled
+//                      block, in the order the blocks are given, the seed takes one step of the 64-bit LCG
+//                      seed * 6364136223846793005 + 1442695040888963407, and block b's sample s is the first n_b draws
+//                      of sample_engine(seed_b, s). Every block draws a table of its own.
+// The tables are drawn on host threads with the reference's own generator and distribution.
 std::vector<std::complex<double>> sample_table(std::uint64_t seed, int k, std::uint64_t len) {
     std::vector<std::complex<double>> G(static_cast<std::size_t>(k) * len);
     auto draw = [&](int s) {
@@ -78,6 +81,45 @@ std::vector<std::complex<double>> sample_table(std::uint64_t seed, int k, std::u
     for (int t = 0; t < nt; ++t)
         pool.emplace_back([&] {
             for (int s = next++; s < k; s = next++) draw(s);
+        });
+    for (auto& t : pool) t.join();
+    return G;
+}
+
+// Block b's samples under QB_SEED_PER_BLOCK: k streams of dims[b] draws each at G[off[b] + s * dims[b] + i].
+std::vector<std::complex<double>> sample_tables_per_block(std::uint64_t seed, int k, const std::vector<std::uint64_t>& dims,
+                                                          std::vector<std::size_t>& off) {
+    const std::size_t nb = dims.size();
+    off.assign(nb, 0);
+    std::vector<std::uint64_t> seeds(nb);
+    std::size_t tot = 0;
+    for (std::size_t b = 0; b < nb; ++b) {
+        seed = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+        seeds[b] = seed;
+        off[b] = tot;
+        tot += static_cast<std::size_t>(k) * dims[b];
+    }
+    std::vector<std::complex<double>> G(tot);
+    const std::size_t items = nb * static_cast<std::size_t>(k);
+    auto draw = [&](std::size_t it) {
+        const std::size_t b = it / k;
+        const int s = static_cast<int>(it % k);
+        std::mt19937 gen = sample_engine(seeds[b], static_cast<std::uint64_t>(s));
+        std::normal_distribution<double> nd(0.0, 1.0);
+        std::complex<double>* g = G.data() + off[b] + static_cast<std::size_t>(s) * dims[b];
+        for (std::uint64_t i = 0; i < dims[b]; ++i) {
+            const double im = nd(gen);   // the imaginary part is drawn first (see gaussian_fill)
+            const double re = nd(gen);
+            g[i] = std::complex<double>(re, im);
+        }
+    };
+    const int nt = static_cast<int>(std::max<std::size_t>(
+        1, std::min<std::size_t>(items, std::max(1u, std::thread::hardware_concurrency()))));
+    std::vector<std::thread> pool;
+    std::atomic<std::size_t> next{0};
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (std::size_t it = next++; it < items; it = next++) draw(it);
         });
     for (auto& t : pool) t.join();
     return G;
@@ -472,6 +514,7 @@ struct PackItem {
     DSector sec;
     DProgram prog;
     unsigned long long a_off, b_off;
+    unsigned long long g_off, g_ld;   // the block's sample table: sample s at G + g_off + s * g_ld
     double tol;
     int cap, in_smem;
 };
@@ -504,7 +547,7 @@ __device__ __forceinline__ double pack_col_sum(double (*red)[33], int c) {
 
 template <class T, class ST, int CPL>
 __global__ void __launch_bounds__(256) ftlm_pack(const PackItem* items, int n_items, unsigned* next_item, int k,
-                                                 int max_entries, const double2* G, std::uint64_t ld, double* alpha,
+                                                 int max_entries, const double2* G_all, double* alpha,
                                                  double* beta, unsigned char* scratch, PackSlot slot) {
     using Rt = typename Work<T>::R;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -528,6 +571,8 @@ __global__ void __launch_bounds__(256) ftlm_pack(const PackItem* items, int n_it
         const PackItem& I = items[it];
         const std::uint64_t n = I.sec.dim;
         const int cap = I.cap;
+        const double2* G = G_all + I.g_off;
+        const std::uint64_t ld = I.g_ld;
         // ---- the block's merged rows ----
         const SmemProgram sp = stage(I.prog, I.sec, smem, I.in_smem != 0);
         for (std::uint64_t r = threadIdx.x; r < n; r += blockDim.x) {
@@ -729,7 +774,8 @@ constexpr int kPackMaxEntries = 256;
 template <class ST>
 void launch_pack(const std::vector<int>& set, const qb_sector* const* secs, const qb_program* const* progs, int k,
                  int dtype, const std::vector<std::size_t>& a_off, const std::vector<std::size_t>& b_off,
-                 const std::vector<int>& caps, const std::vector<double>& tol, const double2* G, std::uint64_t ld,
+                 const std::vector<int>& caps, const std::vector<double>& tol, const double2* G,
+                 const std::vector<std::size_t>& g_off, const std::vector<std::uint64_t>& g_ld,
                  double* alpha, double* beta, DevBuf<PackItem>& d_items, DevBuf<unsigned>& counter,
                  DevBuf<unsigned char>& scratch, cudaStream_t st) {
     if (set.empty()) return;
@@ -741,7 +787,8 @@ void launch_pack(const std::vector<int>& set, const qb_sector* const* secs, cons
         const int b = set[i];
         bool in_smem = false;
         smem = std::max(smem, smem_for(progs[b], secs[b], in_smem));
-        items[i] = PackItem{secs[b]->view(), progs[b]->view, a_off[b], b_off[b], tol[b], caps[b], in_smem ? 1 : 0};
+        items[i] = PackItem{secs[b]->view(), progs[b]->view, a_off[b], b_off[b], g_off[b], g_ld[b], tol[b], caps[b],
+                            in_smem ? 1 : 0};
         n_max = std::max(n_max, secs[b]->dim);
         max_entries = std::max(max_entries, static_cast<int>(progs[b]->view.n_groups));
     }
@@ -765,7 +812,7 @@ void launch_pack(const std::vector<int>& set, const qb_sector* const* secs, cons
         cuda_check(cudaMemcpyAsync(d_items.p, items.data(), items.size() * sizeof(PackItem), cudaMemcpyHostToDevice,
                                    st), "pack items");
         cuda_check(cudaMemsetAsync(counter.p, 0, 4, st), "zero");
-        kernel<<<grid, 256, smem, st>>>(d_items.p, static_cast<int>(items.size()), counter.p, k, max_entries, G, ld,
+        kernel<<<grid, 256, smem, st>>>(d_items.p, static_cast<int>(items.size()), counter.p, k, max_entries, G,
                                         alpha, beta, scratch.p, slot);
         cuda_check(cudaGetLastError(), "ftlm_pack launch");
     };
@@ -972,8 +1019,8 @@ __global__ void k_block_combine(const CurveBlock* blocks, int n_blocks, int k, c
 
 // FTLM over many blocks (qb_ftlm_blocks; one block: qb_ftlm).
 void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int k, int depth,
-                 std::uint64_t seed, const double* betas, int n_beta, int dtype, bool use_csr, double* lnZ, double* E,
-                 double* V, double* e_min, double* stats) {
+                 std::uint64_t seed, int seed_mode, const double* betas, int n_beta, int dtype, bool use_csr, double* lnZ,
+                 double* E, double* V, double* e_min, double* stats) {
     using clock = std::chrono::steady_clock;
     auto secs_since = [](clock::time_point t0) { return std::chrono::duration<double>(clock::now() - t0).count(); };
     auto t_phase = clock::now();
@@ -982,6 +1029,7 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
     if (depth < 2) throw Error(QB_EINVAL, "depth must be >= 2");
     if (dtype != QB_C128 && dtype != QB_C64) throw Error(QB_EINVAL, "bad dtype");
     if (n_blocks < 1 || !secs || !progs) throw Error(QB_EINVAL, "no blocks");
+    if (seed_mode != QB_SEED_SHARED && seed_mode != QB_SEED_PER_BLOCK) throw Error(QB_EINVAL, "bad seed mode");
     std::uint64_t len = 0;
     for (int b = 0; b < n_blocks; ++b) {
         if (!secs[b] || !progs[b]) throw Error(QB_EINVAL, "null block");
@@ -989,10 +1037,22 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         len = std::max(len, secs[b]->dim);
     }
     const std::size_t es = dtype == QB_C64 ? 8 : 16;
-    // the samples of every block: one table, drawn once
-    const std::vector<std::complex<double>> G = sample_table(seed, k, len);
-    DevBuf<double2> dG(G.size());
-    cuda_check(cudaMemcpy(dG.p, G.data(), G.size() * 16, cudaMemcpyHostToDevice), "samples upload");
+    // the samples of every block: one table drawn once, or a table per block; block b's sample s at
+    // dG + g_off[b] + s * g_ld[b]
+    std::vector<std::size_t> g_off(n_blocks, 0);
+    std::vector<std::uint64_t> g_ld(n_blocks, len);
+    DevBuf<double2> dG;
+    {
+        std::vector<std::complex<double>> G;
+        if (seed_mode == QB_SEED_SHARED) {
+            G = sample_table(seed, k, len);
+        } else {
+            for (int b = 0; b < n_blocks; ++b) g_ld[b] = secs[b]->dim;
+            G = sample_tables_per_block(seed, k, g_ld, g_off);
+        }
+        dG.alloc(G.size());
+        cuda_check(cudaMemcpy(dG.p, G.data(), G.size() * 16, cudaMemcpyHostToDevice), "samples upload");
+    }
     st_draw = secs_since(t_phase);
     // blocks, largest first, dealt round robin to a few streams so small blocks overlap
     std::vector<int> order(n_blocks);
@@ -1050,10 +1110,10 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
     DevBuf<unsigned> pack_counter[2];
     DevBuf<unsigned char> pack_scratch[2];
     PackStream pack_guard{pst};
-    launch_pack<u32>(pack_set[0], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, len, d_alpha.p, d_beta.p,
-                     pack_items[0], pack_counter[0], pack_scratch[0], pst);
-    launch_pack<u64>(pack_set[1], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, len, d_alpha.p, d_beta.p,
-                     pack_items[1], pack_counter[1], pack_scratch[1], pst);
+    launch_pack<u32>(pack_set[0], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, g_off, g_ld, d_alpha.p,
+                     d_beta.p, pack_items[0], pack_counter[0], pack_scratch[0], pst);
+    launch_pack<u64>(pack_set[1], secs, progs, k, dtype, a_off, b_off, caps, tol, dG.p, g_off, g_ld, d_alpha.p,
+                     d_beta.p, pack_items[1], pack_counter[1], pack_scratch[1], pst);
     // every block's reduced CSR, built before the recurrences (a build synchronises the device); a block
     // whose CSR does not fit runs on the walk
     struct Csrs {
@@ -1096,9 +1156,9 @@ void ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, i
         const bool grow = B.w.n < static_cast<std::size_t>(n) * k;
         if (grow) cuda_check(cudaStreamSynchronize(st), "stream");
         B.ensure(n, k, es);
-        k_sample_norms<<<k, kThreads, 0, st>>>(n, dG.p, len, B.inv.p);
-        k_sample_start<<<red_blocks(static_cast<std::uint64_t>(n) * k), kThreads, 0, st>>>(n, k, dG.p, len, B.inv.p,
-                                                                                            B.w.p);
+        k_sample_norms<<<k, kThreads, 0, st>>>(n, dG.p + g_off[b], g_ld[b], B.inv.p);
+        k_sample_start<<<red_blocks(static_cast<std::uint64_t>(n) * k), kThreads, 0, st>>>(n, k, dG.p + g_off[b], g_ld[b],
+                                                                                            B.inv.p, B.w.p);
         block_recurrence(sec, progs[b], csrs.h[b], k, caps[b], tol[b], dtype, B, st, d_alpha.p + a_off[b],
                          d_beta.p + b_off[b]);
     }
@@ -1336,18 +1396,19 @@ int qb_ftlm(const qb_sector* sec, const qb_program* prog, int samples, int depth
         const qb_sector* secs[1] = {sec};
         const qb_program* progs[1] = {prog};
         // the program's own lane: its attached CSR for this sector, else the walk
-        ftlm_blocks(secs, progs, 1, samples, depth, seed, betas, n_beta, dtype, false, lnZ, E, V, e_min, nullptr);
+        ftlm_blocks(secs, progs, 1, samples, depth, seed, QB_SEED_SHARED, betas, n_beta, dtype, false, lnZ, E, V, e_min,
+                    nullptr);
     });
 }
 
 int qb_ftlm_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks, int samples, int depth,
-                   uint64_t seed, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ, double* E,
-                   double* V, double* e_min, double* stats) {
+                   uint64_t seed, int seed_mode, const double* betas, int n_beta, int dtype, int use_csr, double* lnZ,
+                   double* E, double* V, double* e_min, double* stats) {
     return qb::guarded([&] {
         using namespace qb;
         if (!betas || !lnZ || !E || !V || !e_min) throw Error(QB_EINVAL, "null argument");
-        ftlm_blocks(secs, progs, n_blocks, samples, depth, seed, betas, n_beta, dtype, use_csr != 0, lnZ, E, V, e_min,
-                    stats);
+        ftlm_blocks(secs, progs, n_blocks, samples, depth, seed, seed_mode, betas, n_beta, dtype, use_csr != 0, lnZ, E, V,
+                    e_min, stats);
     });
 }
 

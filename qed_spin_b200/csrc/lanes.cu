@@ -400,4 +400,95 @@ int qb_dynamics_t0(const qb_sector* src, const qb_program* h_src, const qb_secto
     });
 }
 
+int qb_dynamics_t0_manifold(int n_src, const qb_sector* const* srcs, const qb_program* const* h_srcs,
+                            const qb_sector* const* tgts, const qb_program* const* h_tgts, const qb_program* const* ops,
+                            int depth, const double* omega, int n_omega, double eta, double degeneracy_tol, double* S,
+                            double* e0, int* manifold, int* certified) {
+    return qb::guarded([&] {
+        using namespace qb;
+        if (n_src < 1 || !srcs || !h_srcs || !tgts || !h_tgts || !ops || !omega || !S || !e0 || degeneracy_tol < 0.0)
+            throw Error(QB_EINVAL, "bad argument");
+        for (int b = 0; b < n_src; ++b) {
+            if (!srcs[b] || !h_srcs[b] || !tgts[b] || !h_tgts[b] || !ops[b]) throw Error(QB_EINVAL, "null block");
+            if (srcs[b]->N != tgts[b]->N) throw Error(QB_EINVAL, "sectors of different sizes");
+        }
+        for (int i = 0; i < n_omega; ++i) S[i] = 0.0;
+        // the lowest level of every source block (the k = 1 lane), and the window above the least of them
+        std::vector<double> low(n_src, std::numeric_limits<double>::infinity());
+        bool all_conv = true;
+        for (int b = 0; b < n_src; ++b) {
+            if (srcs[b]->dim == 0) continue;
+            int it = 0, cv = 0, mv = 0;
+            if (qb_eigs_lowest(srcs[b], h_srcs[b], 0, QB_C128, 0, &low[b], &it, &cv, &mv) != QB_OK)
+                throw Error(QB_ECUDA, std::string("ground manifold: ") + qb_last_error());
+            all_conv = all_conv && cv;
+        }
+        double emin = *std::min_element(low.begin(), low.end());
+        if (!std::isfinite(emin)) throw Error(QB_EINVAL, "the source blocks hold no state");
+        const double window = degeneracy_tol * norm_bound(h_srcs[0]);
+        // every level within the window of each block at E0, with its vector: k levels, doubling k until one
+        // lies above the window or the block is exhausted (a multiplet inside a block)
+        struct State {
+            int b;
+            double e;
+            DevBuf<double2> v;
+        };
+        std::vector<State> states;
+        for (int b = 0; b < n_src; ++b) {
+            if (!(low[b] <= emin + window)) continue;
+            const std::uint64_t n = srcs[b]->dim;
+            for (int pb = 2;; pb *= 2) {
+                const int kk = static_cast<int>(std::min<std::uint64_t>(static_cast<std::uint64_t>(pb), n));
+                std::vector<DevBuf<double2>> vec(kk);
+                std::vector<void*> ptr(kk);
+                for (int i = 0; i < kk; ++i) {
+                    vec[i].alloc(n);
+                    ptr[i] = vec[i].p;
+                }
+                std::vector<double> vals(kk);
+                int nf = 0, cv = 0, mv = 0;
+                if (qb_eigs_levels(srcs[b], h_srcs[b], kk, 0, QB_C128, 0, vals.data(), &nf, &cv, &mv, ptr.data()) != QB_OK)
+                    throw Error(QB_ECUDA, std::string("ground manifold: ") + qb_last_error());
+                const bool exhausted = nf < kk || static_cast<std::uint64_t>(kk) >= n;
+                if (exhausted || vals[nf - 1] > emin + window) {
+                    all_conv = all_conv && cv;
+                    for (int i = 0; i < nf; ++i)
+                        if (vals[i] <= emin + window) states.push_back(State{b, vals[i], std::move(vec[i])});
+                    break;
+                }
+            }
+        }
+        if (states.empty()) throw Error(QB_ECUDA, "ground manifold: no level within the window");
+        for (const auto& st : states) emin = std::min(emin, st.e);
+        // one continued fraction per state from phi = O psi in its target block, shifted by E0, averaged
+        std::vector<double> Sk(std::max(1, n_omega));
+        for (const auto& st : states) {
+            const qb_sector* tgt = tgts[st.b];
+            if (tgt->dim == 0) continue;
+            DevBuf<double2> phi(tgt->dim);
+            launch_walk_mixed(tgt, srcs[st.b], ops[st.b], st.v.p, phi.p, QB_C128, QB_C128, nullptr);
+            cuda_check(cudaGetLastError(), "phi");
+            const int kd = std::max(depth, 2);
+            Recurrence R(tgt, h_tgts[st.b], QB_C128, kd);
+            double nrm = 0.0;
+            try {
+                nrm = R.start_from_device(phi.p);
+            } catch (const Error& e) {
+                if (e.code == QB_EINVAL) continue;   // O annihilates this state: no spectral weight
+                throw;
+            }
+            const double tol = kBreakdownRel * norm_bound(h_tgts[st.b]);
+            ScanOut o = run_scan(R, kd, QB_REORTH_NONE, false, tol, false);
+            if (o.alpha.empty()) continue;
+            cf_spectrum(o.alpha, o.beta, static_cast<int>(o.alpha.size()), omega, n_omega, eta, emin, nrm * nrm,
+                        Sk.data());
+            for (int i = 0; i < n_omega; ++i) S[i] += Sk[i];
+        }
+        for (int i = 0; i < n_omega; ++i) S[i] /= static_cast<double>(states.size());
+        *e0 = emin;
+        if (manifold) *manifold = static_cast<int>(states.size());
+        if (certified) *certified = all_conv ? 1 : 0;
+    });
+}
+
 }  // extern "C"

@@ -340,6 +340,22 @@ def dynamics_t0(src: Sector, h_src: Program, tgt: Sector, h_tgt: Program, op: Pr
     return {"S": S, "e0": e0.value, "conv_change": ch.value, "certified": bool(cert.value)}
 
 
+def dynamics_t0_manifold(srcs, h_srcs, tgts, h_tgts, ops, depth: int, omega, eta: float,
+                         degeneracy_tol: float = 1e-8) -> dict:
+    """T = 0 dynamics averaged over the ground manifold of the source blocks (qb_dynamics_t0_manifold): block b's
+    states carried by ops[b] into tgts[b]. Returns S(omega), E0, the manifold's size and whether every solve
+    converged."""
+    nb = len(srcs)
+    omega = np.ascontiguousarray(omega, np.float64)
+    S = np.zeros(len(omega))
+    arr = lambda xs: (C.c_void_p * nb)(*[x.h.value for x in xs])
+    e0, g, cert = C.c_double(), C.c_int(), C.c_int()
+    check(lib().qb_dynamics_t0_manifold(nb, arr(srcs), arr(h_srcs), arr(tgts), arr(h_tgts), arr(ops), depth,
+                                        omega.ctypes.data, len(omega), eta, degeneracy_tol, S.ctypes.data,
+                                        C.byref(e0), C.byref(g), C.byref(cert)))
+    return {"S": S, "e0": e0.value, "manifold": g.value, "certified": bool(cert.value)}
+
+
 def ftlm(sec: Sector, prog: Program, samples: int, depth: int, seed: int, betas, dtype="c128") -> dict:
     betas = np.ascontiguousarray(betas, np.float64)
     nb = len(betas)
@@ -350,10 +366,12 @@ def ftlm(sec: Sector, prog: Program, samples: int, depth: int, seed: int, betas,
     return dict(lnZ=lnZ, E=E, V=V, e_min=em.value)
 
 
-def ftlm_blocks(sectors, progs, samples: int, depth: int, seed: int, betas, dtype="c128", use_csr=True) -> dict:
+def ftlm_blocks(sectors, progs, samples: int, depth: int, seed: int, betas, dtype="c128", use_csr=True,
+                per_block_seeds: bool = False) -> dict:
     """FTLM over many blocks (each a Sector; progs: one Program for all, or one per block). Returns the
     per-block curves [n_blocks, n_beta] (lnZ, E, V), e_min [n_blocks], and their log-space combination
-    (lnZ, E, C, S, F over beta) under "total"."""
+    (lnZ, E, C, S, F over beta) under "total". per_block_seeds: the reference thermal driver's sample streams (the
+    seed advanced by its LCG step before each block, in the order given); else one set of streams for all blocks."""
     nb = len(sectors)
     if isinstance(progs, Program):
         progs = [progs] * nb
@@ -364,8 +382,10 @@ def ftlm_blocks(sectors, progs, samples: int, depth: int, seed: int, betas, dtyp
     lnZ, E, V = (np.zeros((nb, nt)) for _ in range(3))
     e_min = np.zeros(nb)
     stats = np.zeros(4)
-    check(lib().qb_ftlm_blocks(sh, ph, nb, samples, depth, seed, betas.ctypes.data, nt, _dt(dtype), int(bool(use_csr)),
-                               lnZ.ctypes.data, E.ctypes.data, V.ctypes.data, e_min.ctypes.data, stats.ctypes.data))
+    mode = _lib.QB_SEED_PER_BLOCK if per_block_seeds else _lib.QB_SEED_SHARED
+    check(lib().qb_ftlm_blocks(sh, ph, nb, samples, depth, seed, mode, betas.ctypes.data, nt, _dt(dtype),
+                               int(bool(use_csr)), lnZ.ctypes.data, E.ctypes.data, V.ctypes.data, e_min.ctypes.data,
+                               stats.ctypes.data))
     return {"lnZ": lnZ, "E": E, "V": V, "e_min": e_min, "total": thermal_combine(lnZ, E, V, betas),
             "stats": dict(zip(("draw_s", "csr_build_s", "recurrence_s", "curves_s"), stats.tolist()))}
 

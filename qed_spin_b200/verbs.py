@@ -181,10 +181,13 @@ def _exact_curves(levels: np.ndarray, betas: np.ndarray):
 
 def thermal(H, T: Sequence[float], *, sectors: Sequence[SectorSpec], method: str = "ftlm", samples: int = 40,
             krylov: Optional[int] = None, seed: int = 0, device: str = "gpu", dense_max_dim: Optional[int] = None,
-            dtype: str = "c128") -> ThermalResult:
+            dtype: str = "c128", shared_samples: bool = False) -> ThermalResult:
     """Thermodynamics of ``H`` at the temperatures ``T`` over the blocks ``sectors``.
     ``method``: ``"ftlm"`` (blocks above ``dense_max_dim``, default 512, sampled with ``samples`` vectors at depth
-    ``krylov``, default 100) or ``"exact"`` (every block's full spectrum). ``seed`` 0 draws one."""
+    ``krylov``, default 100) or ``"exact"`` (every block's full spectrum). ``seed`` 0 draws one. The sampled blocks
+    draw the reference driver's streams (its seed advanced by one LCG step before each sampled block, in block
+    order, src/engine/thermal.cpp:470-471); ``shared_samples`` instead gives every block the prefixes of one set
+    of streams from ``seed`` (drawn once: faster, equal in distribution)."""
     from . import device as D
     if method not in ("ftlm", "exact"):
         raise InvalidRequest(f"method must be 'ftlm' or 'exact', got {method!r}")
@@ -216,7 +219,8 @@ def thermal(H, T: Sequence[float], *, sectors: Sequence[SectorSpec], method: str
         for j, lv in zip(dense, D.dense_levels_blocks([blocks[j][2] for j in dense], P)):
             lnZ[j], E[j], V[j] = _exact_curves(lv, betas)
     if sampled:
-        r = D.ftlm_blocks([blocks[j][2] for j in sampled], P, int(samples), depth, seed, betas, dtype=dtype)
+        r = D.ftlm_blocks([blocks[j][2] for j in sampled], P, int(samples), depth, seed, betas, dtype=dtype,
+                          per_block_seeds=not shared_samples)
         for q, j in enumerate(sampled):
             lnZ[j], E[j], V[j] = r["lnZ"][q], r["E"][q], r["V"][q]
     tot = D.thermal_combine(lnZ, E, V, betas)
@@ -232,12 +236,19 @@ class DynamicsResult:
     e0: float
     conv_change: float
     certified: bool
+    manifold: int = 1
 
 
-def dynamics(H, O, *, source: SectorSpec, target: SectorSpec, omega: Sequence[float], eta: float = 0.05,
-             krylov: int = 200, device: str = "gpu") -> DynamicsResult:
-    """T = 0 dynamics of the operator ``O`` (a MaskedOperator) from the ground state of ``H`` in ``source`` to the
-    block ``target``: S(omega) = -Im <phi| (omega + E0 - H + i eta)^-1 |phi> / pi, phi = O psi0."""
+def dynamics(H, O, *, source, target, omega: Sequence[float], eta: float = 0.05, krylov: int = 200,
+             device: str = "gpu", degeneracy_tol: float = 1e-8) -> DynamicsResult:
+    """T = 0 dynamics of the operator ``O`` (a MaskedOperator): S(omega) = -Im <phi| (omega + E0 - H + i eta)^-1
+    |phi> / pi, phi = O psi0.
+
+    ``source`` / ``target``: one block each, or equal-length lists, target[b] being the block O carries source[b]
+    into (for O = S^z(q) on momentum blocks: momentum k -> k + q). With lists, psi0 runs over the ground manifold of
+    the source blocks -- every level within ``degeneracy_tol`` times the scale of H (the sum of |c| over its terms)
+    of E0, multiplets inside a block included -- and S is the average over it, as the reference's verb returns for
+    a degenerate ground state (src/engine/dynamics.cpp:395-566). With one block, psi0 is that block's ground state."""
     from . import device as D
     omega = np.asarray(omega, np.float64)
     if omega.ndim != 1 or len(omega) == 0:
@@ -246,8 +257,27 @@ def dynamics(H, O, *, source: SectorSpec, target: SectorSpec, omega: Sequence[fl
         raise InvalidRequest(f"eta must be > 0, got {eta}")
     if not isinstance(O, ops.MaskedOperator):
         raise InvalidRequest("O must be a MaskedOperator")
+    many = isinstance(source, (list, tuple))
+    if many != isinstance(target, (list, tuple)) or (many and len(source) != len(target)):
+        raise InvalidRequest("source and target: one block each, or lists of equal length")
     _resolve(device)
     h = _program(H)
+    if many:
+        srcs = [D.Sector(s) for s in source]
+        tgts = [D.Sector(t) for t in target]
+        if all(S.dim == 0 for S in srcs):
+            raise InvalidRequest("source: the blocks hold no state")
+        hs = [D.Program(h) for _ in srcs]
+        ht = [D.Program(h) for _ in tgts]
+        cross = [D.Program(ops.cross_row_program(O, t, s)) for s, t in zip(source, target)]
+        lanes = [(_lane(S, P) if S.dim else None, P) for S, P in zip(srcs + tgts, hs + ht)]
+        r = D.dynamics_t0_manifold(srcs, hs, tgts, ht, cross, int(krylov), omega, eta, degeneracy_tol)
+        for A, P in lanes:
+            if A is not None:
+                D.detach_csr(P)
+                A.close()
+        return DynamicsResult(omega=omega, S=r["S"], e0=r["e0"], conv_change=float("nan"), certified=r["certified"],
+                              manifold=r["manifold"])
     Ss, St = D.Sector(source), D.Sector(target)
     if Ss.dim == 0:
         raise InvalidRequest("source: an empty block")

@@ -73,6 +73,43 @@ def test_blocks_match_oracle(oracle_curves, monkeypatch, dtype, use_csr, pack):
                                    err_msg=key)
 
 
+def _lcg_seeds(seed, n):
+    """The thermal driver's block seeds: one step of its 64-bit LCG before each sampled block
+    (src/engine/thermal.cpp:470-471)."""
+    out = []
+    for _ in range(n):
+        seed = (seed * 6364136223846793005 + 1442695040888963407) % (1 << 64)
+        out.append(seed)
+    return out
+
+
+@pytest.mark.parametrize("pack", ["4096", "0"])
+def test_per_block_seeds_match_the_driver_loop(monkeypatch, pack):
+    """QB_SEED_PER_BLOCK: block b draws from the seed the reference's thermal driver gives it (its LCG stepped
+    once per sampled block, in the order given); every block's curves equal the oracle's FTLM of that block from
+    that seed within 1e-10 relative (FP64 storage), and so do the combined thermodynamics."""
+    from qed_spin_b200 import device as D
+    monkeypatch.setenv("QB_FTLM_PACK_DIM", pack)
+    specs, prog = _blocks()
+    seeds = _lcg_seeds(SEED, len(specs))
+    P = O.Program(prog)
+    curves = [O.Sector(s).ftlm(P, 8, 30, sd, BETAS) for s, sd in zip(specs, seeds)]
+    r = D.ftlm_blocks([D.Sector(s) for s in specs], D.Program(prog), 8, 30, SEED, BETAS, per_block_seeds=True)
+    tol = 1e-10
+    for b, c in enumerate(curves):
+        for key in ("lnZ", "E", "V"):
+            ref = np.asarray(c[key])
+            np.testing.assert_allclose(r[key][b], ref, rtol=tol, atol=tol * max(np.abs(ref).max(), 1e-3),
+                                       err_msg=f"block {b} {key}")
+    tot = O.combine_blocks(curves, BETAS)
+    for key in ("lnZ", "E", "C", "S", "F"):
+        np.testing.assert_allclose(r["total"][key], tot[key], rtol=tol, atol=tol * np.abs(tot[key]).max(),
+                                   err_msg=key)
+    # a block's draws differ from the shared-stream mode's (distinct streams), as the driver's do
+    shared = D.ftlm_blocks([D.Sector(s) for s in specs[:3]], D.Program(prog), 8, 30, SEED, BETAS)
+    assert not np.array_equal(shared["lnZ"][2], r["lnZ"][2])
+
+
 def test_combine_matches_oracle(oracle_curves):
     """The C combine equals the oracle's restatement of the thermal driver's (1e-13 relative)."""
     from qed_spin_b200 import device as D
