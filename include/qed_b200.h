@@ -199,6 +199,12 @@ int qb_program_attach_csr(qb_program* prog, const qb_csr* csr);
 int qb_lanczos(const qb_sector* sec, const qb_program* prog, const double* v0_host, int max_iter, int reorth,
                double breakdown_tol, int dtype, double* alpha, double* beta, int* iters);
 
+/* The lanes' staged Gaussian start of dimension n from mt19937_64(seed) (staged_seed, src/engine/block_solve.cpp:
+ * 263-277; entry = (re, im) with the imaginary part drawn first): host work, out = 2n doubles. The reference's
+ * stream bit for bit; drawn on the host's cores in parallel past 2^20 entries (the generator's raw outputs in
+ * order on one thread, the normal transform of the accepted polar attempts on the others). */
+int qb_staged_start(uint64_t seed, uint64_t n, double* out);
+
 /* The k = 1 block lane (lowest_scan_lane, src/engine/block_solve.cpp:528-598): a Lanczos scan from
  * the staged Gaussian start of seed 0x51ED0B70 with the Paige-gated, ghost-aware lowest-level test
  * after every step; budget max_iter (0: 400). dtype QB_C64 runs the recurrence on FP32-stored
@@ -253,12 +259,15 @@ int qb_dynamics_t0_manifold(int n_src, const qb_sector* const* srcs, const qb_pr
                             double* e0, int* manifold, int* certified);
 
 /* The full spectrum of a small block (at most 8192 states), ascending, with multiplicity: the dense tail of
- * the thermal and eigs drivers (blocks up to dense_max_dim are solved exactly, include/ed/sectors/thermal.h:35).
- * The block is assembled on the device from the block matvec on identity columns; the host reduces it by
- * Householder reflections to a real tridiagonal and takes its eigenvalues by implicit QL. */
+ * the thermal and eigs drivers (blocks up to dense_max_dim are solved exactly, include/ed/sectors/thermal.h:35;
+ * the reference's device pool of dense eigensolves, src/gpu/little_group.cu:185-188). The block is assembled on
+ * the device from the block matvec on identity columns. Blocks of at most 1024 states are reduced on the device
+ * (Householder reflections to a real tridiagonal, a CTA per block, then every eigenvalue by Sturm bisection);
+ * larger ones on the host (the same reflections, then implicit QL). */
 int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values);
-/* The same for many blocks at once (largest first over host threads, each assembling on its own stream):
- * block b's levels at values[sum of the earlier blocks' dims ...]. */
+/* The same for many blocks at once: block b's levels at values[sum of the earlier blocks' dims ...]. When every
+ * block has at most 1024 states, all are assembled into one device buffer and reduced by one launch (a CTA per
+ * block, largest first); else largest first over host threads, each assembling on its own stream. */
 int qb_dense_levels_blocks(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks,
                            double* values);
 
@@ -347,32 +356,38 @@ int qb_tune_load(const char* path);
 int qb_tune_entries(char* buf, uint64_t len, uint64_t* needed);
 
 /* ---- the request server ---------------------------------------------------------------------
- * Eigs and T = 0 dynamics solves of sectors of different sizes served on one GPU with continuous
+ * Eigs, thermal and T = 0 dynamics solves of sectors of different sizes served on one GPU with continuous
  * batching: requests queue in arrival order; a worker admits the head when one of max_active slots is
  * free and the request's estimated HBM footprint (sectors, reduced CSRs, Krylov vectors) fits what is
  * left of hbm_budget (0: 80% of the free memory); a request larger than the budget runs alone. Admitted
  * requests run concurrently, each on its worker's own stream. No reference counterpart: the reference
- * serves one call at a time through its verbs (python/qed/_verbs). */
+ * serves one call at a time through its verbs (python/qed/_verbs). A thermal request is one block of the
+ * thermal driver's sampled path (the unit its driver dispatches per block, src/engine/thermal.cpp:470-490):
+ * FTLM of the block from sample_engine(seed, s), s < samples, at depth `krylov`, per inverse temperature. */
 typedef struct qb_server qb_server;
-enum { QB_REQ_EIGS = 0, QB_REQ_DYNAMICS = 1 };
+enum { QB_REQ_EIGS = 0, QB_REQ_DYNAMICS = 1, QB_REQ_THERMAL = 2 };
 #define QB_SERVER_MAX_LEVELS 16
 typedef struct {
-    int kind;                 /* QB_REQ_EIGS or QB_REQ_DYNAMICS */
-    qb_sector_desc sector;    /* eigs: the sector; dynamics: the source sector */
+    int kind;                 /* QB_REQ_EIGS, QB_REQ_DYNAMICS or QB_REQ_THERMAL */
+    qb_sector_desc sector;    /* eigs, thermal: the sector; dynamics: the source sector */
     qb_program_desc h;        /* the Hamiltonian's row program (compile_operator(H^dagger)) */
-    int k;                    /* eigs: levels wanted, 1..16 (k = 1: the scan lane; k > 1: Krylov-Schur) */
+    int k;                    /* eigs: levels wanted, 1..16 (k = 1: the scan lane; k > 1: the k > 1 lane) */
     qb_sector_desc target;    /* dynamics: the target sector */
     qb_program_desc op;       /* dynamics: the operator's cross row program (rows in target, columns in source) */
-    int krylov;               /* dynamics: continued-fraction depth */
+    int krylov;               /* dynamics: continued-fraction depth; thermal: Lanczos depth */
     const double* omega;      /* dynamics: n_omega frequencies */
     int n_omega;
     double eta;
+    int samples;              /* thermal: sample vectors, 1..64 */
+    uint64_t seed;            /* thermal: the block's base seed */
+    const double* betas;      /* thermal: n_beta inverse temperatures */
+    int n_beta;
 } qb_request;
 typedef struct {
     int status;               /* QB_OK, or the error of the solve (qb_last_error then describes it) */
     int n_values;
-    double values[QB_SERVER_MAX_LEVELS];   /* eigs: the levels ascending; dynamics: E0 */
-    int converged;            /* eigs: converged; dynamics: the ground state certified */
+    double values[QB_SERVER_MAX_LEVELS];   /* eigs: the levels ascending; dynamics: E0; thermal: the lowest Ritz value */
+    int converged;            /* eigs: converged; dynamics: the ground state certified; thermal: 1 */
     int matvecs;
     double e0, conv_change;   /* dynamics */
     double t_submit, t_admit, t_done;      /* seconds on the server's clock (qb_server_clock) */
@@ -382,7 +397,8 @@ typedef struct {
 int qb_server_create(int max_active, uint64_t hbm_budget, qb_server** out);
 int qb_server_submit(qb_server* s, const qb_request* r, uint64_t* ticket);
 /* Waits up to timeout_ms (< 0: no limit) for a ticket; QB_ETIMEOUT when it is not done. A returned result
- * releases the ticket. S: NULL or n_omega doubles for a dynamics request's spectrum. */
+ * releases the ticket. S: NULL, or the request's curves: a dynamics request's spectrum (n_omega doubles); a
+ * thermal request's lnZ, E and V per beta (3 x n_beta doubles, in that order). */
 int qb_server_wait(qb_server* s, uint64_t ticket, int timeout_ms, qb_result* out, double* S);
 int qb_server_clock(qb_server* s, double* seconds);
 /* Finishes the admitted requests and drops the queued ones; call it once no thread waits on a ticket. */

@@ -26,7 +26,7 @@ EXPORTS = [
     "qb_matvec", "qb_matvec_block", "qb_matvec_host",
     "qb_csr_build", "qb_csr_upload", "qb_csr_destroy", "qb_csr_info", "qb_csr_download", "qb_csr_matvec",
     "qb_program_attach_csr",
-    "qb_lanczos", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
+    "qb_lanczos", "qb_staged_start", "qb_eigs_lowest", "qb_ftlm", "qb_ftlm_blocks", "qb_thermal_combine", "qb_cf",
     "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_eigs_levels", "qb_dynamics_t0", "qb_dynamics_t0_manifold", "qb_dense_levels",
     "qb_dense_levels_blocks",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
@@ -53,7 +53,7 @@ class ProgramDesc(C.Structure):
     ]
 
 
-QB_REQ_EIGS, QB_REQ_DYNAMICS = 0, 1
+QB_REQ_EIGS, QB_REQ_DYNAMICS, QB_REQ_THERMAL = 0, 1, 2
 QB_SERVER_MAX_LEVELS = 16
 
 
@@ -61,6 +61,7 @@ class Request(C.Structure):
     _fields_ = [
         ("kind", C.c_int), ("sector", SectorDesc), ("h", ProgramDesc), ("k", C.c_int), ("target", SectorDesc),
         ("op", ProgramDesc), ("krylov", C.c_int), ("omega", C.c_void_p), ("n_omega", C.c_int), ("eta", C.c_double),
+        ("samples", C.c_int), ("seed", C.c_uint64), ("betas", C.c_void_p), ("n_beta", C.c_int),
     ]
 
 
@@ -132,6 +133,7 @@ def lib():
     L.qb_eigs_k.argtypes = [vp, vp, i, u64, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0_manifold.argtypes = [i, vp, vp, vp, vp, vp, i, vp, i, C.c_double, C.c_double, vp, vp,
                                           C.POINTER(i), C.POINTER(i)]
+    L.qb_staged_start.argtypes = [u64, u64, vp]
     L.qb_eigs_levels.argtypes = [vp, vp, i, u64, i, i, vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]
     L.qb_dynamics_t0.argtypes = [vp, vp, vp, vp, vp, i, vp, i, d, vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
     L.qb_dense_levels.argtypes = [vp, vp, vp]

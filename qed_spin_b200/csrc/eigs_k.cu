@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <limits>
 #include <memory>
 #include <random>
@@ -58,6 +59,77 @@ __global__ void k_take_alpha(const double2* coef, int at, int j, int first, doub
         alpha[j] = -coef[at].x;
     else
         alpha[j] -= coef[at].x;
+}
+
+// Partial inner products of w with up to 8 basis vectors per block: block (x, y) sums conj(V_b[i]) w[i] over chunk
+// x of the rows for b in [8y, 8y + 8) and writes them to part[b * chunks + x] (k_dot_sum then adds the chunks in
+// order and negates). w is read once per 8 vectors. flag (may be null): nothing is done when *flag == 0.
+constexpr int kDotVecs = 8;
+template <class T>
+__global__ void k_dots8(std::uint64_t n, int m, const T* const* basis, const double2* w, double2* part, int chunks,
+                        const int* flag) {
+    if (flag && *flag == 0) return;
+    __shared__ double sm[2 * kDotVecs * 32];
+    const int b0 = blockIdx.y * kDotVecs;
+    const int nv = min(kDotVecs, m - b0);
+    const std::uint64_t per = (n + chunks - 1) / chunks;
+    const std::uint64_t lo = static_cast<std::uint64_t>(blockIdx.x) * per;
+    const std::uint64_t hi = lo + per < n ? lo + per : n;
+    double acc[2 * kDotVecs];
+#pragma unroll
+    for (int q = 0; q < 2 * kDotVecs; ++q) acc[q] = 0.0;
+    const T* vb[kDotVecs];
+#pragma unroll
+    for (int q = 0; q < kDotVecs; ++q) vb[q] = q < nv ? basis[b0 + q] : nullptr;
+    for (std::uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const double2 y = w[i];
+#pragma unroll
+        for (int q = 0; q < kDotVecs; ++q)
+            if (q < nv) {
+                const double2 v = V<T>::ld(vb[q], i);
+                acc[2 * q] += v.x * y.x + v.y * y.y;
+                acc[2 * q + 1] += v.x * y.y - v.y * y.x;
+            }
+    }
+    block_reduce<2 * kDotVecs>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < nv; ++q)
+            part[static_cast<std::size_t>(b0 + q) * chunks + blockIdx.x] = make_double2(acc[2 * q], acc[2 * q + 1]);
+}
+
+// w -= alpha_j v_j + beta_j v_{j-1} (vp null: no beta term), the scalars read from device memory.
+template <class T>
+__global__ void k_recur(std::uint64_t n, double2* w, const T* vj, const T* vp, const double* alpha, const double* beta) {
+    const double a = *alpha, b = vp ? *beta : 0.0;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const double2 x = V<T>::ld(vj, i);
+        double2 y = w[i];
+        y.x -= a * x.x;
+        y.y -= a * x.y;
+        if (vp) {
+            const double2 z = V<T>::ld(vp, i);
+            y.x -= b * z.x;
+            y.y -= b * z.y;
+        }
+        w[i] = y;
+    }
+}
+
+// The DGKS gate of the reorthogonalisation pass just made: *flag = 1 (a second pass) when the projections it
+// removed carry more than 1 - kappa^2 of the squared norm w had before it (||w||^2 before = *before^2; the
+// projections on an orthonormal basis: sum |coef|^2), else 0. With `at` >= 0, alpha[j] -= Re coef[at].
+__global__ void k_gate(const double2* coef, int nb, const double* before, int* flag, int at, int j, double* alpha) {
+    double s = 0.0;
+    for (int i = 0; i < nb; ++i) s += coef[i].x * coef[i].x + coef[i].y * coef[i].y;
+    const double b2 = (*before) * (*before);
+    *flag = s > (1.0 - 0.5) * b2 ? 1 : 0;   // kappa = 1/sqrt(2)
+    if (at >= 0) alpha[j] -= coef[at].x;
+}
+
+// alpha[j] -= Re coef[at] when *flag != 0 (the gated second pass's correction).
+__global__ void k_take_alpha_gated(const double2* coef, int at, int j, const int* flag, double* alpha) {
+    if (*flag) alpha[j] -= coef[at].x;
 }
 
 // out = w / beta stored as T; a beta at or below floor marks a breakdown at step j (the smallest j wins) and
@@ -197,14 +269,17 @@ template <> constexpr int dtype_of<float2>() { return QB_C64; }
 
 template <class T> class ThickRestart {
 public:
-    // cycle: the basis length of a cycle (0: about 2k + 40, at least k + 24), shortened to fit 85% of the free
-    // memory.
+    // cycle: the basis length of a cycle (0: 3k + 10, at least 16; QB_EIGS_CYCLE overrides), shortened to fit 85%
+    // of the free memory. Short cycles keep the full reorthogonalisation cheap: over a sweep of 16 to 44 vectors on
+    // the chain-32 sector (k = 2) and the chain-20 sector (k = 4) the shortest took the fewest matvecs and time.
     ThickRestart(const qb_sector* sec, const qb_program* prog, int k, std::uint64_t budget, std::size_t cycle = 0)
         : sec_(sec), prog_(prog), n_(sec->dim), k_(k), budget_(budget), scale_(norm_bound(prog)),
           floor_(kFloorRel * norm_bound(prog)), nb_(red_blocks(sec->dim)) {
         const std::size_t es = sizeof(T);
+        if (cycle == 0) cycle = env_size("QB_EIGS_CYCLE");
         std::size_t m = cycle > 0 ? cycle
-                                  : std::max<std::size_t>(2 * static_cast<std::size_t>(k) + 40, static_cast<std::size_t>(k) + 24);
+                                  : std::max<std::size_t>(3 * static_cast<std::size_t>(k) + 10, 16);
+        keep_frac_ = env_size("QB_EIGS_KEEP");
         m = static_cast<std::size_t>(std::min<std::uint64_t>(m, n_));
         const double free_b = 0.85 * static_cast<double>(available_bytes());
         auto need = [&](std::size_t mm) {   // basis + kept Ritz vectors + locked + the FP64 work vector
@@ -223,6 +298,8 @@ public:
         const std::size_t cap = m_ + 1 + 2 * static_cast<std::size_t>(k) + 8;
         ptrs_.alloc(cap);
         coef_.alloc(cap);
+        arrow_.alloc(cap);
+        flag_.alloc(1);
         part_.alloc(static_cast<std::size_t>(kMaxRedBlocks) + cap * static_cast<std::size_t>(dot_chunks(n_, 1)));
         alpha_.alloc(m_ + 1);
         beta_.alloc(m_ + 2);
@@ -236,7 +313,7 @@ public:
 
     // The k lowest pairs: values ascending (fewer when the block is smaller); vectors kept as T.
     void run(LevelsOut& out) {
-        start_from_host(staged_seed(n_, kStartSeed));
+        start_from_host(staged_seed(n_, kStartSeed).data());
         std::mt19937_64 fresh(kFreshSeed);
         int null_starts = 0;
         bool stalled = false;
@@ -300,27 +377,29 @@ public:
     int matvecs() const { return matvecs_; }
 
 private:
-    static std::size_t keep_for(std::size_t m) {   // kept Ritz vectors at a restart: about a third of the cycle
+    // kept Ritz vectors at a restart: about a third of the cycle (QB_EIGS_KEEP: that many instead)
+    std::size_t keep_for(std::size_t m) const {
         if (m <= 2) return 1;
-        return std::min<std::size_t>(m - 1, std::max<std::size_t>(m / 3, 4));
+        if (keep_frac_ > 0) return std::min<std::size_t>(m - 1, std::max<std::size_t>(keep_frac_, static_cast<std::size_t>(k_)));
+        return std::min<std::size_t>(m - 1, std::max<std::size_t>(m / 3, static_cast<std::size_t>(k_) + 4));
+    }
+    static std::size_t env_size(const char* name) {   // a tuning override from the environment (0: none)
+        const char* e = std::getenv(name);
+        return e ? static_cast<std::size_t>(std::strtoull(e, nullptr, 10)) : 0;
     }
     double tol() const { return (std::is_same<T, float2>::value ? kLockTolF32 : kLockTol) * scale_; }
     bool budget_exhausted() const { return static_cast<std::uint64_t>(matvecs_) >= budget_; }
     T* col(std::size_t j) { return Vb_.p + j * n_; }
     Scal red() { return Scal{nullptr, nullptr, nullptr, red_part_.p, red_cnt_.p}; }
 
-    void start_from_host(const std::vector<cd>& v) {
-        cuda_check(cudaMemcpy(w_.p, v.data(), n_ * 16, cudaMemcpyHostToDevice), "start upload");
+    void start_from_host(const cd* v) {
+        cuda_check(cudaMemcpy(w_.p, v, n_ * 16, cudaMemcpyHostToDevice), "start upload");
         have_start_ = true;
     }
-    void start_fresh(std::mt19937_64& gen) {
-        std::vector<cd> v(n_);
-        std::normal_distribution<double> nd(0.0, 1.0);
-        for (auto& z : v) {
-            const double re = nd(gen);
-            z = cd(re, nd(gen));
-        }
-        start_from_host(v);
+    void start_fresh(std::mt19937_64& gen) {   // drawn on the device from a seed the lane's generator gives
+        k_fresh_start<<<nb_, kThreads>>>(n_, gen(), w_.p);
+        cuda_check(cudaGetLastError(), "fresh start");
+        have_start_ = true;
     }
 
     // Device pointer table: the locked vectors, then the cycle's columns 0..m.
@@ -332,15 +411,40 @@ private:
     }
     const T* const* basis() const { return reinterpret_cast<const T* const*>(ptrs_.p); }
 
-    // Two classical Gram-Schmidt passes of w against the first nb entries of the table; with at >= 0 the
-    // negated overlap with entry `at` goes to alpha[j] (summed over both passes).
-    void cgs2(int nb, int at, int j) {
+    // coef_[0, nb) = -<table entry i, w> for the nb table entries from `from` (gated by flag when non-null).
+    void dots(int from, int nb, const int* flag) {
+        const int chunks = dot_chunks(n_, (nb + kDotVecs - 1) / kDotVecs);
+        k_dots8<T><<<dim3(chunks, (nb + kDotVecs - 1) / kDotVecs), kThreads>>>(n_, nb, basis() + from, w_.p, part_.p,
+                                                                               chunks, flag);
+        k_dot_sum<<<(nb + 127) / 128, 128>>>(nb, chunks, part_.p, coef_.p, flag);
+    }
+
+    // One reorthogonalisation pass of w against the first nb table entries, then a second when the DGKS gate
+    // asks (its decision on the device); with at >= 0 the pass's overlap with entry `at` corrects alpha[j].
+    void reorth(int nb, int at, int j) {
         if (nb == 0) return;
-        for (int pass = 0; pass < 2; ++pass) {
-            dot_many<T>(n_, nb, basis(), w_.p, coef_.p, part_.p, nullptr, nullptr);
-            k_axpy_many<T><<<nb_, kThreads>>>(n_, nb, basis(), coef_.p, w_.p, nullptr);
-            if (at >= 0) k_take_alpha<<<1, 1>>>(coef_.p, at, j, pass == 0 ? 1 : 0, alpha_.p);
-        }
+        k_norm_to<<<nb_, kThreads>>>(n_, w_.p, red(), slots_.p + 1, nullptr);
+        dots(0, nb, nullptr);
+        k_axpy_many<T><<<nb_, kThreads>>>(n_, nb, basis(), coef_.p, w_.p, nullptr);
+        k_gate<<<1, 1>>>(coef_.p, nb, slots_.p + 1, flag_.p, at, j, alpha_.p);
+        dots(0, nb, flag_.p);
+        k_axpy_many<T><<<nb_, kThreads>>>(n_, nb, basis(), coef_.p, w_.p, flag_.p);
+        if (at >= 0) k_take_alpha_gated<<<1, 1>>>(coef_.p, at, j, flag_.p, alpha_.p);
+    }
+
+    // Step j of a cycle from w = A v_j: alpha_j = Re <v_j, w>; w -= alpha_j v_j and the recurrence's coupling to
+    // the earlier basis (beta_j v_{j-1}, or the kept Ritz vectors' arrow after a restart); then the
+    // reorthogonalisation against the whole basis and the locked vectors, which now removes only rounding-level
+    // components (alpha_j takes its overlap too).
+    void step_projections(int L, std::size_t j, std::size_t p) {
+        const int jj = static_cast<int>(j);
+        dots(L + jj, 1, nullptr);
+        k_take_alpha<<<1, 1>>>(coef_.p, 0, jj, 1, alpha_.p);
+        const T* vp = (j > p) ? col(j - 1) : nullptr;
+        k_recur<T><<<nb_, kThreads>>>(n_, w_.p, col(j), vp, alpha_.p + j, beta_.p + j);
+        if (j == p && p > 0)   // the arrow: w -= sum_i s_i u_i over the kept Ritz vectors (coefficients staged)
+            k_axpy_many<T><<<nb_, kThreads>>>(n_, static_cast<int>(p), basis() + L, arrow_.p, w_.p, nullptr);
+        reorth(L + jj + 1, L + jj, jj);
     }
 
     // One search from the start in w_: lock up to `want` of the lowest pairs. Returns the number locked, or -1
@@ -351,7 +455,7 @@ private:
         have_start_ = false;
         write_ptrs();
         const int L = static_cast<int>(locked_.size());
-        cgs2(L, -1, 0);
+        reorth(L, -1, 0);
         k_norm_to<<<nb_, kThreads>>>(n_, w_.p, red(), slots_.p, nullptr);
         double nrm = 0.0;
         cuda_check(cudaMemcpy(&nrm, slots_.p, 8, cudaMemcpyDeviceToHost), "start norm");
@@ -368,9 +472,14 @@ private:
                 steps = static_cast<std::size_t>(std::min<std::uint64_t>(steps, budget_ - std::min<std::uint64_t>(budget_, matvecs_)));
             if (steps == 0) return 0;
             const std::size_t mend = p + steps;
+            if (p > 0) {   // the arrow couplings of the kept Ritz vectors, negated, as the axpy's coefficients
+                std::vector<double2> ar(p);
+                for (std::size_t i = 0; i < p; ++i) ar[i] = make_double2(-arrow[i], 0.0);
+                cuda_check(cudaMemcpy(arrow_.p, ar.data(), p * 16, cudaMemcpyHostToDevice), "arrow");
+            }
             for (std::size_t j = p; j < mend; ++j) {
                 launch_walk_mixed(sec_, sec_, prog_, col(j), w_.p, dtype_of<T>(), QB_C128, nullptr);
-                cgs2(L + static_cast<int>(j) + 1, L + static_cast<int>(j), static_cast<int>(j));
+                step_projections(L, j, p);
                 k_norm_to<<<nb_, kThreads>>>(n_, w_.p, red(), beta_.p + j + 1, nullptr);
                 k_next_col<T><<<nb_, kThreads>>>(n_, w_.p, col(j + 1), beta_.p + j + 1, floor_, brk_.p, static_cast<int>(j));
             }
@@ -449,9 +558,10 @@ private:
     std::uint64_t budget_;
     double scale_, floor_;
     int nb_;
-    std::size_t m_ = 0, p_ = 0;
+    std::size_t m_ = 0, p_ = 0, keep_frac_ = 0;
     DevBuf<T> Vb_, U_;
-    DevBuf<double2> w_, coef_, part_;
+    DevBuf<double2> w_, coef_, part_, arrow_;
+    DevBuf<int> flag_;
     DevBuf<void*> ptrs_;
     DevBuf<double> alpha_, beta_, slots_, red_part_, S_;
     DevBuf<unsigned> red_cnt_;

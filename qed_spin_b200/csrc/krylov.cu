@@ -1251,6 +1251,13 @@ double* noalloc_scratch() {
 
 extern "C" {
 
+int qb_staged_start(uint64_t seed, uint64_t n, double* out) {
+    return qb::guarded([&] {
+        if (!out && n) throw qb::Error(QB_EINVAL, "null argument");
+        qb::staged_seed_into(reinterpret_cast<std::complex<double>*>(out), static_cast<std::size_t>(n), seed);
+    });
+}
+
 int qb_lanczos(const qb_sector* sec, const qb_program* prog, const double* v0_host, int max_iter, int reorth,
                double breakdown_tol, int dtype, double* alpha, double* beta, int* iters) {
     return qb::guarded([&] {

@@ -275,6 +275,8 @@ extern "C" {
 }  // extern "C"
 
 namespace qb {
+bool dense_levels_device(const qb_sector* const* secs, const qb_program* const* progs, int n_blocks,
+                         const std::vector<std::size_t>& off, double* values);
 namespace {
 // One block's full spectrum: assembled on the calling thread's stream, reduced on the host.
 void dense_levels(const qb_sector* sec, const qb_program* prog, double* values) {
@@ -302,7 +304,9 @@ extern "C" {
 int qb_dense_levels(const qb_sector* sec, const qb_program* prog, double* values) {
     return qb::guarded([&] {
         if (!sec || !prog || !values) throw qb::Error(QB_EINVAL, "null argument");
-        qb::dense_levels(sec, prog, values);
+        const qb_sector* secs[1] = {sec};
+        const qb_program* progs[1] = {prog};
+        if (!qb::dense_levels_device(secs, progs, 1, {0}, values)) qb::dense_levels(sec, prog, values);
     });
 }
 
@@ -316,7 +320,10 @@ int qb_dense_levels_blocks(const qb_sector* const* secs, const qb_program* const
             if (!secs[b] || !progs[b]) throw Error(QB_EINVAL, "null block");
             off[b + 1] = off[b] + secs[b]->dim;
         }
-        // largest first over a pool of host threads, each assembling on its own stream
+        // blocks of at most 1024 states: all at once on the device (dense.cu)
+        if (dense_levels_device(secs, progs, n_blocks, off, values)) return;
+        // larger blocks: largest first over a pool of host threads, each assembling on its own stream and
+        // reducing on the host
         std::vector<int> order(n_blocks);
         for (int b = 0; b < n_blocks; ++b) order[b] = b;
         std::sort(order.begin(), order.end(), [&](int a, int b) { return secs[a]->dim > secs[b]->dim; });

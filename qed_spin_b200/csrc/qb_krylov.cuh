@@ -17,6 +17,9 @@
 #include <random>
 #include <vector>
 
+#include <atomic>
+#include <thread>
+
 #include "qb_internal.cuh"
 
 namespace qb {
@@ -765,11 +768,180 @@ template <class Gen> void gaussian_fill(std::vector<std::complex<double>>& v, Ge
     }
 }
 
-std::vector<std::complex<double>> staged_seed(std::size_t n, std::uint64_t seed) {
-    std::vector<std::complex<double>> v(n);
-    std::mt19937_64 gen(seed);
-    gaussian_fill(v, gen);
-    return v;
+// The staged Gaussian start of dimension n from mt19937_64(seed): entry i = (re, im) with im drawn first, the
+// stream of std::normal_distribution<double> over the generator (block_solve.cpp:263-277), bit for bit. Past 2^20
+// entries the stream is produced in parallel. A normal pair comes from one accepted polar attempt: two raw 64-bit
+// outputs u1, u2 give x = 2 c(u1) - 1, y = 2 c(u2) - 1 with c(u) = u / 2^64 (the largest double below 1 when that
+// rounds to 1, as generate_canonical does), accepted when 0 < x^2 + y^2 <= 1; the first normal is y m, the second
+// x m, m = sqrt(-2 log(r2) / r2); so entry i is (x_i m_i, y_i m_i) of the i-th accepted attempt. One thread runs
+// the generator in order through a ring of chunk buffers and counts each chunk's accepted attempts (so it knows
+// where the chunk's entries go); the other threads take the chunks in turn and form their entries in place.
+inline double polar_canonical(std::uint64_t u) {
+    const double r = static_cast<double>(u) / 18446744073709551616.0;
+    return r >= 1.0 ? std::nextafter(1.0, 0.0) : r;
+}
+
+// MT19937-64 (M. Matsumoto and T. Nishimura, the 64-bit Mersenne Twister of 2000; the parameters std::mt19937_64
+// is defined with), producing its outputs a state block (312 words) at a time: the same sequence as
+// std::mt19937_64 seeded alike, faster than drawing word by word.
+struct Mt64 {
+    static constexpr int kN = 312, kM = 156;
+    static constexpr std::uint64_t kA = 0xB5026F5AA96619E9ULL, kUpper = 0xFFFFFFFF80000000ULL, kLower = 0x7FFFFFFFULL;
+    std::uint64_t mt[kN];
+    explicit Mt64(std::uint64_t seed) {
+        mt[0] = seed;
+        for (int i = 1; i < kN; ++i) mt[i] = 6364136223846793005ULL * (mt[i - 1] ^ (mt[i - 1] >> 62)) + static_cast<std::uint64_t>(i);
+    }
+    static std::uint64_t twist(std::uint64_t a, std::uint64_t b, std::uint64_t c) {
+        const std::uint64_t x = (a & kUpper) | (b & kLower);
+        return c ^ (x >> 1) ^ ((x & 1ULL) ? kA : 0ULL);
+    }
+    // The next kN outputs, tempered, into out.
+    void block(std::uint64_t* out) {
+        for (int i = 0; i < kN - kM; ++i) mt[i] = twist(mt[i], mt[i + 1], mt[i + kM]);
+        for (int i = kN - kM; i < kN - 1; ++i) mt[i] = twist(mt[i], mt[i + 1], mt[i + kM - kN]);
+        mt[kN - 1] = twist(mt[kN - 1], mt[0], mt[kM - 1]);
+        for (int i = 0; i < kN; ++i) {
+            std::uint64_t y = mt[i];
+            y ^= (y >> 29) & 0x5555555555555555ULL;
+            y ^= (y << 17) & 0x71D67FFFEDA60000ULL;
+            y ^= (y << 37) & 0xFFF7EEE000000000ULL;
+            y ^= y >> 43;
+            out[i] = y;
+        }
+    }
+};
+
+// A polar attempt (u1, u2) with the exact generate_canonical arithmetic: x, y and r2, or -1 when rejected.
+inline double polar_r2(std::uint64_t u1, std::uint64_t u2, double& x, double& y) {
+    x = 2.0 * polar_canonical(u1) - 1.0;
+    y = 2.0 * polar_canonical(u2) - 1.0;
+    const double r2 = x * x + y * y;
+    return (r2 > 1.0 || r2 == 0.0) ? -1.0 : r2;
+}
+
+// The accepted polar attempts among `count` (raw output pairs at r): a cheap branch-free estimate of r2 decides every
+// attempt unless one lies within 1e-9 of a boundary (r2 = 1 or r2 = 0), in which case the exact arithmetic
+// recounts them all.
+inline std::size_t polar_count(const std::uint64_t* r, std::size_t count) {
+    std::size_t k = 0;
+    int near = 0;
+    for (std::size_t a = 0; a < count; ++a) {
+        const double xa = static_cast<double>(static_cast<std::int64_t>(r[2 * a] >> 1)) * 0x1.0p-62 - 1.0;
+        const double ya = static_cast<double>(static_cast<std::int64_t>(r[2 * a + 1] >> 1)) * 0x1.0p-62 - 1.0;
+        const double ra = xa * xa + ya * ya;
+        k += static_cast<std::size_t>(ra < 1.0);
+        near |= static_cast<int>(std::fabs(ra - 1.0) <= 1e-9) | static_cast<int>(ra <= 1e-9);
+    }
+    if (!near) return k;
+    k = 0;
+    for (std::size_t a = 0; a < count; ++a) {
+        double x, y;
+        k += polar_r2(r[2 * a], r[2 * a + 1], x, y) >= 0.0 ? 1 : 0;
+    }
+    return k;
+}
+
+// A host vector of complex doubles left uninitialised (the draw writes every entry; its pages are touched by the
+// threads that write them).
+struct HostVec {
+    std::unique_ptr<double[]> buf;
+    std::size_t n = 0;
+    explicit HostVec(std::size_t count) : buf(new double[2 * count]), n(count) {}
+    std::complex<double>* data() { return reinterpret_cast<std::complex<double>*>(buf.get()); }
+    const std::complex<double>* data() const { return reinterpret_cast<const std::complex<double>*>(buf.get()); }
+    std::size_t size() const { return n; }
+};
+
+void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed) {
+    if (n < (std::size_t{1} << 20)) {
+        std::mt19937_64 gen(seed);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        for (std::size_t i = 0; i < n; ++i) {
+            const double im = nd(gen);
+            const double re = nd(gen);
+            v[i] = std::complex<double>(re, im);
+        }
+        return;
+    }
+    constexpr std::size_t kAtt = static_cast<std::size_t>(Mt64::kN) * 256;   // polar attempts per chunk
+    const int nw = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) - 1);
+    const std::size_t ring = 4 * static_cast<std::size_t>(nw);
+    std::vector<std::uint64_t> buf(ring * 2 * kAtt);
+    struct Slot {
+        std::atomic<std::size_t> chunk{~std::size_t{0}};   // the chunk it holds (ready), or none
+        std::atomic<bool> busy{false};
+        std::size_t off = 0;                              // where the chunk's first entry goes
+    };
+    std::vector<Slot> slots(ring);
+    std::atomic<std::size_t> n_chunks{~std::size_t{0}}, next{0};
+    std::vector<std::thread> pool;
+    pool.emplace_back([&] {   // the generator, in order, counting each chunk's accepted attempts
+        Mt64 gen(seed);
+        std::size_t off = 0, c = 0;
+        for (; off < n; ++c) {
+            Slot& sl = slots[c % ring];
+            while (sl.busy.load(std::memory_order_acquire)) std::this_thread::yield();
+            sl.busy.store(true, std::memory_order_relaxed);
+            std::uint64_t* r = buf.data() + (c % ring) * 2 * kAtt;
+            for (std::size_t b = 0; b < 2 * kAtt; b += Mt64::kN) gen.block(r + b);
+            const std::size_t k = polar_count(r, kAtt);
+            sl.off = off;
+            off += k;
+            sl.chunk.store(c, std::memory_order_release);
+        }
+        n_chunks.store(c, std::memory_order_release);
+    });
+    for (int t = 0; t < nw; ++t)
+        pool.emplace_back([&] {
+            for (std::size_t c = next++;; c = next++) {
+                Slot& sl = slots[c % ring];
+                for (;;) {   // wait for chunk c, or for the generator to stop short of it
+                    if (sl.chunk.load(std::memory_order_acquire) == c) break;
+                    const std::size_t nc = n_chunks.load(std::memory_order_acquire);
+                    if (nc != ~std::size_t{0} && c >= nc) return;
+                    std::this_thread::yield();
+                }
+                const std::uint64_t* r = buf.data() + (c % ring) * 2 * kAtt;
+                std::size_t i = sl.off;
+                for (std::size_t a = 0; a < kAtt && i < n; ++a) {
+                    double x, y;
+                    const double r2 = polar_r2(r[2 * a], r[2 * a + 1], x, y);
+                    if (r2 < 0.0) continue;
+                    const double m = std::sqrt(-2 * std::log(r2) / r2);
+                    v[i++] = std::complex<double>(x * m * 1.0 + 0.0, y * m * 1.0 + 0.0);
+                }
+                sl.chunk.store(~std::size_t{0}, std::memory_order_relaxed);
+                sl.busy.store(false, std::memory_order_release);
+            }
+        });
+    for (auto& t : pool) t.join();
+}
+
+HostVec staged_seed(std::size_t n, std::uint64_t seed) {
+    HostVec hv(n);
+    staged_seed_into(hv.data(), n, seed);
+    return hv;
+}
+
+// A fresh random start on the device (no reference stream to follow): entry i = two unit normals by Box-Muller
+// from a counter hash of (seed, i).
+__device__ __forceinline__ std::uint64_t mix64(std::uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+__global__ void k_fresh_start(std::uint64_t n, std::uint64_t seed, double2* x) {
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const std::uint64_t a = mix64(seed + 0x9E3779B97F4A7C15ULL * (2 * i + 1));
+        const std::uint64_t b = mix64(seed + 0x9E3779B97F4A7C15ULL * (2 * i + 2));
+        const double u = (static_cast<double>(a >> 11) + 0.5) * 0x1.0p-53, w = static_cast<double>(b >> 11) * 0x1.0p-53;
+        const double r = sqrt(-2.0 * log(u));
+        double sn, cs;
+        sincospi(2.0 * w, &sn, &cs);
+        x[i] = make_double2(r * cs, r * sn);
+    }
 }
 
 std::mt19937 sample_engine(std::uint64_t base_seed, std::uint64_t sample) {

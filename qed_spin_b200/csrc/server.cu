@@ -1,6 +1,6 @@
 // =============================================================================
-// server.cu -- the request server: eigs and T = 0 dynamics solves of sectors of different sizes, served with
-// continuous batching on one GPU.
+// server.cu -- the request server: eigs, thermal (one block's FTLM) and T = 0 dynamics solves of sectors of
+// different sizes, served with continuous batching on one GPU.
 //
 // Requests queue in arrival order. A worker admits the head of the queue when a slot is free and the request's
 // estimated HBM footprint (sectors, reduced CSRs, Krylov vectors) fits what the budget has left; a request
@@ -80,8 +80,10 @@ struct Job {
     SectorCopy sec, tgt;
     ProgramCopy h, op;
     int k = 1, krylov = 200;
-    std::vector<double> omega;
+    std::vector<double> omega, betas;
     double eta = 0.05;
+    int samples = 0;
+    std::uint64_t seed = 0;
     std::uint64_t footprint = 0, allowance = 0, csr_budget = 0;
     double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
     bool done = false;
@@ -113,7 +115,9 @@ std::uint64_t csr_bytes(std::uint64_t n, const qb_program_desc& p) { return n * 
 void plan(Job& j, std::uint64_t budget) {
     const std::uint64_t n = estimate_dim(j.sec.d);
     std::uint64_t fixed = sector_bytes(n), csr = csr_bytes(n, j.h.d), work = 0, keep = 0;
-    if (j.kind == QB_REQ_EIGS) {
+    if (j.kind == QB_REQ_THERMAL) {
+        work = static_cast<std::uint64_t>(j.samples) * 16 * 4 * n + 16 * n;   // three sample blocks, w, the start
+    } else if (j.kind == QB_REQ_EIGS) {
         if (j.k <= 1) {
             work = 48 * n;   // the recurrence's w and two vectors
         } else {
@@ -260,6 +264,20 @@ void qb_server::run(qb::Job& j) {
             j.converged = cv;
             j.matvecs = mv;
         }
+    } else if (j.kind == QB_REQ_THERMAL) {
+        qb_sector* s = sector(j.sec.d);
+        qb_program* p = s ? program(j.h.d) : nullptr;
+        if (!p) return;
+        lane(s, p);
+        const std::size_t nb = j.betas.size();
+        j.S.assign(3 * nb, 0.0);
+        double e_min = 0.0;
+        if (step(qb_ftlm(s, p, j.samples, j.krylov, j.seed, j.betas.data(), static_cast<int>(nb), QB_C128, j.S.data(),
+                         j.S.data() + nb, j.S.data() + 2 * nb, &e_min),
+                 j) != QB_OK)
+            return;
+        j.values = {e_min};
+        j.converged = 1;
     } else {
         qb_sector* src = sector(j.sec.d);
         qb_sector* tgt = src ? sector(j.tgt.d) : nullptr;
@@ -304,7 +322,8 @@ int qb_server_submit(qb_server* s, const qb_request* r, uint64_t* ticket) {
     return qb::guarded([&] {
         using namespace qb;
         if (!s || !r || !ticket) throw Error(QB_EINVAL, "null argument");
-        if (r->kind != QB_REQ_EIGS && r->kind != QB_REQ_DYNAMICS) throw Error(QB_EINVAL, "request: unknown kind");
+        if (r->kind != QB_REQ_EIGS && r->kind != QB_REQ_DYNAMICS && r->kind != QB_REQ_THERMAL)
+            throw Error(QB_EINVAL, "request: unknown kind");
         auto j = std::make_shared<Job>();
         j->kind = r->kind;
         j->sec.take(r->sector);
@@ -312,6 +331,15 @@ int qb_server_submit(qb_server* s, const qb_request* r, uint64_t* ticket) {
         j->k = r->k;
         if (r->kind == QB_REQ_EIGS && (r->k < 1 || r->k > QB_SERVER_MAX_LEVELS))
             throw Error(QB_EINVAL, "request: k must be in [1, 16]");
+        if (r->kind == QB_REQ_THERMAL) {
+            if (r->samples < 1 || r->samples > 64) throw Error(QB_EINVAL, "request: samples must be in [1, 64]");
+            if (r->krylov < 2) throw Error(QB_EINVAL, "request: krylov must be >= 2");
+            if (!r->betas || r->n_beta < 1) throw Error(QB_EINVAL, "request: no temperatures");
+            j->samples = r->samples;
+            j->krylov = r->krylov;
+            j->seed = r->seed;
+            j->betas.assign(r->betas, r->betas + r->n_beta);
+        }
         if (r->kind == QB_REQ_DYNAMICS) {
             j->tgt.take(r->target);
             j->op.take(r->op);

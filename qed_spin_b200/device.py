@@ -271,6 +271,13 @@ def lanczos(sec: Sector, prog: Program, v0: np.ndarray, max_iter: int, reorth: i
     return a[:m].copy(), b[: m + 1].copy()
 
 
+def staged_start(seed: int, n: int) -> np.ndarray:
+    """The lanes' staged Gaussian start (qb_staged_start): host work, the reference's mt19937_64 stream."""
+    out = np.zeros(n, np.complex128)
+    check(lib().qb_staged_start(seed, n, out.ctypes.data))
+    return out
+
+
 def eigs_lowest(sec: Sector, prog: Program, max_iter: int = 0, dtype="c128", refine: bool = True) -> dict:
     e, it, cv, mv = C.c_double(), C.c_int(), C.c_int(), C.c_int()
     check(lib().qb_eigs_lowest(sec.h, prog.h, max_iter, _dt(dtype), 1 if refine else 0, C.byref(e), C.byref(it),
@@ -439,8 +446,9 @@ def _program_desc(prog: HostProgram, keep: list) -> "_lib.ProgramDesc":
 
 
 class Server:
-    """The request server (qb_server_*): eigs and T = 0 dynamics requests served concurrently on the device
-    with admission by HBM footprint. submit() returns a ticket at once; wait() returns the result."""
+    """The request server (qb_server_*): eigs, thermal (one block's FTLM) and T = 0 dynamics requests served
+    concurrently on the device with admission by HBM footprint. submit() returns a ticket at once; wait() returns
+    the result."""
 
     def __init__(self, max_active: int = 8, hbm_budget: int = 0):
         h = C.c_void_p()
@@ -478,16 +486,42 @@ class Server:
         self.n_omega[t.value] = len(omega)
         return t.value
 
+    def submit_thermal(self, spec, h: HostProgram, samples: int, krylov: int, seed: int, betas) -> int:
+        """One block of the thermal driver's sampled path: its FTLM curves (lnZ, E, V per beta)."""
+        keep = []
+        betas = np.ascontiguousarray(betas, np.float64)
+        keep.append(betas)
+        r = _lib.Request()
+        r.kind = _lib.QB_REQ_THERMAL
+        r.sector = _sector_desc(spec, keep)
+        r.h = _program_desc(h, keep)
+        r.krylov = krylov
+        r.samples = samples
+        r.seed = seed
+        r.betas = betas.ctypes.data
+        r.n_beta = len(betas)
+        t = C.c_uint64()
+        check(lib().qb_server_submit(self.h, C.byref(r), C.byref(t)))
+        self.n_omega[t.value] = ("thermal", len(betas))
+        return t.value
+
     def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
         res = _lib.Result()
         no = self.n_omega.pop(ticket, 0)
+        thermal = isinstance(no, tuple)
+        if thermal:
+            no = 3 * no[1]
         S = np.zeros(no) if no else None
         check(lib().qb_server_wait(self.h, ticket, timeout_ms, C.byref(res), None if S is None else S.ctypes.data))
         if res.status != _lib.QB_OK:
             check(res.status)
-        return {"values": np.array(res.values[: res.n_values]), "converged": bool(res.converged),
-                "matvecs": res.matvecs, "e0": res.e0, "conv_change": res.conv_change, "S": S,
-                "t_submit": res.t_submit, "t_admit": res.t_admit, "t_done": res.t_done, "footprint": res.footprint}
+        out = {"values": np.array(res.values[: res.n_values]), "converged": bool(res.converged),
+               "matvecs": res.matvecs, "e0": res.e0, "conv_change": res.conv_change, "S": S,
+               "t_submit": res.t_submit, "t_admit": res.t_admit, "t_done": res.t_done, "footprint": res.footprint}
+        if thermal:
+            nb = no // 3
+            out.update(lnZ=S[:nb], E=S[nb:2 * nb], V=S[2 * nb:], e_min=out["values"][0], S=None)
+        return out
 
     def clock(self) -> float:
         t = C.c_double()

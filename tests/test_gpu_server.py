@@ -116,3 +116,35 @@ def test_bad_request_fails_alone():
     for t in tickets:
         assert srv.wait(t)["converged"]
     srv.close()
+
+
+def test_thermal_requests_served():
+    """Thermal requests (one block of the thermal driver's sampled path each) served in a mix with eigs requests:
+    each block's lnZ, E, V equal a direct qb_ftlm call on the same reduced-CSR lane bit for bit, and the oracle's
+    FTLM of the block within 1e-8 relative."""
+    from oracle import oracle as O
+    from qed_spin_b200 import device as D
+    N, seed = 12, 4242
+    betas = 1.0 / np.linspace(0.2, 3.0, 15)
+    prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.5) + ops.zeeman_z_products(N, 0.1)
+    h = ops.row_program(ops.from_products(N, prods))
+    blocks = [lat.chain_sector(N, 6, 0), lat.chain_sector(N, 5, 3), lat.chain_sector(N, 4, 7)]
+    srv = D.Server(max_active=4)
+    tickets = [srv.submit_thermal(b, h, 8, 30, seed, betas) for b in blocks]
+    tickets.append(srv.submit_eigs(blocks[0], h, 2))
+    got = [srv.wait(t) for t in tickets]
+    srv.close()
+    Po = O.Program(h)
+    for spec, g in zip(blocks, got[:3]):
+        S, P = D.Sector(spec), D.Program(h)
+        A = D.Csr(S, S, P)
+        A.attach(P)
+        one = D.ftlm(S, P, 8, 30, seed, betas)
+        A.close()
+        for key in ("lnZ", "E", "V"):
+            assert np.array_equal(_bits(g[key]), _bits(one[key])), key
+        ref = O.Sector(spec).ftlm(Po, 8, 30, seed, betas)
+        for key in ("lnZ", "E", "V"):
+            r = np.asarray(ref[key])
+            np.testing.assert_allclose(g[key], r, rtol=1e-8, atol=1e-8 * max(np.abs(r).max(), 1e-3), err_msg=key)
+    assert got[3]["converged"] and len(got[3]["values"]) == 2

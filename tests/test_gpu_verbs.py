@@ -54,8 +54,24 @@ def test_dense_levels_match_dense_solve():
         np.testing.assert_allclose(got, _dense_levels(spec, prog), rtol=0, atol=1e-12 * 20)
 
 
+@pytest.mark.parametrize("N,n_up,k", [(16, 8, 0), (16, 7, 3), (18, 9, 0)])
+def test_dense_levels_device_and_host_reductions(N, n_up, k):
+    """Blocks of 810, 720 (reduced on the device: Householder in a CTA, Sturm bisection) and 2,704 states (reduced on
+    the host) against numpy's dense solve of the oracle's matrix, 1e-11 of the coupling scale."""
+    from qed_spin_b200 import device as D
+    H = _model(N)
+    prog = ops.row_program(H)
+    spec = lat.chain_sector(N, n_up, k)
+    got = D.dense_levels(D.Sector(spec), D.Program(prog))
+    ref = _dense_levels(spec, prog)
+    assert len(got) == len(ref) > 700
+    sc = float(np.abs(np.asarray(prog.term_coeff)).sum())
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-11 * sc)
+
+
 def test_dense_levels_blocks_equal_one_by_one():
-    """The threaded batch returns each block's spectrum exactly as the single-block call does."""
+    """The batch (one device launch for all blocks) returns each block's spectrum exactly as the single-block call
+    does."""
     from qed_spin_b200 import device as D
     N = 12
     prog = ops.row_program(_model(N))
