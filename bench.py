@@ -76,10 +76,11 @@ SQ36_BLOCKS, SQ36_BLOCK_DIV = 4, 256
 
 
 
-# DRAM bytes (read + write) of one spmv1<complex64> launch on the 6x6 workload (None: not captured); the source says how
-# the figure was taken.
-SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH = None
-SPMV1_SQ36_TRAFFIC_SOURCE = "not captured"
+# DRAM bytes (read + write) of one spmv1<complex64> launch on the 6x6 workload, from ncu: dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch (a one-pass metric set, captured on this workload after two warm-up applies).
+SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH = 418.38e9 + 2.02e9
+SPMV1_SQ36_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one spmv1<complex64> launch on this "
+                             "workload (profiles/spmv1_sq36_csr_dram.md)")
 
 class Clocks:
     """SM clock, power and clock-event-reason samples (NVML, read only) taken every 10 ms while the timed
@@ -579,7 +580,7 @@ def chain32_measure(args, stream):
                           "rel_err_fp32_refined": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]),
                           "e0": r64["e0"], "plain_e0": r_plain["e0"]},
            "k2": {"s": k2_s, "values": list(map(float, r2["values"])), "converged": r2["converged"],
-                  "matvecs": r2["matvecs"], "lane": "Krylov-Schur on the CSR"}}
+                  "matvecs": r2["matvecs"], "lane": "thick-restart Lanczos on the CSR"}}
     A.close()
     S.close()
     if not args.no_cpu_baseline:
