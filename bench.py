@@ -607,24 +607,28 @@ def ftlm_workload():
 
 
 def ftlm_reference_sample(threads):
-    """The reference engine's sampled thermal blocks on the host cores, on a bounded stratified sample: the
-    k = 0 block of every S^z sector with 4 samples each at depth 100 (a sample's cost depends only on its
-    block, so samples/s carries over to the whole 600-block workload)."""
+    """The reference engine's sampled thermal blocks on the host cores, on a bounded stratified sample of the same
+    workload: one block of every S^z sector (momentum k = n_up mod 24), with the workload's 40 samples at depth 100.
+    A block's cost grows with its dimension, so the whole workload's time is estimated as the sample's time times
+    (states in all 554 blocks) / (states in the sample), and samples/s = 554 x 40 / that estimate."""
     from oracle import ref as R
     _, prods, _, betas = ftlm_workload()
     R.set_threads(threads)
     from qed_spin_b200 import lattice as lat
-    blocks = [lat.chain_sector(FTLM_N, n_up, 0) for n_up in range(FTLM_N + 1)]
+    blocks = [lat.chain_sector(FTLM_N, n_up, n_up % FTLM_N) for n_up in range(FTLM_N + 1)]
     rs = [R.Sector(s.n_sites, s.n_up, s.perms, s.chars, flips=s.flips, slc_mode=-1) for s in blocks]
+    rs = [r for r in rs if r.dim > 0]
     rp = R.Operator(FTLM_N, prods).row_program()
     dims = [r.dim for r in rs]
     t = time.perf_counter()
-    R.ftlm_blocks(rs, rp, 4, FTLM_DEPTH, FTLM_SEED, betas)
+    R.ftlm_blocks(rs, rp, FTLM_SAMPLES, FTLM_DEPTH, FTLM_SEED, betas)
     dt = time.perf_counter() - t
-    # whole-workload estimate: each S^z sector's 24 blocks have about its k = 0 block's dimension
-    return {"value": 4 * len(rs) / dt, "unit": "samples/s", "cores": threads, "kind": "reference",
-            "sample": f"k=0 block of each of the 25 S^z sectors (dims {min(dims)}..{max(dims)}), 4 samples, depth "
-                      f"{FTLM_DEPTH}, CSR lane, the reference's block scheduling; {dt:.1f} s"}
+    total_states, total_blocks = 2 ** FTLM_N, 554
+    est = dt * total_states / sum(dims)
+    return {"value": total_blocks * FTLM_SAMPLES / est, "unit": "samples/s", "cores": threads, "kind": "reference",
+            "sample": f"one block per S^z sector (momentum n_up mod 24; {len(rs)} blocks, dims {min(dims)}..{max(dims)}, "
+                      f"{sum(dims)} states), {FTLM_SAMPLES} samples each, depth {FTLM_DEPTH}, its CSR lane and block "
+                      f"scheduling, {dt:.1f} s; scaled to the 554 blocks ({total_states} states) by states"}
 
 
 def ftlm_config(args):
