@@ -437,7 +437,7 @@ def main():
     torch.cuda.synchronize()
 
     e0 = None
-    if not args.no_e0:
+    if not args.no_e0 and world == 1:   # the time-to-E0 runs are per-GPU facts: measured on a single replica
         e0 = {}
         A.attach(P)
         t = time.perf_counter()

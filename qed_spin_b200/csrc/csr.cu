@@ -19,6 +19,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -398,6 +399,58 @@ __global__ void __launch_bounds__(kRowsPerBlock) spmv1(u64 rows, const unsigned 
     Lo::store(out, r, acc);
 }
 
+// One vector in FP32 storage (complex64 in and out; FP64 arithmetic): 4 lanes per row. Lane l of a row reads the
+// row's 16-byte column windows l, l + 4, ... (a row's four lanes read 64 contiguous bytes of columns and 16 of ids
+// per step, where a thread per row reads 16 scattered bytes), issues the window's x loads together and sums its
+// products in window order; the four partial sums are added in the fixed order (p0 + p1) + (p2 + p3). A
+// different summation order than spmv1's, so it serves FP32 storage only, where results are compared within a
+// tolerance; FP64 storage keeps spmv1 and its bit-for-bit sums. u8 dictionary ids only.
+// It pays on long rows: 6x6 J1-J2 (75 entries a row) 87.4 -> 74.6 ms, 6x5 (62) 1.08 -> 0.96 ms; on short rows a
+// thread per row stays ahead (chain-32, 17.5 entries a row: 0.27 against 0.35 ms).
+constexpr int kTeamLanes = 4;
+__global__ void __launch_bounds__(256) spmv1_team32(u64 rows, const unsigned long long* __restrict__ row_ptr,
+                                                    const u32* __restrict__ col, const unsigned char* __restrict__ ids,
+                                                    const double2* __restrict__ vals, int n_dict,
+                                                    const float2* __restrict__ in, float2* __restrict__ out) {
+    __shared__ double2 dict[256];
+    for (int i = threadIdx.x; i < n_dict; i += blockDim.x) dict[i] = vals[i];
+    __syncthreads();
+    const u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const u64 r = t / kTeamLanes;
+    const int l = static_cast<int>(t % kTeamLanes);
+    double ar = 0.0, ai = 0.0;
+    if (r < rows) {
+        const u64 e0 = row_ptr[r], e1 = row_ptr[r + 1];
+        for (u64 w = (e0 & ~3ULL) + 4 * static_cast<u64>(l); w < e1; w += 4 * kTeamLanes) {
+            const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + w));
+            const unsigned i4 = __ldg(reinterpret_cast<const unsigned*>(ids + w));
+            const u32 cj[4] = {c4.x, c4.y, c4.z, c4.w};
+            float2 xv[4];
+            bool on[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                on[q] = w + q >= e0 && w + q < e1;
+                if (on[q]) xv[q] = __ldg(in + cj[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (on[q]) {
+                    const double2 v = dict[(i4 >> (8 * q)) & 0xFFu];
+                    const double xr = xv[q].x, xi = xv[q].y;
+                    ar += v.x * xr - v.y * xi;
+                    ai += v.x * xi + v.y * xr;
+                }
+        }
+    }
+    // (p0 + p1) + (p2 + p3) within each row's four lanes
+    double br = __shfl_xor_sync(0xffffffffu, ar, 1), bi = __shfl_xor_sync(0xffffffffu, ai, 1);
+    ar += br;
+    ai += bi;
+    br = __shfl_xor_sync(0xffffffffu, ar, 2);
+    bi = __shfl_xor_sync(0xffffffffu, ai, 2);
+    if (l == 0 && r < rows) out[r] = make_float2(__double2float_rn(ar + br), __double2float_rn(ai + bi));
+}
+
 // k vectors interleaved by row: 8 lanes per row, lane l owns columns l, l + 8, ...; each column summed in
 // CSR order (the single apply's order).
 template <bool kInF32, bool kOutF32, int kCpl>
@@ -437,11 +490,28 @@ __global__ void __launch_bounds__(256) spmvk(u64 rows, int k, const unsigned lon
     }
 }
 
+// The FP32-storage single-vector kernel: four lanes per row when the rows hold at least kTeamMinRow entries on
+// average, else one thread per row (spmv1). QB_SPMV_TEAM=0 or 1 forces one or the other.
+constexpr u64 kTeamMinRow = 32;
+bool team32_for(const qb_csr* A) {
+    static const int force = [] {
+        const char* e = std::getenv("QB_SPMV_TEAM");
+        return e && (e[0] == '0' || e[0] == '1') ? e[0] - '0' : -1;
+    }();
+    if (force >= 0) return force == 1;
+    return A->rows > 0 && A->nnz >= kTeamMinRow * A->rows;
+}
+
 template <bool kInF32, bool kOutF32>
 void spmv_launch(const qb_csr* A, const void* in, void* out, int k, cudaStream_t st) {
     const unsigned char* ids = A->ids.p;
     const double2* vals = A->vals.p;
-    if (k == 1) {
+    if (k == 1 && kInF32 && kOutF32 && A->id_bytes == 1 && team32_for(A)) {
+        const u64 threads = A->rows * kTeamLanes;
+        spmv1_team32<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(
+            A->rows, A->row_ptr.p, A->col_idx.p, ids, vals, A->n_dict, static_cast<const float2*>(in),
+            static_cast<float2*>(out));
+    } else if (k == 1) {
         spmv1<kInF32, kOutF32><<<static_cast<unsigned>((A->rows + kRowsPerBlock - 1) / kRowsPerBlock), kRowsPerBlock, 0, st>>>(
             A->rows, A->row_ptr.p, A->col_idx.p, ids, A->id_bytes, vals, A->n_dict, in, out);
     } else {

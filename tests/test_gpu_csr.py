@@ -193,3 +193,35 @@ def test_empty_sector_csr():
     assert S.dim == 0
     A = d.Csr(S, S, d.Program(ops.row_program(ops.from_products(10, ops.heisenberg_products(lat.chain_bonds(10))))))
     assert A.info()["nnz"] == 0
+
+
+@pytest.mark.parametrize("case", ["chain24", "chain20k3", "sq24"])
+def test_csr_fp32_storage_apply(case):
+    """The FP32-storage CSR apply against the FP64 apply of the same complex64-rounded x: the rows differ only by the
+    FP32 rounding of y and the order of the FP64 sums, within 1e-6 of max |y|. The chains (12 to 25 entries a row)
+    take the thread-per-row kernel, the 6x4 J1-J2 torus (about 49 a row) the four-lanes-per-row kernel."""
+    d = D()
+    if case == "sq24":
+        nn, nnn = lat.square_j1j2_bonds(6, 4)
+        N = 24
+        spec = lat.square_k0_sector(6, 4, 12)
+        prods = ops.heisenberg_products(nn, 1.0) + ops.heisenberg_products(nnn, 0.5)
+    else:
+        N, n_up, k = (24, 12, 0) if case == "chain24" else (20, 9, 3)
+        spec = lat.chain_sector(N, n_up, k)
+        prods = ops.xxz_products(lat.chain_bonds(N), 1.0, 0.7) + ops.zeeman_z_products(N, 0.1)
+    S = d.Sector(spec)
+    A = d.Csr(S, S, d.Program(ops.row_program(ops.from_products(N, prods))))
+    per_row = A.info()["nnz"] / S.dim
+    assert (per_row >= 32) == (case == "sq24")
+    rng = np.random.default_rng(3)
+    x = (rng.normal(size=S.dim) + 1j * rng.normal(size=S.dim)).astype(np.complex64)
+    x32 = torch.from_numpy(x).cuda()
+    y32 = torch.empty_like(x32)
+    A.matvec(x32, y32, dtype="c64")
+    x64 = x32.to(torch.complex128)
+    y64 = torch.empty_like(x64)
+    A.matvec(x64, y64)
+    ref = y64.cpu().numpy()
+    err = np.abs(y32.cpu().numpy().astype(np.complex128) - ref).max() / np.abs(ref).max()
+    assert err < 1e-6
