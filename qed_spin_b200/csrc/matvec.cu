@@ -65,14 +65,22 @@ __global__ void __launch_bounds__(256, (NV <= 2 && sizeof(ST) == 4 ? 6 : 4)) wal
     for (u32 g0 = 0; g0 < ng; g0 += 32) {
         const u32 gend = ng < g0 + 32 ? ng : g0 + 32;
         u32 mask = 0;
+        u64 offs = 0;   // the acting subgroup of each group, as an offset from its first (programs with vsub4)
         if (live)
-            for (u32 g = g0; g < gend; ++g)
-                if (acting_subgroup<ST>(sp.P, s, g) >= 0) mask |= 1u << (g - g0);
+            for (u32 g = g0; g < gend; ++g) {
+                const int vi = acting_subgroup<ST>(sp.P, s, g);
+                if (vi >= 0) {
+                    mask |= 1u << (g - g0);
+                    offs |= static_cast<u64>(vi - static_cast<int>(sp.P.group_vbegin[g])) << (2 * (g - g0));
+                }
+            }
         while (__any_sync(0xffffffffu, mask != 0)) {
             if (mask == 0) continue;
-            const u32 g = g0 + static_cast<u32>(__ffs(mask) - 1);
+            const u32 gi = static_cast<u32>(__ffs(mask) - 1);
+            const u32 g = g0 + gi;
             mask &= mask - 1;
-            const int vi = acting_subgroup<ST>(sp.P, s, g);
+            const int vi = sp.P.vsub4 ? static_cast<int>(sp.P.group_vbegin[g] + ((offs >> (2 * gi)) & 3u))
+                                      : acting_subgroup<ST>(sp.P, s, g);
             const cplx h = subgroup_value<ST>(sp.P, s, vi);
             const ST t = s ^ static_cast<ST>(sp.P.group_flip[g]);
             long long j;
@@ -95,6 +103,7 @@ __global__ void __launch_bounds__(256, (NV <= 2 && sizeof(ST) == 4 ? 6 : 4)) wal
 // order -- the row's entries in group order, with walk_rows's operations.
 struct WarpSlots {
     u64 state[32];
+    u64 offs[32];   // each row's acting-subgroup offsets in the window (programs with vsub4)
     double w[32];
     u32 mask[32], pre[32], incl[32];
     int ok[32];
@@ -125,9 +134,15 @@ __global__ void __launch_bounds__(256, 4) walk_warp(DSector row, DSector col, DP
     for (u32 g0 = 0; g0 < ng; g0 += 32) {
         const u32 gend = ng < g0 + 32 ? ng : g0 + 32;
         u32 mask = 0;
+        u64 offs = 0;
         if (live)
-            for (u32 g = g0; g < gend; ++g)
-                if (acting_subgroup<ST>(sp.P, s, g) >= 0) mask |= 1u << (g - g0);
+            for (u32 g = g0; g < gend; ++g) {
+                const int vi = acting_subgroup<ST>(sp.P, s, g);
+                if (vi >= 0) {
+                    mask |= 1u << (g - g0);
+                    offs |= static_cast<u64>(vi - static_cast<int>(sp.P.group_vbegin[g])) << (2 * (g - g0));
+                }
+            }
         const u32 cnt = static_cast<u32>(__popc(mask));
         u32 incl = cnt;   // inclusive prefix over the lanes
 #pragma unroll
@@ -138,6 +153,7 @@ __global__ void __launch_bounds__(256, 4) walk_warp(DSector row, DSector col, DP
         const u32 pre = incl - cnt;
         const u32 total = __shfl_sync(0xffffffffu, incl, 31);
         W.mask[lane] = mask;
+        W.offs[lane] = offs;
         W.pre[lane] = pre;
         W.incl[lane] = incl;
         __syncwarp();
@@ -152,7 +168,9 @@ __global__ void __launch_bounds__(256, 4) walk_warp(DSector row, DSector col, DP
                     if (W.incl[o + step - 1] <= q) o += step;
                 const ST so = static_cast<ST>(W.state[o]);
                 const u32 g = g0 + __fns(W.mask[o], 0, static_cast<int>(q - W.pre[o]) + 1);
-                const int vi = acting_subgroup<ST>(sp.P, so, g);
+                const int vi = sp.P.vsub4
+                                   ? static_cast<int>(sp.P.group_vbegin[g] + ((W.offs[o] >> (2 * (g - g0))) & 3u))
+                                   : acting_subgroup<ST>(sp.P, so, g);
                 const cplx h = subgroup_value<ST>(sp.P, so, vi);
                 const ST t = so ^ static_cast<ST>(sp.P.group_flip[g]);
                 long long j;
@@ -563,6 +581,9 @@ int qb_program_create(const qb_program_desc* d, qb_program** out) {
         v.term_sign = reinterpret_cast<const u64*>(b + offs[5]);
         v.term_coeff = reinterpret_cast<const double2*>(b + offs[6]);
         v.smem_bytes = total;
+        v.vsub4 = 1;
+        for (uint32_t g = 0; g < d->n_groups; ++g)
+            if (d->group_vbegin[g + 1] - d->group_vbegin[g] > 4) v.vsub4 = 0;
         for (uint32_t k = 0; k < d->n_terms; ++k) p->norm_bound += std::hypot(d->term_coeff[2 * k], d->term_coeff[2 * k + 1]);
         *out = p.release();
     });

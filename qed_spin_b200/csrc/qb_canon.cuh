@@ -85,14 +85,14 @@ template <class ST> __device__ __forceinline__ u32 pattern_of(ST k, int j, int N
 
 // The several-blocks case of for_each_candidate: merge the ascending candidate lists of every block that
 // reaches the least leading block (each element maps exactly one block to the lead).
-template <class ST, class Fn>
-__device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pack, ST k, u32 best, Fn& fn) {
-    const int L = S.slc.L, m = S.slc.m, N = S.N;
+template <class Pat, class Fn>
+__device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pack, const Pat& pat, u32 best, Fn& fn) {
+    const int L = S.slc.L, m = S.slc.m;
     u64 sel[8];
     u32 pos[8];
     int n = 0;
     for (int j = 0; j < m; ++j) {
-        const u64 e = pack[(static_cast<u32>(j) << L) + pattern_of(k, j, N, L)];
+        const u64 e = pack[(static_cast<u32>(j) << L) + pat(j)];
         if (static_cast<u32>(e & 0xFFFFu) == best) {
             sel[n] = e;
             pos[n] = 0;
@@ -119,15 +119,16 @@ __device__ __forceinline__ void merge_candidates(const DSector& S, const u64* pa
 }
 
 // fn(g) in ascending order for the elements whose image has the least leading block
-// (sublattice_code.h:102-131); returns that least leading block. One packed load per block.
-template <class ST, class Fn>
-__device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* pack, ST k, Fn&& fn) {
-    const int L = S.slc.L, m = S.slc.m, N = S.N;
+// (sublattice_code.h:102-131); returns that least leading block. One packed load per block; pat(j) is block j's
+// pattern.
+template <class Pat, class Fn>
+__device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* pack, const Pat& pat, Fn&& fn) {
+    const int L = S.slc.L, m = S.slc.m;
     u32 best = 0xFFFFFFFFu;
     u64 first = 0;
     int n = 0;
     for (int j = 0; j < m; ++j) {
-        const u64 e = pack[(static_cast<u32>(j) << L) + pattern_of(k, j, N, L)];
+        const u64 e = pack[(static_cast<u32>(j) << L) + pat(j)];
         const u32 v = static_cast<u32>(e & 0xFFFFu);
         if (v < best) {
             best = v;
@@ -147,34 +148,91 @@ __device__ __forceinline__ u32 for_each_candidate(const DSector& S, const u64* p
         }
         return best;
     }
-    merge_candidates(S, pack, k, best, fn);
+    if (S.unit_chars) {
+        // +1/-1 characters: the sum over the ties is exact in any order, so each tied block's list is walked in
+        // turn (the representative is the least key whichever order finds it)
+        for (int j = 0; j < m; ++j) {
+            const u64 e = pack[(static_cast<u32>(j) << L) + pat(j)];
+            if (static_cast<u32>(e & 0xFFFFu) != best) continue;
+            const u32 cnt = static_cast<u32>((e >> 16) & 0xFFFFu);
+            const u32 pay = static_cast<u32>(e >> 32);
+            if (cnt == 1) {
+                fn(static_cast<int>(pay));
+            } else {
+                for (u32 p = 0; p < cnt; ++p) fn(static_cast<int>(__ldg(S.slc.cand + pay + p)));
+            }
+        }
+        return best;
+    }
+    merge_candidates(S, pack, pat, best, fn);
     return best;
 }
 
+template <class ST> __device__ __forceinline__ int top_bit(ST x);
+template <> __device__ __forceinline__ int top_bit<u64>(u64 x) { return 63 - __clzll(static_cast<long long>(x)); }
+template <> __device__ __forceinline__ int top_bit<u32>(u32 x) { return 31 - __clz(static_cast<int>(x)); }
+
+// key(a) < key(b) for a != b, read from the states themselves: the first block in which they differ decides, and
+// within it the highest differing site (sublattice_code.h:23-34: block 0 leads the key, a block's sites in
+// ascending order take ascending key bits).
+template <class ST> __device__ __forceinline__ bool key_below(const DSlc& c, ST a, ST b) {
+    const ST d = a ^ b;
+    for (int j = 0; j < c.m; ++j) {
+        const ST dj = d & static_cast<ST>(c.bmask[j]);
+        if (dj) return ((a >> top_bit<ST>(dj)) & static_cast<ST>(1)) == 0;
+    }
+    return false;
+}
+
+// Block j's pattern of a state: its sites' bits in ascending site order (the key's block-j field).
+template <class ST> struct BlockPattern {
+    ST t;
+    int N, L, contig;
+    __device__ BlockPattern(const DSector& S, const u64* to_key, ST x)
+        : t(S.slc.contig ? x : key_of<ST>(to_key, S.bpw, x)), N(S.N), L(S.slc.L), contig(S.slc.contig) {}
+    __device__ u32 operator()(int j) const {
+        return contig ? static_cast<u32>(t >> (j * L)) & ((1u << L) - 1u) : pattern_of<ST>(t, j, N, L);
+    }
+};
+
 // Representative of t and the conjugated character sum over the elements that reach it.
+// With a key order the images are compared in place (key_below), so no image is mapped to its key.
 template <class ST>
 __device__ __forceinline__ ST canonicalize(const DSector& S, const Tables& T, ST t, double& acc_re, double& acc_im) {
-    ST rb = static_cast<ST>(~static_cast<ST>(0)), best = static_cast<ST>(~static_cast<ST>(0));
+    ST rb = static_cast<ST>(~static_cast<ST>(0));
     acc_re = 0.0;
     acc_im = 0.0;
-    auto visit = [&](int g) {
-        const ST img = apply_elem<ST>(S, T, t, g);
-        const ST k = S.slc.on ? key_of<ST>(T.to_key, S.bpw, img) : img;
-        if (k < best) {
-            best = k;
-            rb = img;
-            const double2 c = T.chars[g];
-            acc_re = __dadd_rn(0.0, c.x);
-            acc_im = __dsub_rn(0.0, c.y);
-        } else if (k == best) {
-            const double2 c = T.chars[g];
-            acc_re = __dadd_rn(acc_re, c.x);
-            acc_im = __dsub_rn(acc_im, c.y);
-        }
-    };
     if (S.slc.on) {
-        for_each_candidate<ST>(S, T.pack, key_of<ST>(T.to_key, S.bpw, t), visit);
+        bool have = false;
+        auto visit = [&](int g) {
+            const ST img = apply_elem<ST>(S, T, t, g);
+            if (!have || (img != rb && key_below<ST>(S.slc, img, rb))) {
+                have = true;
+                rb = img;
+                const double2 c = T.chars[g];
+                acc_re = __dadd_rn(0.0, c.x);
+                acc_im = __dsub_rn(0.0, c.y);
+            } else if (img == rb) {
+                const double2 c = T.chars[g];
+                acc_re = __dadd_rn(acc_re, c.x);
+                acc_im = __dsub_rn(acc_im, c.y);
+            }
+        };
+        for_each_candidate(S, T.pack, BlockPattern<ST>(S, T.to_key, t), visit);
     } else {
+        auto visit = [&](int g) {
+            const ST img = apply_elem<ST>(S, T, t, g);
+            if (img < rb) {
+                rb = img;
+                const double2 c = T.chars[g];
+                acc_re = __dadd_rn(0.0, c.x);
+                acc_im = __dsub_rn(0.0, c.y);
+            } else if (img == rb) {
+                const double2 c = T.chars[g];
+                acc_re = __dadd_rn(acc_re, c.x);
+                acc_im = __dsub_rn(acc_im, c.y);
+            }
+        };
         for (int g = 0; g < S.G; ++g) visit(g);
     }
     return rb;

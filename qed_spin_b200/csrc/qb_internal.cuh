@@ -134,6 +134,11 @@ struct DSlc {
     // the candidate itself when there is one, else the offset of the block's list in `cand`
     const u64* pack = nullptr;      // m << L
     const u16* cand = nullptr;
+    // the sites of block j as a state mask; within a block, a higher site holds a higher key bit, so two states
+    // compare in the key order by the highest differing site of the first block in which they differ
+    u64 bmask[8] = {};
+    // block j is sites [jL, (j+1)L) in order: its pattern is state bits jL .. jL+L-1, no key needed
+    int contig = 0;
 };
 
 // Group element kinds with an arithmetic action (0: the byte-LUT action).
@@ -147,6 +152,9 @@ struct DSector {
     const u64* lut = nullptr;       // G x bpw x 256
     const u64* flips = nullptr;     // G
     const double2* chars = nullptr; // G
+    // every character exactly +1 or -1 (imaginary part zero): a character sum is then an exact integer whatever
+    // the order of its terms, so tied candidate lists need no ordered merge
+    int unit_chars = 0;
     // arithmetic group action (gkind != 0): per element kind | rotation << 8 | row shift << 16, and the
     // torus row mask; gkind 1 chains (rotations, reflections), 2 torus translations with row length Lx
     int gkind = 0, Lx = 0;
@@ -178,6 +186,7 @@ struct DProgram {
     const u64* term_sign = nullptr;
     const double2* term_coeff = nullptr;
     std::size_t smem_bytes = 0;   // bytes to stage the whole program in shared memory
+    int vsub4 = 0;                // every group has at most 4 value subgroups (a 2-bit offset names one)
 };
 
 }  // namespace qb
@@ -201,7 +210,8 @@ struct qb_sector {
     int idx_bits = 0;
     qb::DevBuf<double> inv_class;
     int hash_bits = 0, n_class = 0;
-    int slc_on = 0, slc_L = 0, slc_m = 0;
+    int slc_on = 0, slc_L = 0, slc_m = 0, slc_contig = 0;
+    qb::u64 slc_bmask[8] = {};
     int lookup = 0;
     qb::u64 bucket_base = 0, bucket_count = 0;
     int bucket_shift = 0;

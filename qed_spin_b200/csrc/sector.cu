@@ -60,7 +60,9 @@ std::vector<u64> build_lut(const int32_t* perms, int G, int N) {
 
 struct SlcHost {
     bool on = false;
+    bool contig = false;
     int L = 0, m = 0;
+    std::vector<u64> bmask;   // the sites of each block
     std::vector<u64> to_key;
     std::vector<u16> lead;
     std::vector<u32> cand_off;
@@ -158,6 +160,12 @@ SlcHost build_slc(const int32_t* perms, const u64* flips, int G, int N, int mode
     c.on = true;
     c.L = L;
     c.m = m;
+    c.bmask.assign(m, 0ULL);
+    c.contig = true;
+    for (int s = 0; s < N; ++s) {
+        c.bmask[block[s]] |= 1ULL << s;
+        if (block[s] != s / L || slot[s] != s % L) c.contig = false;
+    }
     const int bpw = (N + 7) / 8;
     std::vector<int> key_bit(N);
     for (int s = 0; s < N; ++s) key_bit[s] = N - (block[s] + 1) * L + slot[s];
@@ -284,7 +292,7 @@ __device__ __forceinline__ double visit_inv_norm(const DSector& S, const Tables&
         }
         if (least < pattern_of<u64>(k, 0, S.N, S.slc.L)) return 0.0;
         bool rep = true;
-        for_each_candidate<u64>(S, T.pack, k, [&](int g) {
+        for_each_candidate(S, T.pack, [&](int j) { return pattern_of<u64>(k, j, S.N, S.slc.L); }, [&](int g) {
             if (!rep) return;
             const u64 ik = key_of<u64>(T.to_key, S.bpw, apply_elem<u64>(S, T, s, g));
             if (ik < k) {
@@ -524,6 +532,8 @@ void upload_group(qb_sector& s, const qb_sector_desc& d) {
     if (slc.on) {
         s.slc_L = slc.L;
         s.slc_m = slc.m;
+        s.slc_contig = slc.contig ? 1 : 0;
+        for (int j = 0; j < slc.m; ++j) s.slc_bmask[j] = slc.bmask[j];
         s.to_key.upload(slc.to_key);
         std::vector<u64> pack(slc.lead.size());
         for (std::size_t i = 0; i < pack.size(); ++i) {
@@ -681,9 +691,14 @@ qb::DSector qb_sector::view() const {
     v.lut = lut.p;
     v.flips = flips.p;
     v.chars = chars.p;
+    v.unit_chars = 1;
+    for (std::size_t i = 0; i + 1 < chars_host.size(); i += 2)
+        if (chars_host[i + 1] != 0.0 || (chars_host[i] != 1.0 && chars_host[i] != -1.0)) v.unit_chars = 0;
     v.slc.on = slc_on;
     v.slc.L = slc_L;
     v.slc.m = slc_m;
+    v.slc.contig = slc_contig;
+    for (int j = 0; j < 8; ++j) v.slc.bmask[j] = slc_bmask[j];
     v.slc.to_key = to_key.p;
     v.slc.pack = lead_pack.p;
     v.slc.cand = cand.p;

@@ -5,7 +5,8 @@
 // per state, a warp's states compacted, or for one vector a team of 4 to 32 lanes per state; the block walk:
 // 4, 8, 16 or 32 lanes per state) asks tune_choose for a shape. The first call for a shape key (the kernel family, the sector's and
 // program's size classes, the vector count and types, the device) times every candidate on the caller's stream
-// with CUDA events -- each candidate runs once to warm up, then three times timed -- and keeps the fastest;
+// with CUDA events -- each candidate runs once to warm up, then three times timed (once when a run takes more than
+// 50 ms, and not at all when its warm-up is already half again slower than the pick) -- and keeps the fastest;
 // later calls reuse it. Because the candidates agree bit for bit, a choice changes only the time.
 //
 // Modes (QB_TUNE, or qb_tune_mode): 1 measure on first use (default); 2 use only choices already known (from
@@ -128,14 +129,28 @@ int tune_choose(const char* family, const std::string& key, int n, int fallback,
     float best = 0.0f;
     try {
         for (int i = 0; i < n; ++i) {
-            run(i);   // warm-up: module load, first touch of the tables
+            // warm-up: module load, first touch of the tables. A long candidate (above kLongMs) whose warm-up is
+            // already half again slower than the pick is not timed further, and long candidates are timed once:
+            // on a 252M-state sector one walk takes seconds, and three runs of every shape took two minutes.
             cuda_check(cudaEventRecord(e0, st), "event");
-            for (int r = 0; r < 3; ++r) run(i);
+            run(i);
+            cuda_check(cudaEventRecord(e1, st), "event");
+            cuda_check(cudaEventSynchronize(e1), "tune");
+            float wms = 0.0f;
+            cuda_check(cudaEventElapsedTime(&wms, e0, e1), "event time");
+            constexpr float kLongMs = 50.0f;
+            if (i > 0 && wms > kLongMs && wms > 1.5f * best) {
+                c.ms.push_back(wms);
+                continue;
+            }
+            const int reps = wms > kLongMs ? 1 : 3;
+            cuda_check(cudaEventRecord(e0, st), "event");
+            for (int r = 0; r < reps; ++r) run(i);
             cuda_check(cudaEventRecord(e1, st), "event");
             cuda_check(cudaEventSynchronize(e1), "tune");
             float ms = 0.0f;
             cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
-            ms /= 3.0f;
+            ms /= static_cast<float>(reps);
             c.ms.push_back(ms);
             // a candidate must beat the current pick by 3% to replace it (lower indices are the defaults)
             if (i == 0 || ms < 0.97f * best) {
