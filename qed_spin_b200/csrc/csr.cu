@@ -8,9 +8,9 @@
 // zeros dropped. The values go into a dictionary when there are at most 65536 distinct ones (u8 ids for
 // at most 256), else they are stored whole.
 //
-// Build: a count pass (merged row lengths) -> CUB scan -> a dictionary pass (every merged value into a
-// device hash set keyed by its bits) -> a fill pass (columns and ids; each id's value is checked bit
-// for bit). Each pass recomputes the rows from the walk.
+// Build: a count pass (merged row lengths; every merged value into a device hash set keyed by its bits) -> CUB
+// scan -> a fill pass (columns and ids; each id's value is checked bit for bit). Each pass recomputes the rows
+// from the walk.
 //
 // The matvec sums each row sequentially in CSR order, one thread per row; with k vectors interleaved by
 // row each lane owns a slice of the columns and sums them in the same order, so every vector of a block
@@ -164,7 +164,7 @@ template <class T> struct PoolBuf {
 // warp's buffer in group (emission) order under the key column << 8 | emission index. A bitonic sort of the
 // keys orders the entries by column and, within a column, by emission; each column's run is then summed in
 // that order and kept when not exactly zero (merge_row, include/ed/matvec/sector_rows.h:147-158).
-// pass 0: merged row lengths; pass 1: the merged values into the dictionary set; pass 2: columns and ids.
+// pass 0: merged row lengths, and the merged values into the dictionary set; pass 2: columns and ids.
 constexpr int kBuildWarps = 4;
 
 template <class ST, bool kSame>
@@ -244,25 +244,32 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
             }
             continue;
         }
-        // bitonic sort of keys[0, n), n the power of two >= m, padded with ~0
-        int n = 32;
-        while (n < m) n <<= 1;
-        for (int i = m + lane; i < n; i += 32) keys[i] = ~0ULL;
+        // the keys (distinct: column << 8 | emission index) sorted by rank: lane l holds keys l, l + 32, ...; every
+        // key of the row is read once by the whole warp (a broadcast) and counted against the held ones, then each
+        // held key is written to its rank
         __syncwarp();
-        for (int k = 2; k <= n; k <<= 1) {
-            for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                for (int i = lane; i < n; i += 32) {
-                    const int l = i ^ jj;
-                    if (l > i) {
-                        const u64 a = keys[i], b = keys[l];
-                        if ((a > b) == ((i & k) == 0)) {
-                            keys[i] = b;
-                            keys[l] = a;
-                        }
-                    }
-                }
-                __syncwarp();
+        {
+            constexpr int kHeld = kMaxRowEntries / 32;
+            u64 mine[kHeld];
+            int rank[kHeld];
+#pragma unroll
+            for (int i = 0; i < kHeld; ++i) {
+                const int at = i * 32 + lane;
+                mine[i] = at < m ? keys[at] : ~0ULL;
+                rank[i] = 0;
             }
+            const int held = (m + 31) >> 5;
+            for (int q = 0; q < m; ++q) {
+                const u64 kq = keys[q];
+#pragma unroll
+                for (int i = 0; i < kHeld; ++i)
+                    if (i < held) rank[i] += kq < mine[i] ? 1 : 0;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < kHeld; ++i)
+                if (i * 32 + lane < m) keys[rank[i]] = mine[i];
+            __syncwarp();
         }
         // each column's run summed in emission order; exact zeros dropped; kept entries compacted in order
         int mo = 0;
@@ -285,7 +292,7 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
             const unsigned bal = __ballot_sync(0xffffffffu, keep);
             if (keep) {
                 const u64 o = static_cast<u64>(mo + __popc(bal & lt));
-                if (pass == 1) {
+                if (pass == 0) {
                     dict_insert(D, sum);
                 } else if (pass == 2) {
                     col_out[base + o] = cj;
@@ -638,7 +645,17 @@ int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* p
         PoolBuf<int> flags(4);
         cuda_check(cudaMemsetAsync(flags.p, 0, 16, nullptr), "flags clear");
         int hflags[4] = {0, 0, 0, 0};
-        Dict D{nullptr, 0, nullptr, nullptr, flags.p + 1, reinterpret_cast<u32*>(flags.p + 2)};
+        // the value set, filled by the count pass: at most half full while it can still become a dictionary
+        // (65536 values in 2^kDictBits slots), and no larger than twice the entries can fill (rows x groups)
+        u64 nslots = 1024;
+        const u64 most = row->dim * std::max<u64>(1, prog->view.n_groups);
+        while (nslots < 2 * most && nslots < (1ULL << kDictBits)) nslots <<= 1;
+        PoolBuf<u64> keys(nslots);
+        PoolBuf<double2> dvals(nslots);
+        PoolBuf<u32> dids(nslots);
+        PoolBuf<double2> dict(kMaxDict);
+        cuda_check(cudaMemsetAsync(keys.p, 0xFF, nslots * 8, nullptr), "dict clear");
+        Dict D{keys.p, nslots - 1, dvals.p, dids.p, flags.p + 1, reinterpret_cast<u32*>(flags.p + 2)};
         {
             PoolBuf<unsigned long long> counts(row->dim);
             auto passes = [&](int pass, unsigned char* ids, int id_bytes, double2* full) {
@@ -660,18 +677,6 @@ int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* p
         cuda_check(cudaMemcpy(&A->nnz, A->row_ptr.p + row->dim, 8, cudaMemcpyDeviceToHost), "nnz read");
         cuda_check(cudaMemcpy(hflags, flags.p, 16, cudaMemcpyDeviceToHost), "flags read");
         if (hflags[0]) throw Error(QB_EUNSUPPORTED, "CSR: a row has more than 256 entries before merging");
-        // the value set: at most half full while it can still become a dictionary
-        u64 nslots = 1024;
-        while (nslots < 2 * A->nnz && nslots < (1ULL << kDictBits)) nslots <<= 1;
-        PoolBuf<u64> keys(nslots);
-        PoolBuf<double2> dvals(nslots);
-        PoolBuf<u32> dids(nslots);
-        PoolBuf<double2> dict(kMaxDict);
-        cuda_check(cudaMemsetAsync(keys.p, 0xFF, nslots * 8, nullptr), "dict clear");
-        D.keys = keys.p;
-        D.mask = nslots - 1;
-        D.vals = dvals.p;
-        D.ids = dids.p;
         auto passes = [&](int pass, unsigned char* ids, int id_bytes, double2* full) {
             if (narrow)
                 build_passes<u32>(row, col, prog, pass, nullptr, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
@@ -680,7 +685,6 @@ int qb_csr_build(const qb_sector* row, const qb_sector* col, const qb_program* p
                 build_passes<u64>(row, col, prog, pass, nullptr, A->row_ptr.p, A->col_idx.p, ids, id_bytes, full, D,
                                   flags.p);
         };
-        passes(1, nullptr, 0, nullptr);
         dict_compact<<<1, 1024>>>(keys.p, dvals.p, nslots, dids.p, dict.p, flags.p + 3);
         cuda_check(cudaGetLastError(), "dictionary");
         cuda_check(cudaMemcpy(hflags, flags.p, 16, cudaMemcpyDeviceToHost), "dictionary read");
