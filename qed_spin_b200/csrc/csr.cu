@@ -66,6 +66,13 @@ __device__ __forceinline__ void dict_insert(const Dict& D, cplx v) {
     const u64 key = value_key(v);
     u64 h = key & mask;
     for (u64 probe = 0; probe <= mask; ++probe) {
+        // a plain read first: most values are already in the set, and a key once written never changes
+        const u64 seen = __ldcg(reinterpret_cast<const unsigned long long*>(D.keys + h));
+        if (seen == key) return;
+        if (seen != kEmpty) {
+            h = (h + 1) & mask;
+            continue;
+        }
         const u64 old = atomicCAS(reinterpret_cast<unsigned long long*>(D.keys + h), kEmpty, key);
         if (old == kEmpty) {
             D.vals[h] = make_double2(v.re, v.im);
@@ -166,6 +173,8 @@ template <class T> struct PoolBuf {
 // that order and kept when not exactly zero (merge_row, include/ed/matvec/sector_rows.h:147-158).
 // pass 0: merged row lengths, and the merged values into the dictionary set; pass 2: columns and ids.
 constexpr int kBuildWarps = 4;
+constexpr int kColSetBits = 8;   // the count pass's per-warp column set: 256 slots, for rows of up to 128 entries
+constexpr int kColSet = 1 << kColSetBits;
 
 template <class ST, bool kSame>
 __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSector col, DProgram P, bool prog_in_smem,
@@ -173,13 +182,19 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
                                                              unsigned long long* counts,
                                                              const unsigned long long* row_ptr, u32* col_out,
                                                              unsigned char* ids, int id_bytes, double2* full_vals,
-                                                             Dict D, int* too_long) {
+                                                             Dict D, int* too_long, bool tag_rows) {
     extern __shared__ __align__(16) unsigned char smem[];
     const SmemProgram sp = stage(P, col, smem, prog_in_smem);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     u64* keys = reinterpret_cast<u64*>(smem + stage_bytes) + wid * kMaxRowEntries;
     double2* vals = reinterpret_cast<double2*>(smem + stage_bytes + kBuildWarps * kMaxRowEntries * 8) +
                     wid * kMaxRowEntries;
+    // the count pass's column set: a warp's slots tagged row << 32 | column, so no row clears them
+    u64* cset = reinterpret_cast<u64*>(smem + stage_bytes + kBuildWarps * kMaxRowEntries * 24) + wid * kColSet;
+    if (pass == 0) {
+        for (int i = lane; i < kColSet; i += 32) cset[i] = ~0ULL;
+        __syncwarp();
+    }
     const unsigned lt = (1u << lane) - 1u;
     const u64 nwarps = static_cast<u64>(gridDim.x) * kBuildWarps;
     for (u64 r = static_cast<u64>(blockIdx.x) * kBuildWarps + wid; r < row.dim; r += nwarps) {
@@ -244,10 +259,54 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
             }
             continue;
         }
+        __syncwarp();
+        if (pass == 0 && tag_rows && 2 * m <= kColSet) {
+            // Does any column repeat? Each entry's column goes into the warp's set; a column already tagged with this
+            // row is a repeat. Without one (the rule: 99.9% of the 6x6 J1-J2 rows) every entry is its own merged
+            // value, so the row keeps its nonzero entries and needs no sort.
+            bool rep = false;
+            for (int i = lane; i < m; i += 32) {
+                const u64 tag = (r << 32) | (keys[i] >> 8);
+                u32 h = (static_cast<u32>(keys[i] >> 8) * 0x9E3779B1u) >> (32 - kColSetBits);
+                // a slot tagged with another row is free; a lost race re-reads the slot. The loop is bounded (the
+                // row fills at most half the set, and each lost race is another lane's win); past the bound the
+                // row takes the sorting path, which is right whatever the set says.
+                int tries = 0;
+                for (;; ++tries) {
+                    if (tries > 4 * kColSet) {
+                        rep = true;
+                        break;
+                    }
+                    const u64 v = *reinterpret_cast<volatile u64*>(cset + h);
+                    if (v == tag) {
+                        rep = true;
+                        break;
+                    }
+                    if ((v >> 32) != (r & 0xFFFFFFFFULL)) {
+                        if (atomicCAS(reinterpret_cast<unsigned long long*>(cset + h), v, tag) == v) break;
+                        continue;
+                    }
+                    h = (h + 1) & (kColSet - 1);
+                }
+            }
+            if (!__any_sync(0xffffffffu, rep)) {
+                int kept = 0;
+                for (int i = lane; i < m; i += 32) {
+                    const double2 v = vals[i];
+                    if (v.x != 0.0 || v.y != 0.0) {
+                        dict_insert(D, {v.x, v.y});
+                        ++kept;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+                if (lane == 0) counts[r] = static_cast<unsigned long long>(kept);
+                __syncwarp();
+                continue;
+            }
+        }
         // the keys (distinct: column << 8 | emission index) sorted by rank: lane l holds keys l, l + 32, ...; every
         // key of the row is read once by the whole warp (a broadcast) and counted against the held ones, then each
         // held key is written to its rank
-        __syncwarp();
         {
             constexpr int kHeld = kMaxRowEntries / 32;
             u64 mine[kHeld];
@@ -546,7 +605,7 @@ void run_pass(const qb_sector* row, const qb_sector* col, const qb_program* P, i
               const Dict& D, int* too_long) {
     bool in_smem = false;
     const std::size_t stage_bytes = (smem_for(P, col, in_smem) + 15) & ~std::size_t(15);
-    const std::size_t smem = stage_bytes + kBuildWarps * kMaxRowEntries * (8 + 16);
+    const std::size_t smem = stage_bytes + kBuildWarps * kMaxRowEntries * (8 + 16) + kBuildWarps * kColSet * 8;
     auto k = csr_pass<ST, kSame>;
     set_smem(k, smem);
     int sms = 148, dev = 0;
@@ -554,8 +613,10 @@ void run_pass(const qb_sector* row, const qb_sector* col, const qb_program* P, i
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const u64 want = (row->dim + kBuildWarps - 1) / kBuildWarps;
     const unsigned blocks = static_cast<unsigned>(std::max<u64>(1, std::min<u64>(want, static_cast<u64>(sms) * 16)));
+    // row tags hold the low 32 bits of the row: rows past 2^32 take the sorting path
+    const bool tag_rows = row->dim < (1ULL << 32);
     k<<<blocks, 32 * kBuildWarps, smem>>>(row->view(), col->view(), P->view, in_smem, stage_bytes, pass, counts,
-                                          row_ptr, col_out, ids, id_bytes, full, D, too_long);
+                                          row_ptr, col_out, ids, id_bytes, full, D, too_long, tag_rows);
     cuda_check(cudaGetLastError(), "CSR build pass");
 }
 
