@@ -393,7 +393,7 @@ private:
     Scal red() { return Scal{nullptr, nullptr, nullptr, red_part_.p, red_cnt_.p}; }
 
     void start_from_host(const cd* v) {
-        cuda_check(cudaMemcpy(w_.p, v, n_ * 16, cudaMemcpyHostToDevice), "start upload");
+        upload_host(w_.p, v, n_ * 16, nullptr);
         have_start_ = true;
     }
     void start_fresh(std::mt19937_64& gen) {   // drawn on the device from a seed the lane's generator gives

@@ -107,7 +107,7 @@ GsOut gs_vector(const qb_sector* sec, const qb_program* prog, double2* u, int ma
     DevBuf<double2> seed(n), w(n);
     {
         const auto v0 = staged_seed(n, kGsStartSeed);
-        cuda_check(cudaMemcpy(seed.p, v0.data(), n * 16, cudaMemcpyHostToDevice), "seed upload");
+        upload_host(seed.p, v0.data(), n * 16, nullptr);
     }
     Reducer red;
     const int nb = red_blocks(n);

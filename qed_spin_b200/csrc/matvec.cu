@@ -373,7 +373,9 @@ void launch_rows_st(const qb_sector* row, const qb_sector* col, const qb_program
             launch_rows_shape<NV, ST, kF32, kOutF32, false>(shape, row, col, P, io, st);
         }
     };
-    const int shapes = NV == 1 ? 6 : 2;
+    // teams of lanes per state fill the GPU on small sectors; from 2^20 rows one thread per row already does (on
+    // chain-32 and 6x5, 4.7 M and 5.2 M rows, every team shape was 2-6x slower), so the tuner does not time them
+    const int shapes = NV == 1 && row->dim < (1ULL << 20) ? 6 : 2;
     const int tag = (NV << 4) | (static_cast<int>(sizeof(ST)) << 1) | (kF32 ? 1 : 0) | (kOutF32 ? 256 : 0);
     const unsigned gen = tune_generation();
     int shape = t_memo.find(row, col, P, tag, gen);

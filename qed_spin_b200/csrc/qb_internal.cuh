@@ -84,6 +84,8 @@ template <class F> int guarded(F&& f) {
 // calling thread's stream and the block is reused once it completes, so releasing never synchronises the device.
 void* dev_alloc(std::size_t bytes);
 void dev_free(void* p, std::size_t bytes);
+// A host-to-device copy that has completed on return; large pageable sources go through pinned slots (hostio.cu).
+void upload_host(void* dst, const void* src, std::size_t bytes, cudaStream_t st);
 std::size_t idle_cached_bytes();
 
 // A device allocation owned by a host object (released on the thread whose stream last used it, or after a
@@ -118,7 +120,7 @@ template <class T> struct DevBuf {
     }
     void upload(const T* h, std::size_t count) {
         alloc(count);
-        if (count) cuda_check(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+        if (count) upload_host(p, h, count * sizeof(T), nullptr);
     }
     void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
     std::size_t bytes() const { return n * sizeof(T); }

@@ -1024,7 +1024,7 @@ struct Recurrence {
         return nrm;
     }
     double start_from_host(const std::complex<double>* v0) {
-        cuda_check(cudaMemcpyAsync(w.p, v0, n * 16, cudaMemcpyHostToDevice, st), "v0 upload");
+        upload_host(w.p, v0, n * 16, st);
         return start_from_device(w.p);
     }
 

@@ -92,6 +92,8 @@ def test_chain32_a1_flip_bit_exact():
     D.matvec(S, S, P, [xd], [yd])
     torch.cuda.synchronize()
     assert np.array_equal(_bits(yd.cpu().numpy()), _bits(rs.gather(rp, x)))
+    # the host entry point: its 75 MB input goes through the pinned slots in 16 MB chunks (the last one partial)
+    assert np.array_equal(_bits(D.matvec_host(S, S, P, x)), _bits(yd.cpu().numpy()))
 
 
 def test_chain32_k2_levels_against_reference():
