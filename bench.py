@@ -80,7 +80,9 @@ SQ36_BLOCKS, SQ36_BLOCK_DIV = 4, 256
 # dram__bytes_write.sum of one launch (a one-pass metric set, captured on this workload after two warm-up applies).
 SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH = 418.38e9 + 2.02e9
 SPMV1_SQ36_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one spmv1<complex64> launch on this "
-                             "workload (profiles/spmv1_sq36_csr_dram.md)")
+                             "workload (profiles/spmv1_sq36_csr_dram.md): the thread-per-row kernel, which makes the "
+                             "same x gathers and reads the same CSR bytes as the timed four-lanes-per-row kernel; the "
+                             "timed kernel's full capture is of the 6.5 GB small case (profiles/spmv1_team32_sq36n11.md)")
 
 class Clocks:
     """SM clock, power and clock-event-reason samples (NVML, read only) taken every 10 ms while the timed
@@ -500,7 +502,8 @@ def main():
                        parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": hbm, "unit": "GB/s", "frac": ach32 / hbm,
                      "traffic": SPMV1_SQ36_DRAM_BYTES_PER_LAUNCH, "traffic_source": SPMV1_SQ36_TRAFFIC_SOURCE,
-                     "peak_kind": peak_kind, "kernel": "spmv1<complex64>",
+                     "peak_kind": peak_kind, "kernel": "spmv1_team32 (complex64 in and out, 4 lanes per row)",
+                     "traffic_kernel": "spmv1<complex64>",
                      "alg_bytes_per_launch": b_alg(8),
                      "alg_bytes_rule": "D*(8 rep + 8 inv_norm + 8 y) + D*e_bar*8 (one complex64 x element per "
                                        "emitted entry)",

@@ -519,83 +519,6 @@ __global__ void __launch_bounds__(256) spmv1_team32(u64 rows, const unsigned lon
     if (l == 0 && r < rows) Ld<kOutF32>::store(out, r, {ar + br, ai + bi});
 }
 
-// One vector with the reference's sum on long rows: 4 lanes per row as in spmv1_team32 (lane l reads the row's
-// windows l, l + 4, ...; a row's lanes read 64 contiguous bytes of columns a round and issue their x loads
-// together), each lane forms its window's products, and the row's first lane adds the round's 16 products
-// in entry order (its own, then lanes 1, 2 and 3's, passed by shuffles), acc += value * x from zero as in
-// spmv1. The same y as spmv1 bit for bit, in FP64 as in FP32 storage. u8 dictionary ids only.
-template <bool kInF32, bool kOutF32>
-__global__ void __launch_bounds__(256) spmv1_team_ordered(u64 rows, const unsigned long long* __restrict__ row_ptr,
-                                                          const u32* __restrict__ col,
-                                                          const unsigned char* __restrict__ ids,
-                                                          const double2* __restrict__ vals, int n_dict,
-                                                          const void* in_v, void* out_v) {
-    __shared__ double2 dict[256];
-    for (int i = threadIdx.x; i < n_dict; i += blockDim.x) dict[i] = vals[i];
-    __syncthreads();
-    using Li = Ld<kInF32>;
-    using Lo = Ld<kOutF32>;
-    const auto* in = static_cast<const typename Li::T*>(in_v);
-    auto* out = static_cast<typename Lo::T*>(out_v);
-    const u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const u64 r = t / kTeamLanes;
-    const int l = static_cast<int>(t % kTeamLanes);
-    const bool live = r < rows;
-    const u64 e0 = live ? row_ptr[r] : 0, e1 = live ? row_ptr[r + 1] : 0;
-    cplx acc{0.0, 0.0};
-    // rounds of 16 entries: base is the round's first window, shared by the row's lanes; the warp runs rounds while
-    // any of its rows has one left (the shuffles take every lane)
-    u64 base = e0 & ~3ULL;
-    while (__any_sync(0xffffffffu, base < e1)) {
-        const u64 w = base + 4 * static_cast<u64>(l);
-        double pr[4], pi[4];
-        bool on[4];
-        const bool mine = w < e1;
-        if (mine) {
-            const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + w));
-            const unsigned i4 = __ldg(reinterpret_cast<const unsigned*>(ids + w));
-            const u32 cj[4] = {c4.x, c4.y, c4.z, c4.w};
-            typename Li::T xv[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                on[q] = w + q >= e0 && w + q < e1;
-                if (on[q]) xv[q] = __ldg(in + cj[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                pr[q] = 0.0;
-                pi[q] = 0.0;
-                if (on[q]) {
-                    const double2 v = dict[(i4 >> (8 * q)) & 0xFFu];
-                    const cplx p = cmul({v.x, v.y}, Li::load(xv, q));
-                    pr[q] = p.re;
-                    pi[q] = p.im;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                on[q] = false;
-                pr[q] = 0.0;
-                pi[q] = 0.0;
-            }
-        }
-        // the round's products to the row's first lane, in entry order
-#pragma unroll
-        for (int src = 0; src < kTeamLanes; ++src) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double a = __shfl_sync(0xffffffffu, pr[q], src, kTeamLanes);
-                const double b = __shfl_sync(0xffffffffu, pi[q], src, kTeamLanes);
-                const bool o = __shfl_sync(0xffffffffu, on[q] ? 1 : 0, src, kTeamLanes) != 0;
-                if (l == 0 && o) acc = cadd(acc, {a, b});
-            }
-        }
-        base += 4 * kTeamLanes;
-    }
-    if (l == 0 && live) Lo::store(out, r, acc);
-}
-
 // k vectors interleaved by row: 8 lanes per row, lane l owns columns l, l + 8, ...; each column summed in
 // CSR order (the single apply's order).
 template <bool kInF32, bool kOutF32, int kCpl>
@@ -635,9 +558,10 @@ __global__ void __launch_bounds__(256) spmvk(u64 rows, int k, const unsigned lon
     }
 }
 
-// The single-vector kernel: four lanes per row when the rows hold at least kTeamMinRow entries on average (FP32 input:
-// spmv1_team32; FP64 input: spmv1_team_ordered, spmv1's sums), else one thread per row (spmv1). QB_SPMV_TEAM=0 or 1
-// forces one or the other.
+// The FP32-storage single-vector kernel: four lanes per row when the rows hold at least kTeamMinRow entries on
+// average, else one thread per row (spmv1). QB_SPMV_TEAM=0 or 1 forces one or the other. FP64 storage keeps spmv1:
+// four lanes per row with spmv1's ordered sums (the products passed to the row's first lane by shuffles) was 7%
+// slower on 6x6 (123 against 115 ms).
 constexpr u64 kTeamMinRow = 32;
 bool team32_for(const qb_csr* A) {
     static const int force = [] {
@@ -652,16 +576,11 @@ template <bool kInF32, bool kOutF32>
 void spmv_launch(const qb_csr* A, const void* in, void* out, int k, cudaStream_t st) {
     const unsigned char* ids = A->ids.p;
     const double2* vals = A->vals.p;
-    if (k == 1 && A->id_bytes == 1 && team32_for(A)) {
+    if (k == 1 && kInF32 && A->id_bytes == 1 && team32_for(A)) {
         const u64 threads = A->rows * kTeamLanes;
-        const unsigned grid = static_cast<unsigned>((threads + 255) / 256);
-        if (kInF32)
-            spmv1_team32<kOutF32><<<grid, 256, 0, st>>>(A->rows, A->row_ptr.p, A->col_idx.p, ids, vals, A->n_dict,
-                                                        static_cast<const float2*>(in),
-                                                        static_cast<typename Ld<kOutF32>::T*>(out));
-        else
-            spmv1_team_ordered<false, kOutF32><<<grid, 256, 0, st>>>(A->rows, A->row_ptr.p, A->col_idx.p, ids, vals,
-                                                                     A->n_dict, in, out);
+        spmv1_team32<kOutF32><<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(
+            A->rows, A->row_ptr.p, A->col_idx.p, ids, vals, A->n_dict, static_cast<const float2*>(in),
+            static_cast<typename Ld<kOutF32>::T*>(out));
     } else if (k == 1) {
         spmv1<kInF32, kOutF32><<<static_cast<unsigned>((A->rows + kRowsPerBlock - 1) / kRowsPerBlock), kRowsPerBlock, 0, st>>>(
             A->rows, A->row_ptr.p, A->col_idx.p, ids, A->id_bytes, vals, A->n_dict, in, out);
