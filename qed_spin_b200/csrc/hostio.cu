@@ -6,8 +6,8 @@
 // per-device set of pinned slots: worker threads copy the source chunk by chunk into the slots while the calling
 // thread queues each chunk's DMA on the caller's stream, in order, and records the slot's event; a slot is
 // refilled once its event has completed. The call returns when every chunk's copy has completed, as a pageable
-// cudaMemcpy would, so the caller may reuse its buffer at once. Small copies and pinned sources go straight to
-// cudaMemcpyAsync.
+// cudaMemcpy would, so the caller may reuse its buffer at once. Small copies, and sources that are not pageable host
+// memory (pinned, managed or device memory), go straight to cudaMemcpyAsync.
 // =============================================================================
 #include <atomic>
 #include <cstring>
@@ -43,12 +43,15 @@ Stager& stager(int dev) {
 void upload_host(void* dst, const void* src, std::size_t bytes, cudaStream_t st) {
     if (bytes == 0) return;
     cudaPointerAttributes attr{};
-    const bool pinned_src = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    const bool known = cudaPointerGetAttributes(&attr, src) == cudaSuccess;
     cudaGetLastError();   // an unregistered pointer may leave an error behind on older drivers
+    // only ordinary (pageable) host memory is staged; pinned, managed or device sources are copied directly
+    const bool pageable = !known || attr.type == cudaMemoryTypeUnregistered;
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (bytes < kStagedFrom || pinned_src || dev < 0 || dev >= 64) {
-        cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload");
+    if (bytes < kStagedFrom || !pageable || dev < 0 || dev >= 64) {
+        cuda_check(cudaMemcpyAsync(dst, src, bytes, pageable ? cudaMemcpyHostToDevice : cudaMemcpyDefault, st),
+                   "upload");
         cuda_check(cudaStreamSynchronize(st), "upload");
         return;
     }
