@@ -129,6 +129,12 @@ int qb_sector_acquire(const qb_sector_desc* desc, qb_sector** out);
 int qb_sector_release(qb_sector* s);
 int qb_registry_capacity(uint64_t bytes);
 int qb_registry_stats(uint64_t* sectors, uint64_t* idle_sectors, uint64_t* idle_bytes);
+/* The library's cache of released device blocks on the current device (a released block is kept, up to 16 GiB,
+ * for a later allocation of about its size, because cudaFree synchronises the device): free the oldest idle
+ * blocks until at most keep_bytes remain, and report what remains in *idle_bytes (may be NULL). After a large
+ * solve, trimming to 0 returns its buffers to the device, as torch.cuda.empty_cache does for torch's cache, so
+ * later small solves do not pay the frees one by one. The reference has no such cache (it frees per call). */
+int qb_memory_trim(uint64_t keep_bytes, uint64_t* idle_bytes);
 /* A sector's descriptor, representatives and 1/norms in a file (a checksummed little-endian format), and a
  * sector made from such a file (the tables and lookup rebuilt, no enumeration): the cached sector-table
  * format of repeated runs (the reference keeps its orbit tables in a registry, include/ed/basis/orbit_table.h). */

@@ -30,7 +30,8 @@ EXPORTS = [
     "qb_lanczos_noalloc", "qb_ground_state", "qb_eigs_k", "qb_eigs_levels", "qb_dynamics_t0", "qb_dynamics_t0_manifold", "qb_dense_levels",
     "qb_dense_levels_blocks",
     "qb_server_create", "qb_server_submit", "qb_server_wait", "qb_server_clock", "qb_server_destroy",
-    "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_sector_save",
+    "qb_sector_acquire", "qb_sector_release", "qb_registry_capacity", "qb_registry_stats", "qb_memory_trim",
+    "qb_sector_save",
     "qb_sector_load",
     "qb_tune_mode", "qb_tune_force", "qb_tune_clear", "qb_tune_save", "qb_tune_load", "qb_tune_entries",
 ]
@@ -141,6 +142,7 @@ def lib():
     L.qb_sector_acquire.argtypes = [C.POINTER(SectorDesc), C.POINTER(vp)]
     L.qb_sector_release.argtypes = [vp]
     L.qb_registry_capacity.argtypes = [u64]
+    L.qb_memory_trim.argtypes = [u64, C.c_void_p]
     L.qb_registry_stats.argtypes = [C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)]
     L.qb_sector_save.argtypes = [vp, C.c_char_p]
     L.qb_sector_load.argtypes = [C.c_char_p, C.POINTER(vp)]

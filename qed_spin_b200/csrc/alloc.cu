@@ -117,3 +117,12 @@ std::size_t idle_cached_bytes() {
 }
 
 }  // namespace qb
+
+extern "C" int qb_memory_trim(uint64_t keep_bytes, uint64_t* idle_bytes) {
+    return qb::guarded([&] {
+        qb::Cache& c = qb::cache(qb::current_device());
+        std::lock_guard<std::mutex> lk(c.mu);
+        qb::trim(c, static_cast<std::size_t>(keep_bytes));
+        if (idle_bytes) *idle_bytes = c.idle_bytes;
+    });
+}

@@ -544,6 +544,14 @@ def registry_capacity(nbytes: int) -> None:
     check(lib().qb_registry_capacity(int(nbytes)))
 
 
+def memory_trim(keep_bytes: int = 0) -> int:
+    """Frees the library's idle cached device blocks on the current device down to keep_bytes; returns the idle
+    bytes left (qb_memory_trim)."""
+    left = C.c_uint64()
+    check(lib().qb_memory_trim(int(keep_bytes), C.byref(left)))
+    return left.value
+
+
 def registry_stats() -> dict:
     a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
     check(lib().qb_registry_stats(C.byref(a), C.byref(b), C.byref(c)))
