@@ -168,11 +168,12 @@ template <class T> struct PoolBuf {
 
 // A warp per row (the reference's csr_count / csr_fill, src/gpu/rep_matvec.cu:933-989, likewise deal a row's
 // groups to the lanes of a warp). Lane l tests groups l, l + 32, ...; the acting ones' entries land in the
-// warp's buffer in group (emission) order under the key column << 8 | emission index. A bitonic sort of the
-// keys orders the entries by column and, within a column, by emission; each column's run is then summed in
-// that order and kept when not exactly zero (merge_row, include/ed/matvec/sector_rows.h:147-158).
+// warp's buffer in group (emission) order under the key column << 8 | emission index. A rank sort of the keys
+// orders the entries by column and, within a column, by emission; each column's run is then summed in that order
+// and kept when not exactly zero (merge_row, include/ed/matvec/sector_rows.h:147-158). Eight warps a block share
+// the staged tables.
 // pass 0: merged row lengths, and the merged values into the dictionary set; pass 2: columns and ids.
-constexpr int kBuildWarps = 4;
+constexpr int kBuildWarps = 8;
 constexpr int kColSetBits = 8;   // the count pass's per-warp column set: 256 slots, for rows of up to 128 entries
 constexpr int kColSet = 1 << kColSetBits;
 
@@ -182,15 +183,17 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
                                                              unsigned long long* counts,
                                                              const unsigned long long* row_ptr, u32* col_out,
                                                              unsigned char* ids, int id_bytes, double2* full_vals,
-                                                             Dict D, int* too_long, bool tag_rows) {
+                                                             Dict D, int* too_long, bool tag_rows, int cap) {
     extern __shared__ __align__(16) unsigned char smem[];
     const SmemProgram sp = stage(P, col, smem, prog_in_smem);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    u64* keys = reinterpret_cast<u64*>(smem + stage_bytes) + wid * kMaxRowEntries;
-    double2* vals = reinterpret_cast<double2*>(smem + stage_bytes + kBuildWarps * kMaxRowEntries * 8) +
-                    wid * kMaxRowEntries;
+    // each warp's row buffer holds cap entries (a multiple of 32, at least the program's groups up to 256)
+    u64* keys = reinterpret_cast<u64*>(smem + stage_bytes) + wid * cap;
+    double2* vals = reinterpret_cast<double2*>(smem + stage_bytes + static_cast<std::size_t>(kBuildWarps) * cap * 8) +
+                    wid * cap;
     // the count pass's column set: a warp's slots tagged row << 32 | column, so no row clears them
-    u64* cset = reinterpret_cast<u64*>(smem + stage_bytes + kBuildWarps * kMaxRowEntries * 24) + wid * kColSet;
+    u64* cset = reinterpret_cast<u64*>(smem + stage_bytes + static_cast<std::size_t>(kBuildWarps) * cap * 24) +
+                wid * kColSet;
     if (pass == 0) {
         for (int i = lane; i < kColSet; i += 32) cset[i] = ~0ULL;
         __syncwarp();
@@ -246,13 +249,13 @@ __global__ void __launch_bounds__(32 * kBuildWarps) csr_pass(DSector row, DSecto
             }
             const unsigned bal = __ballot_sync(0xffffffffu, ok);
             const int pos = m + __popc(bal & lt);
-            if (ok && pos < kMaxRowEntries) {
+            if (ok && pos < cap) {
                 keys[pos] = (static_cast<u64>(j) << 8) | static_cast<u64>(pos);
                 vals[pos] = make_double2(c.re, c.im);
             }
             m += __popc(bal);
         }
-        if (m > kMaxRowEntries) {
+        if (m > cap) {
             if (lane == 0) {
                 *too_long = 1;
                 if (pass == 0) counts[r] = 0;
@@ -609,7 +612,13 @@ void run_pass(const qb_sector* row, const qb_sector* col, const qb_program* P, i
               const Dict& D, int* too_long) {
     bool in_smem = false;
     const std::size_t stage_bytes = (smem_for(P, col, in_smem) + 15) & ~std::size_t(15);
-    const std::size_t smem = stage_bytes + kBuildWarps * kMaxRowEntries * (8 + 16) + kBuildWarps * kColSet * 8;
+    // a row holds at most one entry per group: buffers of the program's groups rounded up to 32 (256 at most), so
+    // more warps fit an SM than with 256-entry buffers
+    const u32 ng = P->view.n_groups;
+    const int cap = ng <= static_cast<u32>(kMaxRowEntries) ? std::max(32, static_cast<int>((ng + 31) / 32 * 32))
+                                                          : kMaxRowEntries;
+    const std::size_t smem = stage_bytes + static_cast<std::size_t>(kBuildWarps) * cap * (8 + 16) +
+                             static_cast<std::size_t>(kBuildWarps) * kColSet * 8;
     auto k = csr_pass<ST, kSame>;
     set_smem(k, smem);
     int sms = 148, dev = 0;
@@ -620,7 +629,7 @@ void run_pass(const qb_sector* row, const qb_sector* col, const qb_program* P, i
     // row tags hold the low 32 bits of the row: rows past 2^32 take the sorting path
     const bool tag_rows = row->dim < (1ULL << 32);
     k<<<blocks, 32 * kBuildWarps, smem>>>(row->view(), col->view(), P->view, in_smem, stage_bytes, pass, counts,
-                                          row_ptr, col_out, ids, id_bytes, full, D, too_long, tag_rows);
+                                          row_ptr, col_out, ids, id_bytes, full, D, too_long, tag_rows, cap);
     cuda_check(cudaGetLastError(), "CSR build pass");
 }
 
