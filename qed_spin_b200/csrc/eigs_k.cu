@@ -416,7 +416,7 @@ private:
         const int chunks = dot_chunks(n_, (nb + kDotVecs - 1) / kDotVecs);
         k_dots8<T><<<dim3(chunks, (nb + kDotVecs - 1) / kDotVecs), kThreads>>>(n_, nb, basis() + from, w_.p, part_.p,
                                                                                chunks, flag);
-        k_dot_sum<<<(nb + 127) / 128, 128>>>(nb, chunks, part_.p, coef_.p, flag);
+        k_dot_sum<<<dot_sum_blocks(nb), 32 * kDotSumWarps>>>(nb, chunks, part_.p, coef_.p, flag);
     }
 
     // One reorthogonalisation pass of w against the first nb table entries, then a second when the DGKS gate

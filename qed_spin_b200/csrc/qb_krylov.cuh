@@ -13,8 +13,10 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <random>
+#include <utility>
 #include <vector>
 
 #include <atomic>
@@ -292,17 +294,26 @@ __global__ void k_dot_part(std::uint64_t n, const T* const* basis, const double2
     if (threadIdx.x == 0) part[static_cast<std::size_t>(blockIdx.y) * chunks + blockIdx.x] = make_double2(acc[0], acc[1]);
 }
 
+// A warp per vector: lane l adds chunks l, l + 32, ... in order, then a fixed butterfly adds the lanes (the same
+// order every call). Launch with kDotSumWarps warps a block: k_dot_sum<<<dot_sum_blocks(m), 32 * kDotSumWarps>>>.
+constexpr int kDotSumWarps = 4;
+inline int dot_sum_blocks(int m) { return (m + kDotSumWarps - 1) / kDotSumWarps; }
 __global__ void k_dot_sum(int m, int chunks, const double2* part, double2* coeff, const int* flag) {
     if (flag && *flag == 0) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m) return;
+    const int k = blockIdx.x * kDotSumWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    if (k >= m) return;   // whole warps leave together
     double sx = 0.0, sy = 0.0;
-    for (int c = 0; c < chunks; ++c) {
+    for (int c = lane; c < chunks; c += 32) {
         const double2 p = part[static_cast<std::size_t>(k) * chunks + c];
         sx += p.x;
         sy += p.y;
     }
-    coeff[k] = make_double2(-sx, -sy);
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (lane == 0) coeff[k] = make_double2(-sx, -sy);
 }
 
 // The chunk count of a dot_many over m vectors of length n: about kMaxRedBlocks blocks in all.
@@ -318,7 +329,7 @@ void dot_many(std::uint64_t n, int m, const T* const* basis, const double2* w, d
               const int* flag, cudaStream_t st) {
     const int chunks = dot_chunks(n, m);
     k_dot_part<T><<<dim3(chunks, m), kThreads, 0, st>>>(n, basis, w, part, chunks, flag);
-    k_dot_sum<<<(m + 127) / 128, 128, 0, st>>>(m, chunks, part, coeff, flag);
+    k_dot_sum<<<dot_sum_blocks(m), 32 * kDotSumWarps, 0, st>>>(m, chunks, part, coeff, flag);
 }
 
 // w += sum_k coeff[k] V_k, each element accumulated in k order.
@@ -897,6 +908,33 @@ struct HostVec {
     std::size_t size() const { return n; }
 };
 
+// The generator's ring of raw outputs, kept between draws: a fresh ring (77 MB with 16 host threads) cost its page
+// faults on every draw. One ring per draw in flight; a draw takes an idle ring of its size or makes one.
+struct SeedRings {
+    std::mutex mu;
+    std::vector<std::pair<std::size_t, std::unique_ptr<std::uint64_t[]>>> idle;
+    std::pair<std::size_t, std::unique_ptr<std::uint64_t[]>> take(std::size_t n) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (auto it = idle.begin(); it != idle.end(); ++it)
+                if (it->first == n) {
+                    auto r = std::move(*it);
+                    idle.erase(it);
+                    return r;
+                }
+        }
+        return {n, std::unique_ptr<std::uint64_t[]>(new std::uint64_t[n])};   // left uninitialised
+    }
+    void give(std::pair<std::size_t, std::unique_ptr<std::uint64_t[]>> r) {
+        std::lock_guard<std::mutex> lk(mu);
+        idle.push_back(std::move(r));
+    }
+};
+inline SeedRings& seed_rings() {
+    static SeedRings* r = new SeedRings;   // never destroyed: rings may outlive static destructors at exit
+    return *r;
+}
+
 void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed) {
     if (n < (std::size_t{1} << 20)) {
         std::mt19937_64 gen(seed);
@@ -911,7 +949,8 @@ void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed
     constexpr std::size_t kAtt = static_cast<std::size_t>(Mt64::kN) * 256;   // polar attempts per chunk
     const int nw = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) - 1);
     const std::size_t ring = 4 * static_cast<std::size_t>(nw);
-    std::vector<std::uint64_t> buf(ring * 2 * kAtt);
+    auto ring_buf = seed_rings().take(ring * 2 * kAtt);
+    std::uint64_t* const buf_p = ring_buf.second.get();
     struct Slot {
         std::atomic<std::size_t> chunk{~std::size_t{0}};   // the chunk it holds (ready), or none
         std::atomic<bool> busy{false};
@@ -927,7 +966,7 @@ void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed
             Slot& sl = slots[c % ring];
             while (sl.busy.load(std::memory_order_acquire)) std::this_thread::yield();
             sl.busy.store(true, std::memory_order_relaxed);
-            std::uint64_t* r = buf.data() + (c % ring) * 2 * kAtt;
+            std::uint64_t* r = buf_p + (c % ring) * 2 * kAtt;
             for (std::size_t b = 0; b < 2 * kAtt; b += Mt64::kN) gen.block(r + b);
             const std::size_t k = polar_count(r, kAtt);
             sl.off = off;
@@ -946,7 +985,7 @@ void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed
                     if (nc != ~std::size_t{0} && c >= nc) return;
                     std::this_thread::yield();
                 }
-                const std::uint64_t* r = buf.data() + (c % ring) * 2 * kAtt;
+                const std::uint64_t* r = buf_p + (c % ring) * 2 * kAtt;
                 std::size_t i = sl.off;
                 for (std::size_t a = 0; a < kAtt && i < n; ++a) {
                     double x, y;
@@ -960,6 +999,7 @@ void staged_seed_into(std::complex<double>* v, std::size_t n, std::uint64_t seed
             }
         });
     for (auto& t : pool) t.join();
+    seed_rings().give(std::move(ring_buf));
 }
 
 HostVec staged_seed(std::size_t n, std::uint64_t seed) {
