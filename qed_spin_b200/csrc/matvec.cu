@@ -41,15 +41,17 @@ template <int NV> struct VecPtrs {
     void* out[NV];
 };
 
-// Five blocks per SM for one or two vectors (48 registers): the walk is bound by instruction issue and by the
-// latency of its dependent loads, and the extra warps hide it. A sweep of 4, 5, 6 and 8 blocks per SM (CUDA events,
-// one FP32 vector): chain-32 2.94 / 2.58 / 2.63 / 2.69 ms, 6x5 9.45 / 8.35 / 8.98 / 9.79 ms, 6x6 1,332 / 1,204 /
-// 1,298 / 1,534 ms. More vectors keep four.
+// One or two vectors: six blocks per SM for 32-bit states (40 registers), five for 64-bit states (48 registers);
+// the walk is bound by instruction issue and by the latency of its dependent loads, and the extra warps hide it.
+// A sweep of 4, 5, 6 and 8 blocks per SM (CUDA events, one FP32 vector, copies of this kernel): chain-32 2.94 /
+// 2.58 / 2.63 / 2.69 ms, 6x5 9.45 / 8.35 / 8.98 / 9.79 ms, 6x6 1,332 / 1,204 / 1,298 / 1,534 ms; in the library
+// itself five blocks measured no faster than six on chain-32 (2.64 ms at six in four bench runs), so 32-bit states
+// keep six. More vectors keep four.
 // One thread per row. The row's groups are tested 32 at a time by every lane together (a converged
 // pass that builds the bitmask of the groups acting on the lane's row); the lanes then walk their own
 // acting groups in ascending order -- the diagonal first -- canonicalising one target each per step.
 template <int NV, class ST, bool kInF32, bool kOutF32, bool kSame>
-__global__ void __launch_bounds__(256, (NV <= 2 ? 5 : 4)) walk_rows(DSector row, DSector col, DProgram P, bool prog_in_smem,
+__global__ void __launch_bounds__(256, (NV <= 2 ? (sizeof(ST) == 4 ? 6 : 5) : 4)) walk_rows(DSector row, DSector col, DProgram P, bool prog_in_smem,
                                                     VecPtrs<NV> io) {
     extern __shared__ __align__(16) unsigned char smem[];
     using St = Store<kInF32>;
